@@ -1,0 +1,275 @@
+"""Python mirror of fastbart's R interface (R/fwbart.R, R/fpbart.R, R/predict_draw.R) on the B200 library.
+
+fwbart()/fpbart() take BART's arguments and return the fields of BART's "wbart"/"pbart" objects (R names, dots
+included); compile_trees()/predict_draw() reproduce the fast single-draw evaluator.  All compute runs in
+libfastbart_b200.so on the GPU; there is no CPU fallback (the reference falls back to BART::wbart / BART::pbart for
+unsupported settings; BART is not available here, so those settings raise FastbartError(FB_ERR_LIMIT)).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+from scipy import stats
+
+from . import _lib, prep, workloads
+from ._lib import NODES, FastbartError, check, ptr
+
+__all__ = ["fwbart", "fpbart", "compile_trees", "predict_draw", "fit_batch", "Batch", "trees_text", "varcount",
+           "FastbartError"]
+
+
+class BartFit(dict):
+    """A fitted model: a dict with the R object's fields; .cls is "wbart" or "pbart"."""
+
+    def __init__(self, cls: str, **kw):
+        super().__init__(**kw)
+        self.cls = cls
+
+
+# ------------------------------------------------------------------------------------------------ batches
+def _as_chain(ch: dict, keep: list) -> _lib.Chain:
+    q = np.ascontiguousarray(ch["q"], dtype=np.uint8)
+    p, n = q.shape
+    probit = int(ch.get("probit", 0))
+    y = None if probit else np.ascontiguousarray(ch["y"], dtype=np.float64)
+    wt = ch.get("wt")
+    wt = None if wt is None else np.ascontiguousarray(wt, dtype=np.float64)
+    ybin = np.ascontiguousarray(ch["ybin"], dtype=np.int32) if probit else None
+    numcut = np.ascontiguousarray(ch["numcut"], dtype=np.int32)
+    pg = np.ascontiguousarray(ch["pgtab"], dtype=np.float64)
+    keep += [q, y, wt, ybin, numcut, pg]
+    return _lib.Chain(n, p, int(ch["ntree"]), ptr(q), ptr(y), ptr(wt), ptr(ybin), ptr(numcut), ptr(pg),
+                      float(ch["tau"]), float(ch["lambda"]), float(ch["nu"]), float(ch["sigest"]),
+                      float(ch.get("offset", 0.0)), int(ch["seed"]) & 0xFFFFFFFFFFFFFFFF, probit,
+                      int(ch.get("fx_shift", 0)), int(ch.get("rss_shift", 0)))
+
+
+def _alloc_out(ch: dict, nskip: int, ndpost: int, trees: bool = True, alloc=np.empty):
+    n = np.asarray(ch["q"]).shape[1]
+    m = int(ch["ntree"])
+    o = dict(sigma=alloc(nskip + ndpost, dtype=np.float64), yhat_mean=alloc(n, dtype=np.float64),
+             yhat=alloc((ndpost, n), dtype=np.float64),
+             trees=alloc((ndpost, m, NODES), dtype=np.uint64) if trees else None)
+    s = _lib.ChainOut(ptr(o["sigma"]), ptr(o["yhat_mean"]), ptr(o["yhat"]), ptr(o["trees"]))
+    return o, s
+
+
+def _collect(o: dict, s: _lib.ChainOut) -> dict:
+    o["moves"] = np.array(list(s.moves), dtype=np.int32)
+    o["rtnorm_caps"] = int(s.rtnorm_caps)
+    return o
+
+
+def _options(nskip, ndpost, threads=0, sweeps_per_launch=0, device=0) -> _lib.Options:
+    return _lib.Options(int(nskip), int(ndpost), int(threads), int(sweeps_per_launch), int(device))
+
+
+def fit_batch(chains: Sequence[dict], nskip: int, ndpost: int, threads: int = 0, sweeps_per_launch: int = 0,
+              device: int = 0, trees: bool = True) -> list:
+    """Runs prepared chains (dicts as built by workloads.fwbart_chain / fpbart_chain) in one device batch."""
+    keep: list = []
+    arr = (_lib.Chain * len(chains))(*[_as_chain(c, keep) for c in chains])
+    outs = [_alloc_out(c, nskip, ndpost, trees) for c in chains]
+    oarr = (_lib.ChainOut * len(chains))(*[s for _, s in outs])
+    opt = _options(nskip, ndpost, threads, sweeps_per_launch, device)
+    check(_lib.lib().fb_fit_batch(arr, len(chains), C.byref(opt), oarr))
+    return [_collect(o, oarr[k]) for k, (o, _) in enumerate(outs)]
+
+
+class Batch:
+    """Staged batch: inputs uploaded once; run() repeats the full MCMC on the device; download() copies outputs."""
+
+    def __init__(self, chains: Sequence[dict], nskip: int, ndpost: int, threads: int = 0, sweeps_per_launch: int = 0,
+                 device: int = 0):
+        self._keep: list = []
+        self.chains = list(chains)
+        self.nskip, self.ndpost = int(nskip), int(ndpost)
+        arr = (_lib.Chain * len(chains))(*[_as_chain(c, self._keep) for c in chains])
+        opt = _options(nskip, ndpost, threads, sweeps_per_launch, device)
+        h = C.c_void_p()
+        check(_lib.lib().fb_batch_create(arr, len(chains), C.byref(opt), C.byref(h)))
+        self._h = h
+
+    def run(self, stream: int | None = None):
+        check(_lib.lib().fb_batch_run(self._h, stream))
+
+    def sync(self):
+        check(_lib.lib().fb_batch_sync(self._h))
+
+    def launch_info(self) -> dict:
+        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+        check(_lib.lib().fb_batch_launch_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return dict(launches=a.value, threads=b.value, grid=c.value, smem=d.value)
+
+    def download(self, trees: bool = True, alloc=np.empty) -> list:
+        outs = [_alloc_out(c, self.nskip, self.ndpost, trees, alloc) for c in self.chains]
+        oarr = (_lib.ChainOut * len(outs))(*[s for _, s in outs])
+        check(_lib.lib().fb_batch_download(self._h, oarr))
+        return [_collect(o, oarr[k]) for k, (o, _) in enumerate(outs)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().fb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------------------------------------ tree text
+def trees_text(trees: np.ndarray, p: int) -> str:
+    t = np.ascontiguousarray(trees, dtype=np.uint64)
+    nd, m = t.shape[0], t.shape[1]
+    L = _lib.lib()
+    ln = L.fb_trees_text(ptr(t), nd, m, p, None, 0)
+    buf = C.create_string_buffer(ln + 1)
+    L.fb_trees_text(ptr(t), nd, m, p, buf, ln + 1)
+    return buf.raw[:ln].decode()
+
+
+def varcount(trees: np.ndarray, p: int) -> np.ndarray:
+    t = np.ascontiguousarray(trees, dtype=np.uint64)
+    out = np.zeros((t.shape[0], p), dtype=np.int32)
+    check(_lib.lib().fb_varcount(ptr(t), t.shape[0], t.shape[1], p, ptr(out)))
+    return out
+
+
+# ------------------------------------------------------------------------------------------------ R-shaped API
+def _unsupported(name, sparse, x_test, n, p, ntree, numcut_v, extra):
+    if sparse or (x_test is not None and np.size(x_test) > 0) or n > prep.NMAX or p > prep.PMAX or \
+            ntree > prep.MMAX or (numcut_v.size and numcut_v.max() > prep.NUMCUT_MAX) or extra:
+        raise FastbartError(_lib.FB_ERR_LIMIT, f"{name}: unsupported settings (sparse, x.test, n > 65536, p > 32, "
+                                               f"ntree > 200, numcut > 255 or extra arguments)")
+
+
+def fwbart(x_train, y_train, x_test=None, sparse=False, xinfo=None, usequants=False, cont=False, rm_const=True,
+           sigest=None, sigdf=3, sigquant=0.90, k=2.0, power=2.0, base=0.95, sigmaf=None, lambda_=None, fmean=None,
+           w=None, ntree=200, numcut=100, ndpost=1000, nskip=100, printevery=100, seed=None, device=0, **extra) -> BartFit:
+    """Drop-in for BART::wbart (R/fwbart.R:4-45).  Returns the "wbart" fields."""
+    d = prep.model_matrix(x_train, numcut, rm_const, xinfo)
+    y = np.asarray(y_train, dtype=np.float64)
+    n, p = y.size, d.X.shape[1]
+    _unsupported("fwbart", sparse, x_test, n, p, ntree, d.numcut, extra)
+    fm = float(np.mean(y)) if fmean is None else float(fmean)
+    w = np.ones(n) if w is None else np.asarray(w, dtype=np.float64)
+    yc = y - fm
+    nu = float(sigdf)
+    if lambda_ is None:
+        if sigest is None:
+            sigest = prep.sigest_lm(d.X, yc) if p < n else float(np.std(yc, ddof=1))
+        lambda_ = sigest * sigest * stats.chi2.ppf(1.0 - sigquant, nu) / nu
+    else:
+        sigest = float(np.sqrt(lambda_))
+    tau = (yc.max() - yc.min()) / (2 * k * np.sqrt(ntree)) if sigmaf is None else sigmaf / np.sqrt(ntree)
+    if seed is None:
+        seed = int(np.random.default_rng().integers(1, 2**63))
+    ch = dict(q=d.q, y=yc, wt=1.0 / (w * w), numcut=d.numcut, pgtab=prep.pg_table(base, power), tau=float(tau),
+              nu=nu, sigest=float(sigest), offset=0.0, seed=int(seed), probit=0, ntree=int(ntree))
+    ch["lambda"] = float(lambda_)
+    o = fit_batch([ch], nskip, ndpost, device=device)[0]
+    names = d.colnames
+    xi = {nm: d.xi[v] for v, nm in enumerate(names)}
+    return BartFit("wbart", sigma=o["sigma"], **{"yhat.train.mean": o["yhat_mean"] + fm,
+                                                "yhat.train": o["yhat"] + fm},
+                   varcount=varcount(o["trees"], p), varprob=np.full((ndpost, p), 1.0 / p),
+                   treedraws=dict(cutpoints=xi, trees=trees_text(o["trees"], p)), mu=fm, moves=o["moves"],
+                   **{"rm.const": d.rm_const, "varcount.mean": varcount(o["trees"], p).mean(axis=0),
+                      "varprob.mean": np.full(p, 1.0 / p)}, colnames=names)
+
+
+def fpbart(x_train, y_train, x_test=None, sparse=False, xinfo=None, usequants=False, cont=False, rm_const=True,
+           k=2.0, power=2.0, base=0.95, binaryOffset=None, ntree=50, numcut=100, ndpost=1000, nskip=100,
+           printevery=100, seed=None, device=0, **extra) -> BartFit:
+    """Drop-in for BART::pbart (R/fpbart.R:4-41).  Returns the "pbart" fields."""
+    y = np.asarray(y_train).astype(np.int32)
+    off = float(stats.norm.ppf(np.mean(y))) if binaryOffset is None else float(binaryOffset)
+    d = prep.model_matrix(x_train, numcut, rm_const, xinfo)
+    n, p = y.size, d.X.shape[1]
+    _unsupported("fpbart", sparse, x_test, n, p, ntree, d.numcut, extra)
+    tau = 3.0 / (k * np.sqrt(ntree))
+    if seed is None:
+        seed = int(np.random.default_rng().integers(1, 2**63))
+    ch = dict(q=d.q, ybin=y, numcut=d.numcut, pgtab=prep.pg_table(base, power), tau=float(tau), nu=3.0, sigest=1.0,
+              offset=off, seed=int(seed), probit=1, ntree=int(ntree))
+    ch["lambda"] = 1.0
+    o = fit_batch([ch], nskip, ndpost, device=device)[0]
+    names = d.colnames
+    yh = o["yhat"] + off
+    prob = stats.norm.cdf(yh)
+    vc = varcount(o["trees"], p)
+    return BartFit("pbart", **{"yhat.train": yh, "prob.train": prob, "prob.train.mean": prob.mean(axis=0)},
+                   varcount=vc, varprob=np.full((ndpost, p), 1.0 / p),
+                   treedraws=dict(cutpoints={nm: d.xi[v] for v, nm in enumerate(names)}, trees=trees_text(o["trees"], p)),
+                   binaryOffset=off, moves=o["moves"],
+                   **{"rm.const": d.rm_const, "varcount.mean": vc.mean(axis=0), "varprob.mean": np.full(p, 1.0 / p)},
+                   colnames=names)
+
+
+class CompiledTrees:
+    """Result of compile_trees(): flat node arrays on the device (and host copies, as compile_trees_cpp returns)."""
+
+    def __init__(self, text: str, cutpoints: Sequence[np.ndarray], mu: float = 0.0, rm_const=None,
+                 probit: bool = False, device: int = 0):
+        xs = [np.ascontiguousarray(c, dtype=np.float64) for c in cutpoints]
+        self._xs = xs
+        ptrs = (C.c_void_p * max(1, len(xs)))(*[x.ctypes.data for x in xs])
+        nc = np.array([x.size for x in xs], dtype=np.int32)
+        h = C.c_void_p()
+        raw = text.encode()
+        check(_lib.lib().fb_compile_trees(raw, len(raw), ptrs, ptr(nc), len(xs), int(device), C.byref(h)))
+        self._h = h
+        nd, m, p, nn = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(_lib.lib().fb_compiled_info(h, C.byref(nd), C.byref(m), C.byref(p), C.byref(nn)))
+        self.ndpost, self.ntree, self.p, self.nnodes = nd.value, m.value, p.value, nn.value
+        self.mu, self.rm_const, self.probit = float(mu), rm_const, bool(probit)
+
+    def arrays(self) -> dict:
+        N = self.nnodes
+        var, child = np.zeros(N, np.int32), np.zeros(N, np.int32)
+        cut, theta = np.zeros(N), np.zeros(N)
+        root = np.zeros(self.ndpost * self.ntree, np.int32)
+        check(_lib.lib().fb_compiled_arrays(self._h, ptr(var), ptr(child), ptr(cut), ptr(theta), ptr(root)))
+        return dict(ndpost=self.ndpost, ntree=self.ntree, p=self.p, var=var, child=child, cut=cut, theta=theta,
+                    root=root)
+
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                _lib.lib().fb_compiled_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def compile_trees(fit: BartFit, device: int = 0) -> CompiledTrees:
+    """compile_trees() of R/predict_draw.R:3-10."""
+    cps = list(fit["treedraws"]["cutpoints"].values())
+    if fit.get("binaryOffset") is not None:
+        mu = fit["binaryOffset"]
+    else:
+        mu = fit.get("mu", fit.get("offset", 0.0))
+    return CompiledTrees(fit["treedraws"]["trees"], cps, mu, fit.get("rm.const"), getattr(fit, "cls", "") == "pbart",
+                         device)
+
+
+def predict_draw(ct: CompiledTrees, newdata, m: int) -> np.ndarray:
+    """predict_draw() of R/predict_draw.R:13-18: f (+ mu) of posterior draw m (1-based) on the rows of newdata."""
+    X = np.asarray(newdata, dtype=np.float64)
+    if X.ndim == 1:
+        X = X[:, None]
+    if ct.rm_const is not None and len(ct.rm_const) < X.shape[1]:
+        X = X[:, np.asarray(ct.rm_const) - 1]
+    cols = [np.ascontiguousarray(X[:, j]) for j in range(X.shape[1])]
+    n = X.shape[0]
+    ptrs = (C.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+    out = np.zeros(n)
+    check(_lib.lib().fb_predict_draw(ct.handle(), ptrs, len(cols), n, int(m), ct.mu, ptr(out)))
+    return out

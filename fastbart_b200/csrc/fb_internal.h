@@ -1,0 +1,105 @@
+// fb_internal.h -- layouts shared by the host code (host.cpp) and the CUDA kernels (sampler.cu, predict.cu).
+#pragma once
+#include <cstdint>
+
+namespace fb {
+
+constexpr int NODES = 64;      // node slots per tree (src/bart_kernel.h:23)
+constexpr int PMAX = 32;       // predictors (src/bart_kernel.h:20)
+constexpr int MMAX = 200;      // trees (src/bart_kernel.h:21)
+constexpr int NMAX = 65536;    // rows per chain (src/bart_kernel.h:16)
+constexpr int MAXDEPTH = 24;   // src/bart_kernel.h:33
+constexpr int NB_MAX = 8;      // per-thread register bins of the fused pass; leaves beyond use shared atomics
+constexpr int MAX_THREADS = 512;
+
+// Topology of one tree: 64 node slots (leaf values are kept apart, in th[]).  464 bytes, 16-byte multiple.
+struct DTree {
+  uint8_t l[NODES], r[NODES], par[NODES], v[NODES], c[NODES], d[NODES], ngv[NODES];
+  unsigned long long used, leaf;
+};
+static_assert(sizeof(DTree) == 464, "DTree layout");
+
+// Per-chain descriptor (device resident, read-only while sampling).  Offsets are in elements of the batch arrays.
+struct DChain {
+  int n, p, m, n_pad;
+  int probit, fx_shift, rss_shift, root_ngv;
+  int nskip, ndpost, pad0, pad1;
+  int numcut[PMAX];
+  double tau, lambda, nu, sigest, offset;
+  double pg[NODES];
+  unsigned long long seed;
+  long long off_row;    // y, w, ybin, tm, rsave: [n_pad]
+  long long off_q;      // codes [p][n_pad]
+  long long off_leaf;   // leaf ids [m][n_pad]
+  long long off_tree;   // trees, th [m][64], s0 [m][64]
+  long long off_sigma;  // [nskip + ndpost]
+  long long off_yhat;   // [ndpost][n]
+  long long off_tout;   // [ndpost][m][64]
+};
+
+// Mutable per-chain state kept between launches.
+struct DState {
+  double sigma;
+  int births, deaths, caps, rtcaps;
+  int it_done, status, pad0, pad1;
+};
+
+// Device buffers of one batch.
+struct DBufs {
+  const DChain* chains;
+  DState* states;
+  const uint8_t* q;
+  const double* yin;
+  double* ywork;
+  const float* win;
+  const int8_t* ybin;
+  float* rsave;
+  uint8_t* leaf;
+  DTree* trees;
+  long long* s0;
+  float* th;
+  double* tm;
+  double* sigma_out;
+  double* yhat_out;
+  unsigned long long* trees_out;
+  const int* order;
+  int* queue;
+  int nchains;
+  int m_max;
+  int n_pad_max;
+  int rows_in_smem;
+};
+
+size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem);
+int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, void* stream);
+int sampler_max_grid(int threads, size_t smem, int device);
+
+// Per-tree pass on explicit state (diagnostics / parity tests): one CTA.
+struct DPassArgs {
+  int n, n_pad, apply, stats;
+  int pmode, pnx, pc, pL, pR, pl, pr;
+  int cmode, cnx, cc;
+  int fx_shift, rows_in_smem;
+  unsigned long long leafmask;   // leaves of the current tree
+  uint8_t* leaf_prev;            // [n_pad] in/out
+  const uint8_t* leaf_cur;       // [n_pad]
+  const uint8_t* qprev;          // [n_pad]
+  const uint8_t* qcur;           // [n_pad]
+  float* r;                      // [n_pad] in/out
+  const float* w;                // [n_pad]
+  const float* tho;              // [64]
+  const float* thn;              // [64]
+  const float* thc;              // [64]
+  long long* out;                // [64 + 4 + 2]: S1 per slot, sL0 sL1 sR0 sR1, nL nR
+};
+int launch_debug_pass(DPassArgs a, int threads, void* stream);
+
+// Evaluator (predict_draw) on device.
+struct DForest {
+  const int* var; const int* child; const double* cut; const double* theta; const int* root;
+  int ntree, ndpost, p, nnodes;
+};
+int launch_predict(const DForest& f, const double* x, int n, int ld, int draw0, int ndraws, double mu, double* out,
+                   int ldo, void* stream);
+
+}  // namespace fb

@@ -1,0 +1,661 @@
+// host.cpp -- C ABI of libfastbart_b200.so (include/fastbart_b200.h): batch set-up and transfers for the sampler
+// kernel, BART tree-text assembly, compile_trees parsing and predict_draw launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/fastbart_b200.h"
+#include "fb_internal.h"
+
+using namespace fb;
+
+namespace {
+
+thread_local std::string g_err;
+
+fb_status fail(fb_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return s;
+}
+
+#define CK(call)                                                                                     \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess) return fail(FB_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));        \
+  } while (0)
+
+long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+// Fixed-point scales: every per-row term llrint(w*R*2^S) (and llrint(w*e^2*2^Srss)) summed over n rows stays below
+// 2^61 even for residuals 64 times the data range.
+void auto_shifts(const fb_chain& c, int* s, int* srss) {
+  double wmax = 1.0, ymax = 10.0;
+  if (c.wt) { wmax = 0.0; for (int i = 0; i < c.n; i++) wmax = std::max(wmax, c.wt[i]); }
+  if (!c.probit && c.y) { ymax = 0.0; for (int i = 0; i < c.n; i++) ymax = std::max(ymax, std::fabs(c.y[i])); }
+  const double rb = 64.0 * (ymax + 1.0);
+  int a = 61 - (int)std::ceil(std::log2((double)c.n * std::max(wmax, 1e-300) * rb + 1.0));
+  int b = 61 - (int)std::ceil(std::log2((double)c.n * std::max(wmax, 1e-300) * rb * rb + 1.0));
+  *s = std::min(std::max(a, 8), 40);
+  *srss = std::min(std::max(b, 0), 40);
+}
+
+fb_status check_chain(const fb_chain& c, int k) {
+  if (c.n < 1 || c.p < 1 || c.ntree < 1) return fail(FB_ERR_ARG, "chain %d: n, p and ntree must be positive", k);
+  if (c.n > NMAX) return fail(FB_ERR_LIMIT, "chain %d: n = %d exceeds %d rows", k, c.n, NMAX);
+  if (c.p > PMAX) return fail(FB_ERR_LIMIT, "chain %d: p = %d exceeds %d predictors", k, c.p, PMAX);
+  if (c.ntree > MMAX) return fail(FB_ERR_LIMIT, "chain %d: ntree = %d exceeds %d trees", k, c.ntree, MMAX);
+  if (!c.q || !c.numcut || !c.pgtab) return fail(FB_ERR_ARG, "chain %d: q, numcut and pgtab are required", k);
+  if (c.probit ? !c.ybin : !c.y) return fail(FB_ERR_ARG, "chain %d: %s is required", k, c.probit ? "ybin" : "y");
+  int any = 0;
+  for (int v = 0; v < c.p; v++) {
+    if (c.numcut[v] < 0 || c.numcut[v] > 255)
+      return fail(FB_ERR_LIMIT, "chain %d: numcut[%d] = %d is outside 0..255", k, v, c.numcut[v]);
+    any |= c.numcut[v] > 0;
+  }
+  if (!any) return fail(FB_ERR_ARG, "chain %d: no predictor has a cutpoint", k);
+  if (!(c.tau > 0) || !std::isfinite(c.tau)) return fail(FB_ERR_ARG, "chain %d: tau must be positive", k);
+  if (!c.probit) {
+    if (!(c.sigest > 0) || !std::isfinite(c.sigest)) return fail(FB_ERR_ARG, "chain %d: sigest must be positive", k);
+    for (int i = 0; i < c.n; i++)
+      if (!std::isfinite(c.y[i])) return fail(FB_ERR_ARG, "chain %d: y[%d] is not finite", k, i);
+  }
+  if (c.wt)
+    for (int i = 0; i < c.n; i++)
+      if (!(c.wt[i] >= 0) || !std::isfinite(c.wt[i])) return fail(FB_ERR_ARG, "chain %d: wt[%d] is invalid", k, i);
+  return FB_OK;
+}
+
+template <class T>
+fb_status dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T)));
+  return FB_OK;
+}
+
+}  // namespace
+
+struct fb_batch {
+  int device = 0, nchains = 0, nskip = 0, ndpost = 0;
+  int threads = 256, grid = 0, spl = 0, launches = 0;
+  size_t smem = 0;
+  std::vector<DChain> hch;
+  std::vector<int> order;
+  DBufs d{};
+  std::vector<void*> allocs;
+  long long rows = 0, qbytes = 0, leafbytes = 0, ntrees = 0, nsig = 0, nyhat = 0, ntout = 0;
+  cudaStream_t stream = nullptr;
+  ~fb_batch() {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    for (void* p : allocs) cudaFree(p);
+    cudaSetDevice(cur);
+  }
+};
+
+extern "C" {
+
+const char* fb_last_error(void) { return g_err.c_str(); }
+const char* fb_version(void) { return "fastbart_b200 0.1.0 (sm_100a)"; }
+
+fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options* opt, fb_batch** out) {
+  if (!out) return fail(FB_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!chains || nchains < 1 || !opt) return fail(FB_ERR_ARG, "chains, nchains >= 1 and opt are required");
+  if (opt->nskip < 0 || opt->ndpost < 1) return fail(FB_ERR_ARG, "nskip must be >= 0 and ndpost >= 1");
+  if (opt->threads != 0 && (opt->threads < 32 || opt->threads > MAX_THREADS || opt->threads % 32))
+    return fail(FB_ERR_ARG, "threads must be a multiple of 32 in 32..%d", MAX_THREADS);
+  for (int k = 0; k < nchains; k++) {
+    fb_status s = check_chain(chains[k], k);
+    if (s != FB_OK) return s;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  if (opt->device < 0 || opt->device >= ndev) return fail(FB_ERR_ARG, "device %d does not exist", opt->device);
+  CK(cudaSetDevice(opt->device));
+
+  auto* b = new fb_batch();
+  b->device = opt->device; b->nchains = nchains; b->nskip = opt->nskip; b->ndpost = opt->ndpost;
+  const int S = opt->nskip + opt->ndpost;
+  b->hch.resize(nchains);
+  int m_max = 0, n_pad_max = 0;
+  for (int k = 0; k < nchains; k++) {
+    const fb_chain& c = chains[k];
+    DChain& D = b->hch[k];
+    std::memset(&D, 0, sizeof D);
+    D.n = c.n; D.p = c.p; D.m = c.ntree; D.n_pad = (int)round_up(c.n, 16);
+    D.probit = c.probit ? 1 : 0;
+    int s1, s2;
+    auto_shifts(c, &s1, &s2);
+    D.fx_shift = c.fx_shift > 0 ? c.fx_shift : s1;
+    D.rss_shift = c.rss_shift > 0 ? c.rss_shift : s2;
+    int rn = 0;
+    for (int v = 0; v < c.p; v++) { D.numcut[v] = c.numcut[v]; rn += c.numcut[v] >= 1; }
+    D.root_ngv = rn;
+    D.nskip = opt->nskip; D.ndpost = opt->ndpost;
+    D.tau = c.tau; D.lambda = c.lambda; D.nu = c.nu; D.sigest = c.probit ? (c.sigest > 0 ? c.sigest : 1.0) : c.sigest;
+    D.offset = c.offset;
+    for (int d = 0; d < NODES; d++) D.pg[d] = c.pgtab[d];
+    D.seed = c.seed;
+    D.off_row = b->rows; D.off_q = b->qbytes; D.off_leaf = b->leafbytes; D.off_tree = b->ntrees;
+    D.off_sigma = b->nsig; D.off_yhat = b->nyhat; D.off_tout = b->ntout;
+    b->rows += D.n_pad; b->qbytes += (long long)c.p * D.n_pad; b->leafbytes += (long long)c.ntree * D.n_pad;
+    b->ntrees += c.ntree; b->nsig += S; b->nyhat += (long long)opt->ndpost * c.n;
+    b->ntout += (long long)opt->ndpost * c.ntree * NODES;
+    m_max = std::max(m_max, c.ntree); n_pad_max = std::max(n_pad_max, D.n_pad);
+  }
+  // largest chains first (n * ntree), then the queue hands them out as CTAs free up
+  b->order.resize(nchains);
+  for (int k = 0; k < nchains; k++) b->order[k] = k;
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int a, int c) {
+    return (long long)b->hch[a].n * b->hch[a].m > (long long)b->hch[c].n * b->hch[c].m;
+  });
+
+  // launch shape
+  int T = opt->threads;
+  if (T == 0) {
+    const int groups = n_pad_max / 4;
+    T = groups >= 4096 ? 512 : 256;
+  }
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt->device) != cudaSuccess) optin = 232448;
+  int rows_in_smem = 1;
+  size_t smem = sampler_smem_bytes(T, m_max, n_pad_max, 1);
+  if (smem > (size_t)optin) { rows_in_smem = 0; smem = sampler_smem_bytes(T, m_max, n_pad_max, 0); }
+  if (smem > (size_t)optin) { delete b; return fail(FB_ERR_LIMIT, "shared memory %zu exceeds %d", smem, optin); }
+  const int maxgrid = sampler_max_grid(T, smem, opt->device);
+  if (maxgrid <= 0) { delete b; return fail(FB_ERR_CUDA, "sampler kernel cannot be resident with %zu bytes of shared memory", smem); }
+  b->threads = T; b->smem = smem; b->grid = std::min(nchains, maxgrid);
+  b->spl = opt->sweeps_per_launch > 0 ? opt->sweeps_per_launch : S;
+  b->launches = (S + b->spl - 1) / b->spl;
+
+  // device arrays
+  DBufs& d = b->d;
+  auto A = [&](auto** p, size_t cnt) -> fb_status {
+    fb_status s = dalloc(p, cnt);
+    if (s == FB_OK) b->allocs.push_back((void*)*p);
+    return s;
+  };
+  DChain* dch; DState* dst; uint8_t* dq; double* dyin; double* dyw; float* dw; int8_t* dyb; float* drs; uint8_t* dleaf;
+  DTree* dtr; long long* ds0; float* dth; double* dtm; double* dsig; double* dyh; unsigned long long* dto; int* dord;
+  int* dqueue;
+  fb_status s = FB_OK;
+  if ((s = A(&dch, nchains)) || (s = A(&dst, nchains)) || (s = A(&dq, b->qbytes)) || (s = A(&dyin, b->rows)) ||
+      (s = A(&dyw, b->rows)) || (s = A(&dw, b->rows)) || (s = A(&dyb, b->rows)) || (s = A(&drs, b->rows)) ||
+      (s = A(&dleaf, b->leafbytes)) || (s = A(&dtr, b->ntrees)) || (s = A(&ds0, b->ntrees * NODES)) ||
+      (s = A(&dth, b->ntrees * NODES)) || (s = A(&dtm, b->rows)) || (s = A(&dsig, b->nsig)) ||
+      (s = A(&dyh, b->nyhat)) || (s = A(&dto, b->ntout)) || (s = A(&dord, nchains)) || (s = A(&dqueue, 1))) {
+    delete b;
+    return s;
+  }
+  // inputs, padded rows are zero
+  std::vector<uint8_t> hq((size_t)b->qbytes, 0);
+  std::vector<double> hy((size_t)b->rows, 0.0);
+  std::vector<float> hw((size_t)b->rows, 0.0f);
+  std::vector<int8_t> hyb((size_t)b->rows, 0);
+  for (int k = 0; k < nchains; k++) {
+    const fb_chain& c = chains[k];
+    const DChain& D = b->hch[k];
+    for (int v = 0; v < c.p; v++) std::memcpy(&hq[(size_t)D.off_q + (size_t)v * D.n_pad], c.q + (size_t)v * c.n, (size_t)c.n);
+    for (int i = 0; i < c.n; i++) {
+      hy[(size_t)D.off_row + i] = c.probit ? 0.0 : c.y[i];
+      hw[(size_t)D.off_row + i] = c.wt ? (float)c.wt[i] : 1.0f;
+      hyb[(size_t)D.off_row + i] = c.probit ? (int8_t)(c.ybin[i] != 0) : 0;
+    }
+  }
+  std::vector<DState> hst(nchains);
+  std::memset(hst.data(), 0, sizeof(DState) * nchains);
+  CK(cudaMemcpy(dch, b->hch.data(), sizeof(DChain) * nchains, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dst, hst.data(), sizeof(DState) * nchains, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dq, hq.data(), hq.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dyin, hy.data(), hy.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw, hw.data(), hw.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dyb, hyb.data(), hyb.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dord, b->order.data(), sizeof(int) * nchains, cudaMemcpyHostToDevice));
+  d.chains = dch; d.states = dst; d.q = dq; d.yin = dyin; d.ywork = dyw; d.win = dw; d.ybin = dyb; d.rsave = drs;
+  d.leaf = dleaf; d.trees = dtr; d.s0 = ds0; d.th = dth; d.tm = dtm; d.sigma_out = dsig; d.yhat_out = dyh;
+  d.trees_out = dto; d.order = dord; d.queue = dqueue; d.nchains = nchains; d.m_max = m_max;
+  d.n_pad_max = n_pad_max; d.rows_in_smem = rows_in_smem;
+  *out = b;
+  return FB_OK;
+}
+
+fb_status fb_batch_run(fb_batch* b, void* stream) {
+  if (!b) return fail(FB_ERR_ARG, "batch is NULL");
+  CK(cudaSetDevice(b->device));
+  b->stream = reinterpret_cast<cudaStream_t>(stream);
+  const int S = b->nskip + b->ndpost;
+  for (int it0 = 0; it0 < S; it0 += b->spl) {
+    const int it1 = std::min(S, it0 + b->spl);
+    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, stream) != 0)
+      return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  return FB_OK;
+}
+
+fb_status fb_batch_sync(fb_batch* b) {
+  if (!b) return fail(FB_ERR_ARG, "batch is NULL");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  CK(cudaGetLastError());
+  return FB_OK;
+}
+
+fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes) {
+  if (!b) return fail(FB_ERR_ARG, "batch is NULL");
+  if (launches) *launches = b->launches;
+  if (threads) *threads = b->threads;
+  if (grid) *grid = b->grid;
+  if (smem_bytes) *smem_bytes = b->smem;
+  return FB_OK;
+}
+
+fb_status fb_batch_download(fb_batch* b, fb_chain_out* outs) {
+  if (!b || !outs) return fail(FB_ERR_ARG, "batch and outs are required");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  std::vector<DState> st(b->nchains);
+  CK(cudaMemcpy(st.data(), b->d.states, sizeof(DState) * b->nchains, cudaMemcpyDeviceToHost));
+  const int S = b->nskip + b->ndpost;
+  std::vector<double> tm;
+  for (int k = 0; k < b->nchains; k++) {
+    const DChain& D = b->hch[k];
+    fb_chain_out& o = outs[k];
+    if (o.sigma) CK(cudaMemcpy(o.sigma, b->d.sigma_out + D.off_sigma, sizeof(double) * S, cudaMemcpyDeviceToHost));
+    if (o.yhat)
+      CK(cudaMemcpy(o.yhat, b->d.yhat_out + D.off_yhat, sizeof(double) * (size_t)b->ndpost * D.n, cudaMemcpyDeviceToHost));
+    if (o.trees)
+      CK(cudaMemcpy(o.trees, b->d.trees_out + D.off_tout, sizeof(uint64_t) * (size_t)b->ndpost * D.m * NODES,
+                    cudaMemcpyDeviceToHost));
+    if (o.yhat_mean) {
+      CK(cudaMemcpy(o.yhat_mean, b->d.tm + D.off_row, sizeof(double) * D.n, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < D.n; i++) o.yhat_mean[i] = o.yhat_mean[i] / (double)b->ndpost;
+    }
+    o.moves[0] = st[k].births; o.moves[1] = st[k].deaths; o.moves[2] = st[k].caps;
+    o.rtnorm_caps = st[k].rtcaps;
+  }
+  return FB_OK;
+}
+
+void fb_batch_destroy(fb_batch* b) { delete b; }
+
+fb_status fb_fit_batch(const fb_chain* chains, int nchains, const fb_options* opt, fb_chain_out* outs) {
+  fb_batch* b = nullptr;
+  fb_status s = fb_batch_create(chains, nchains, opt, &b);
+  if (s != FB_OK) return s;
+  s = fb_batch_run(b, nullptr);
+  if (s == FB_OK) s = fb_batch_sync(b);
+  if (s == FB_OK) s = fb_batch_download(b, outs);
+  fb_batch_destroy(b);
+  return s;
+}
+
+// ------------------------------------------------------------------------------------------------ tree text
+size_t fb_trees_text(const uint64_t* trees, int ndpost, int ntree, int p, char* buf, size_t cap) {
+  std::string s;
+  s.reserve((size_t)ndpost * ntree * 64);
+  char line[128];
+  int k = std::snprintf(line, sizeof line, "%d %d %d\n", ndpost, ntree, p);
+  s.append(line, (size_t)k);
+  std::vector<std::pair<int, unsigned long long>> stack, order;
+  for (int dr = 0; dr < ndpost; dr++)
+    for (int j = 0; j < ntree; j++) {
+      const uint64_t* T = trees + ((size_t)dr * ntree + j) * NODES;
+      auto L = [&](int x) { return (int)((T[x] >> 16) & 255); };
+      auto R = [&](int x) { return (int)((T[x] >> 24) & 255); };
+      stack.assign(1, {0, 1ull});
+      order.clear();
+      while (!stack.empty() && order.size() <= (size_t)NODES) {   // pre-order: node, left subtree, right subtree
+        auto e = stack.back();
+        stack.pop_back();
+        order.push_back(e);
+        if (L(e.first)) { stack.push_back({R(e.first), 2 * e.second + 1}); stack.push_back({L(e.first), 2 * e.second}); }
+      }
+      k = std::snprintf(line, sizeof line, "%zu\n", order.size());
+      s.append(line, (size_t)k);
+      for (auto& e : order) {
+        const uint64_t w = T[e.first];
+        const bool leaf = L(e.first) == 0;
+        float th;
+        const uint32_t u = (uint32_t)(w >> 32);
+        std::memcpy(&th, &u, 4);
+        k = std::snprintf(line, sizeof line, "%llu %d %d %.10g\n", e.second, leaf ? 0 : (int)(w & 255),
+                          leaf ? 0 : (int)((w >> 8) & 255), leaf ? (double)th : 0.0);
+        s.append(line, (size_t)k);
+      }
+    }
+  if (buf && cap > 0) {
+    const size_t c = std::min(cap - 1, s.size());
+    std::memcpy(buf, s.data(), c);
+    buf[c] = 0;
+  }
+  return s.size();
+}
+
+fb_status fb_varcount(const uint64_t* trees, int ndpost, int ntree, int p, int* varcount) {
+  if (!trees || !varcount) return fail(FB_ERR_ARG, "trees and varcount are required");
+  std::memset(varcount, 0, sizeof(int) * (size_t)ndpost * p);
+  for (int dr = 0; dr < ndpost; dr++)
+    for (int j = 0; j < ntree; j++) {
+      const uint64_t* T = trees + ((size_t)dr * ntree + j) * NODES;
+      int st[2 * NODES + 2], sp = 0, seen = 0;
+      st[sp++] = 0;
+      while (sp > 0 && seen <= NODES) {
+        const int x = st[--sp];
+        seen++;
+        const int l = (int)((T[x] >> 16) & 255), r = (int)((T[x] >> 24) & 255), v = (int)(T[x] & 255);
+        if (l) {
+          if (v < p) varcount[(size_t)dr * p + v] += 1;
+          st[sp++] = r; st[sp++] = l;
+        }
+      }
+    }
+  return FB_OK;
+}
+
+fb_status fb_fbart(const int* q, int n, int p, const double* y, const double* wt, const int* ybin, const int* numcut,
+                   const double* pgtab, int ntree, int nskip, int ndpost, double tau, double lambda, double nu,
+                   double sigest, uint64_t seed, int probit, double offset, double* sigma, double* yhat_train_mean,
+                   double* yhat_train, int* varcount, char* trees_text, size_t text_cap, size_t* text_len, int* moves) {
+  if (!q || n < 1 || p < 1) return fail(FB_ERR_ARG, "q, n >= 1 and p >= 1 are required");
+  std::vector<uint8_t> qv((size_t)n * p);
+  for (size_t k = 0; k < qv.size(); k++) {
+    if (q[k] < 0 || q[k] > 255) return fail(FB_ERR_LIMIT, "code %d at %zu is outside 0..255", q[k], k);
+    qv[k] = (uint8_t)q[k];
+  }
+  fb_chain c;
+  std::memset(&c, 0, sizeof c);
+  c.n = n; c.p = p; c.ntree = ntree; c.q = qv.data(); c.y = y; c.wt = wt; c.ybin = ybin; c.numcut = numcut;
+  c.pgtab = pgtab; c.tau = tau; c.lambda = lambda; c.nu = nu; c.sigest = sigest; c.offset = offset; c.seed = seed;
+  c.probit = probit;
+  fb_options o;
+  std::memset(&o, 0, sizeof o);
+  o.nskip = nskip; o.ndpost = ndpost;
+  std::vector<double> yh((size_t)ndpost * n);
+  std::vector<uint64_t> tr((size_t)ndpost * ntree * NODES);
+  fb_chain_out out;
+  std::memset(&out, 0, sizeof out);
+  out.sigma = sigma; out.yhat_mean = yhat_train_mean; out.yhat = yh.data(); out.trees = tr.data();
+  fb_status s = fb_fit_batch(&c, 1, &o, &out);
+  if (s != FB_OK) return s;
+  if (yhat_train)
+    for (int dr = 0; dr < ndpost; dr++)
+      for (int i = 0; i < n; i++) yhat_train[(size_t)dr + (size_t)i * ndpost] = yh[(size_t)dr * n + i];
+  if (varcount) {
+    std::vector<int> vc((size_t)ndpost * p);
+    fb_varcount(tr.data(), ndpost, ntree, p, vc.data());
+    for (int dr = 0; dr < ndpost; dr++)
+      for (int v = 0; v < p; v++) varcount[(size_t)dr + (size_t)v * ndpost] = vc[(size_t)dr * p + v];
+  }
+  const size_t len = fb_trees_text(tr.data(), ndpost, ntree, p, trees_text, text_cap);
+  if (text_len) *text_len = len;
+  if (moves) { moves[0] = out.moves[0]; moves[1] = out.moves[1]; moves[2] = out.moves[2]; }
+  return FB_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------ evaluator
+struct fb_compiled {
+  int device = 0, ndpost = 0, ntree = 0, p = 0;
+  std::vector<int> var, child, root;
+  std::vector<double> cut, theta;
+  int* dvar = nullptr; int* dchild = nullptr; int* droot = nullptr;
+  double* dcut = nullptr; double* dtheta = nullptr;
+  ~fb_compiled() {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    cudaFree(dvar); cudaFree(dchild); cudaFree(droot); cudaFree(dcut); cudaFree(dtheta);
+    cudaSetDevice(cur);
+  }
+  DForest forest() const {
+    DForest f;
+    f.var = dvar; f.child = dchild; f.cut = dcut; f.theta = dtheta; f.root = droot;
+    f.ntree = ntree; f.ndpost = ndpost; f.p = p; f.nnodes = (int)var.size();
+    return f;
+  }
+};
+
+namespace {
+
+struct Scanner {
+  const char* s;
+  const char* end;
+  bool skip() { while (s < end && (*s == ' ' || *s == '\n' || *s == '\r' || *s == '\t')) s++; return s < end; }
+  bool lng(long long* v) {
+    if (!skip()) return false;
+    char* e;
+    *v = std::strtoll(s, &e, 10);
+    if (e == s || e > end) return false;
+    s = e;
+    return true;
+  }
+  bool ull(unsigned long long* v) {
+    if (!skip()) return false;
+    char* e;
+    *v = std::strtoull(s, &e, 10);
+    if (e == s || e > end) return false;
+    s = e;
+    return true;
+  }
+  bool dbl(double* v) {
+    if (!skip()) return false;
+    char* e;
+    *v = std::strtod(s, &e);
+    if (e == s || e > end) return false;
+    s = e;
+    return true;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+fb_status fb_compile_trees(const char* text, size_t len, const double* const* cutpoints, const int* ncut, int ncol,
+                           int device, fb_compiled** out) {
+  if (!out) return fail(FB_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!text || !cutpoints || !ncut) return fail(FB_ERR_ARG, "text, cutpoints and ncut are required");
+  std::string owned(text, len);   // NUL-terminated copy so strtod cannot read past the end
+  Scanner sc{owned.c_str(), owned.c_str() + owned.size()};
+  long long nd, m, p;
+  if (!sc.lng(&nd) || !sc.lng(&m) || !sc.lng(&p) || nd < 1 || m < 1 || p < 0)
+    return fail(FB_ERR_PARSE, "tree text header must be \"ndpost ntree p\"");
+  auto* ct = new fb_compiled();
+  ct->device = device; ct->ndpost = (int)nd; ct->ntree = (int)m; ct->p = (int)p;
+  ct->root.resize((size_t)(nd * m));
+  std::vector<unsigned long long> nid;
+  std::vector<int> v, c;
+  std::vector<double> th;
+  std::unordered_map<unsigned long long, int> pos;
+  std::vector<int> qk, slot;
+  for (long long t = 0; t < nd * m; t++) {
+    long long nn;
+    if (!sc.lng(&nn) || nn < 1) { delete ct; return fail(FB_ERR_PARSE, "tree %lld: bad node count", t); }
+    nid.resize(nn); v.resize(nn); c.resize(nn); th.resize(nn);
+    pos.clear();
+    for (long long k = 0; k < nn; k++) {
+      long long vv, cc;
+      if (!sc.ull(&nid[k]) || !sc.lng(&vv) || !sc.lng(&cc) || !sc.dbl(&th[k])) {
+        delete ct;
+        return fail(FB_ERR_PARSE, "tree %lld: bad node line %lld", t, k);
+      }
+      v[k] = (int)vv; c[k] = (int)cc;
+      pos[nid[k]] = (int)k;
+    }
+    // breadth-first from the root (id 1), each node's two children placed next to each other (predict.cpp:87-101)
+    auto it1 = pos.find(1ull);
+    if (it1 == pos.end()) { delete ct; return fail(FB_ERR_PARSE, "tree %lld has no root (id 1)", t); }
+    qk.assign(1, it1->second);
+    slot.assign(1, (int)ct->var.size());
+    ct->root[(size_t)t] = slot[0];
+    ct->var.push_back(0); ct->child.push_back(-1); ct->cut.push_back(0.0); ct->theta.push_back(0.0);
+    for (size_t h = 0; h < qk.size(); h++) {
+      const int k = qk[h], me = slot[h];
+      ct->theta[me] = th[k];
+      auto L = pos.find(2 * nid[k]);
+      if (L != pos.end()) {
+        auto R = pos.find(2 * nid[k] + 1);
+        if (R == pos.end()) { delete ct; return fail(FB_ERR_PARSE, "tree %lld: node %llu has one child", t, nid[k]); }
+        if (v[k] < 0 || v[k] >= ncol || c[k] < 0 || c[k] >= ncut[v[k]]) {
+          delete ct;
+          return fail(FB_ERR_PARSE, "tree %lld: split (v %d, c %d) is not a cutpoint", t, v[k], c[k]);
+        }
+        const int ch = (int)ct->var.size();
+        ct->var[me] = v[k]; ct->cut[me] = cutpoints[v[k]][c[k]]; ct->child[me] = ch;
+        for (int z = 0; z < 2; z++) { ct->var.push_back(0); ct->child.push_back(-1); ct->cut.push_back(0.0); ct->theta.push_back(0.0); }
+        qk.push_back(L->second); slot.push_back(ch);
+        qk.push_back(R->second); slot.push_back(ch + 1);
+      }
+    }
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete ct; return fail(FB_ERR_CUDA, "no CUDA device is available"); }
+  if (cudaSetDevice(device) != cudaSuccess) { delete ct; return fail(FB_ERR_CUDA, "cannot use device %d", device); }
+  const size_t N = ct->var.size();
+  if (cudaMalloc(&ct->dvar, N * 4) != cudaSuccess || cudaMalloc(&ct->dchild, N * 4) != cudaSuccess ||
+      cudaMalloc(&ct->dcut, N * 8) != cudaSuccess || cudaMalloc(&ct->dtheta, N * 8) != cudaSuccess ||
+      cudaMalloc(&ct->droot, ct->root.size() * 4) != cudaSuccess ||
+      cudaMemcpy(ct->dvar, ct->var.data(), N * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(ct->dchild, ct->child.data(), N * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(ct->dcut, ct->cut.data(), N * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(ct->dtheta, ct->theta.data(), N * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(ct->droot, ct->root.data(), ct->root.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+    delete ct;
+    return fail(FB_ERR_CUDA, "cannot upload the compiled trees");
+  }
+  *out = ct;
+  return FB_OK;
+}
+
+fb_status fb_compiled_info(const fb_compiled* ct, int* ndpost, int* ntree, int* p, int* nnodes) {
+  if (!ct) return fail(FB_ERR_ARG, "compiled trees are NULL");
+  if (ndpost) *ndpost = ct->ndpost;
+  if (ntree) *ntree = ct->ntree;
+  if (p) *p = ct->p;
+  if (nnodes) *nnodes = (int)ct->var.size();
+  return FB_OK;
+}
+
+fb_status fb_compiled_arrays(const fb_compiled* ct, int* var, int* child, double* cut, double* theta, int* root) {
+  if (!ct) return fail(FB_ERR_ARG, "compiled trees are NULL");
+  const size_t N = ct->var.size();
+  if (var) std::memcpy(var, ct->var.data(), N * 4);
+  if (child) std::memcpy(child, ct->child.data(), N * 4);
+  if (cut) std::memcpy(cut, ct->cut.data(), N * 8);
+  if (theta) std::memcpy(theta, ct->theta.data(), N * 8);
+  if (root) std::memcpy(root, ct->root.data(), ct->root.size() * 4);
+  return FB_OK;
+}
+
+void fb_compiled_free(fb_compiled* ct) { delete ct; }
+
+fb_status fb_predict_draws_device(const fb_compiled* ct, const double* x_dev, int ncol, int n, int ld, int draw0,
+                                  int ndraws, double mu, double* out_dev, int ldo, void* stream) {
+  if (!ct) return fail(FB_ERR_ARG, "compiled trees are NULL");
+  if (ncol != ct->p) return fail(FB_ERR_SHAPE, "newdata has %d columns, the trees use %d", ncol, ct->p);
+  if (draw0 < 1 || ndraws < 0 || draw0 + ndraws - 1 > ct->ndpost)
+    return fail(FB_ERR_RANGE, "draw %d out of range 1..%d", draw0 + (draw0 < 1 ? 0 : ndraws - 1), ct->ndpost);
+  if (n < 0 || ld < n || ldo < n) return fail(FB_ERR_ARG, "need 0 <= n <= ld and n <= ldo");
+  if (n == 0 || ndraws == 0) return FB_OK;
+  if ((!x_dev && ncol > 0) || !out_dev) return fail(FB_ERR_ARG, "x_dev and out_dev are required");
+  CK(cudaSetDevice(ct->device));
+  if (launch_predict(ct->forest(), x_dev, n, ld, draw0 - 1, ndraws, mu, out_dev, ldo, stream) != 0)
+    return fail(FB_ERR_CUDA, "predict launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return FB_OK;
+}
+
+fb_status fb_predict_draw(const fb_compiled* ct, const double* const* cols, int ncol, int n, int draw, double mu,
+                          double* out) {
+  if (!ct) return fail(FB_ERR_ARG, "compiled trees are NULL");
+  if (ncol != ct->p) return fail(FB_ERR_SHAPE, "newdata has %d columns, the trees use %d", ncol, ct->p);
+  if (draw < 1 || draw > ct->ndpost) return fail(FB_ERR_RANGE, "draw %d out of range 1..%d", draw, ct->ndpost);
+  if (n <= 0) return FB_OK;
+  if (!cols || !out) return fail(FB_ERR_ARG, "cols and out are required");
+  CK(cudaSetDevice(ct->device));
+  double* dx = nullptr;
+  double* dout = nullptr;
+  CK(cudaMalloc(&dx, sizeof(double) * (size_t)n * std::max(ncol, 1)));
+  if (cudaMalloc(&dout, sizeof(double) * (size_t)n) != cudaSuccess) { cudaFree(dx); return fail(FB_ERR_CUDA, "out of device memory"); }
+  fb_status s = FB_OK;
+  for (int v = 0; v < ncol && s == FB_OK; v++)
+    if (cudaMemcpy(dx + (size_t)v * n, cols[v], sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+      s = fail(FB_ERR_CUDA, "copy of column %d failed", v);
+  if (s == FB_OK && launch_predict(ct->forest(), dx, n, n, draw - 1, 1, mu, dout, n, nullptr) != 0)
+    s = fail(FB_ERR_CUDA, "predict launch failed");
+  if (s == FB_OK && cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    s = fail(FB_ERR_CUDA, "copy of the result failed: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaFree(dx);
+  cudaFree(dout);
+  return s;
+}
+
+// ------------------------------------------------------------------------------------------------ diagnostics
+fb_status fb_debug_tree_pass(const fb_pass_state* s, int64_t* out) {
+  if (!s || !out || !s->r || !s->w || !s->tho || !s->thn || !s->thc) return fail(FB_ERR_ARG, "missing argument");
+  if (s->n < 1 || s->n > NMAX) return fail(FB_ERR_LIMIT, "n must be in 1..%d", NMAX);
+  const int T = s->threads ? s->threads : 256;
+  if (T < 32 || T > MAX_THREADS || T % 32) return fail(FB_ERR_ARG, "threads must be a multiple of 32 in 32..%d", MAX_THREADS);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  const int n = s->n, n_pad = (int)round_up(n, 16);
+  std::vector<uint8_t> lp(n_pad, 0), lc(n_pad, 0), qp(n_pad, 0), qc(n_pad, 0);
+  std::vector<float> r(n_pad, 0.0f), w(n_pad, 0.0f);
+  if (s->leaf_prev) std::memcpy(lp.data(), s->leaf_prev, n);
+  if (s->leaf_cur) std::memcpy(lc.data(), s->leaf_cur, n);
+  if (s->qprev) std::memcpy(qp.data(), s->qprev, n);
+  if (s->qcur) std::memcpy(qc.data(), s->qcur, n);
+  std::memcpy(r.data(), s->r, sizeof(float) * n);
+  std::memcpy(w.data(), s->w, sizeof(float) * n);
+  uint8_t* dbytes = nullptr;
+  float* dfl = nullptr;
+  long long* dout = nullptr;
+  CK(cudaMalloc(&dbytes, (size_t)n_pad * 4));
+  CK(cudaMalloc(&dfl, sizeof(float) * ((size_t)n_pad * 2 + 3 * NODES)));
+  CK(cudaMalloc(&dout, sizeof(long long) * 70));
+  CK(cudaMemcpy(dbytes, lp.data(), n_pad, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dbytes + n_pad, lc.data(), n_pad, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dbytes + 2 * n_pad, qp.data(), n_pad, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dbytes + 3 * n_pad, qc.data(), n_pad, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfl, r.data(), sizeof(float) * n_pad, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfl + n_pad, w.data(), sizeof(float) * n_pad, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfl + 2 * n_pad, s->tho, sizeof(float) * NODES, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfl + 2 * n_pad + NODES, s->thn, sizeof(float) * NODES, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dfl + 2 * n_pad + 2 * NODES, s->thc, sizeof(float) * NODES, cudaMemcpyHostToDevice));
+  DPassArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.n = n; a.n_pad = n_pad; a.apply = s->apply; a.stats = s->stats;
+  a.pmode = s->pmode; a.pnx = s->pnx; a.pc = s->pc; a.pL = s->pL; a.pR = s->pR; a.pl = s->pl; a.pr = s->pr;
+  a.cmode = s->cmode; a.cnx = s->cnx; a.cc = s->cc; a.fx_shift = s->fx_shift; a.leafmask = s->leafmask;
+  a.leaf_prev = dbytes; a.leaf_cur = dbytes + n_pad; a.qprev = dbytes + 2 * n_pad; a.qcur = dbytes + 3 * n_pad;
+  a.r = dfl; a.w = dfl + n_pad; a.tho = dfl + 2 * n_pad; a.thn = dfl + 2 * n_pad + NODES;
+  a.thc = dfl + 2 * n_pad + 2 * NODES; a.out = dout;
+  fb_status st = FB_OK;
+  if (launch_debug_pass(a, T, nullptr) != 0) st = fail(FB_ERR_CUDA, "debug pass launch failed");
+  if (st == FB_OK && cudaDeviceSynchronize() != cudaSuccess) st = fail(FB_ERR_CUDA, "debug pass failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if (st == FB_OK) {
+    if (cudaMemcpy(out, dout, sizeof(long long) * 70, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(s->r, dfl, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        (s->leaf_prev && cudaMemcpy(s->leaf_prev, dbytes, n, cudaMemcpyDeviceToHost) != cudaSuccess))
+      st = fail(FB_ERR_CUDA, "copy back failed");
+  }
+  cudaFree(dbytes); cudaFree(dfl); cudaFree(dout);
+  return st;
+}
+
+}  // extern "C"

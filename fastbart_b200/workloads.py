@@ -1,0 +1,136 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+The reference's own datasets (titer models, person-week hazard data) come from an external pipeline and are not
+shipped, so these generators stand in for them with the same shapes, sizes and value distributions:
+
+  fwbart_friedman   n 4,096, p 16, x ~ U(0,1), y = 10 sin(pi x1 x2) + 20 (x3 - .5)^2 + 10 x4 + 5 x5 + N(0,1),
+                    w ~ Gamma(4, rate 4), numcut 100, ntree 200, nskip 1000, ndpost 100
+  fpbart_hazard     n 24,576 person-weeks, p 3 (week 1..52, Bernoulli(.5), N(0,1)),
+                    y ~ Bernoulli(Phi(-1.8 + .015 x1 + .5 x2 + .3 x3)), ntree 50, nskip 1000, ndpost 100
+  titer_bootstrap   96 chains: 6 shapes (n, p) in {(3091,15), (3400,16), (3760,17), (4102,18), (4388,19), (4573,19)}
+                    x 16 multinomial bootstrap resamples; half U(0,1) and half integer 0..9 columns;
+                    y = linear term on 4 columns + sin(pi xa xb) + N(0, .5^2); w ~ Gamma(4, 4); ntree 200
+  friedman_large    n 65,536, p 32, numcut 255, Friedman-5 on x1..x5 + N(0,1), 16 chains
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy import stats
+
+from . import prep
+
+TITER_SHAPES = [(3091, 15), (3400, 16), (3760, 17), (4102, 18), (4388, 19), (4573, 19)]
+
+
+def friedman(x: np.ndarray) -> np.ndarray:
+    """Friedman's function of the first five columns (columns beyond p count as 0.5)."""
+    c = [x[:, k] if k < x.shape[1] else np.full(x.shape[0], 0.5) for k in range(5)]
+    return 10 * np.sin(np.pi * c[0] * c[1]) + 20 * (c[2] - 0.5) ** 2 + 10 * c[3] + 5 * c[4]
+
+
+def fwbart_chain(x, y, w=None, *, ntree=200, nskip=1000, ndpost=100, numcut=100, k=2.0, power=2.0, base=0.95,
+                 sigdf=3.0, sigquant=0.9, seed=1, fmean=None) -> dict:
+    """Prepares one fwbart chain exactly as the R wrapper does (R/fwbart.R:8-27); returns the chain dict."""
+    d = prep.model_matrix(x, numcut)
+    y = np.asarray(y, dtype=np.float64)
+    n = y.size
+    w = np.ones(n) if w is None else np.asarray(w, dtype=np.float64)
+    fm = float(np.mean(y)) if fmean is None else float(fmean)
+    yc = y - fm
+    nu = float(sigdf)
+    sig = prep.sigest_lm(d.X, yc)
+    lam = sig * sig * stats.chi2.ppf(1.0 - sigquant, nu) / nu
+    tau = (yc.max() - yc.min()) / (2 * k * np.sqrt(ntree))
+    wt = 1.0 / (w * w)
+    s, srss = prep.fx_shifts(n, wt, float(np.max(np.abs(yc))))
+    return dict(q=d.q, y=yc, wt=wt, numcut=d.numcut, pgtab=prep.pg_table(base, power), tau=float(tau),
+                **{"lambda": float(lam)}, nu=nu, sigest=float(sig), offset=0.0, seed=int(seed), probit=0,
+                ntree=int(ntree), nskip=int(nskip), ndpost=int(ndpost), fx_shift=s, rss_shift=srss,
+                fmean=fm, xi=d.xi, rm_const=d.rm_const)
+
+
+def fpbart_chain(x, y, *, ntree=50, nskip=1000, ndpost=100, numcut=100, k=2.0, power=2.0, base=0.95,
+                 binary_offset=None, seed=1) -> dict:
+    """Prepares one fpbart chain as R/fpbart.R:7-24 does."""
+    d = prep.model_matrix(x, numcut)
+    y = np.asarray(y).astype(np.int32)
+    n = y.size
+    off = float(stats.norm.ppf(np.mean(y))) if binary_offset is None else float(binary_offset)
+    tau = 3.0 / (k * np.sqrt(ntree))
+    s, srss = prep.fx_shifts(n, np.ones(n), 10.0)
+    return dict(q=d.q, y=np.zeros(n), wt=np.ones(n), ybin=y, numcut=d.numcut, pgtab=prep.pg_table(base, power),
+                tau=float(tau), **{"lambda": 1.0}, nu=3.0, sigest=1.0, offset=off, seed=int(seed), probit=1,
+                ntree=int(ntree), nskip=int(nskip), ndpost=int(ndpost), fx_shift=s, rss_shift=srss,
+                binaryOffset=off, xi=d.xi, rm_const=d.rm_const)
+
+
+def friedman_data(n=4096, p=16, seed=0, weights=True):
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, p))
+    y = friedman(x) + rng.standard_normal(n)
+    w = rng.gamma(4.0, 1.0 / 4.0, n) if weights else np.ones(n)
+    return x, y, w
+
+
+def fwbart_friedman(n=4096, p=16, seed=0, **kw) -> dict:
+    x, y, w = friedman_data(n, p, seed)
+    kw.setdefault("seed", seed + 1)
+    return fwbart_chain(x, y, w, **kw)
+
+
+def hazard_data(n=24576, seed=0):
+    rng = np.random.default_rng(seed)
+    x1 = rng.integers(1, 53, n).astype(np.float64)
+    x2 = rng.integers(0, 2, n).astype(np.float64)
+    x3 = rng.standard_normal(n)
+    eta = -1.8 + 0.015 * x1 + 0.5 * x2 + 0.3 * x3
+    y = (rng.random(n) < stats.norm.cdf(eta)).astype(np.int32)
+    return np.column_stack([x1, x2, x3]), y
+
+
+def fpbart_hazard(n=24576, seed=0, **kw) -> dict:
+    x, y = hazard_data(n, seed)
+    kw.setdefault("seed", seed + 1)
+    return fpbart_chain(x, y, **kw)
+
+
+def titer_model(shape_idx: int, seed=0):
+    """Base data of one titer-like model: half U(0,1), half integer 0..9 columns."""
+    n, p = TITER_SHAPES[shape_idx]
+    rng = np.random.default_rng(1000 + 17 * shape_idx + seed)
+    x = np.empty((n, p))
+    half = p // 2
+    x[:, :half] = rng.random((n, half))
+    x[:, half:] = rng.integers(0, 10, (n, p - half))
+    cols = rng.choice(p, 6, replace=False)
+    beta = rng.normal(0, 1, 4)
+    xs = x / np.maximum(x.max(axis=0), 1e-12)
+    y = xs[:, cols[:4]] @ beta + np.sin(np.pi * xs[:, cols[4]] * xs[:, cols[5]]) + rng.normal(0, 0.5, n)
+    w = rng.gamma(4.0, 1.0 / 4.0, n)
+    return x, y, w
+
+
+def titer_bootstrap(reps=16, shapes=range(6), seed=0, **kw) -> list:
+    """The 96-chain batched workload: every shape x `reps` multinomial bootstrap resamples of its rows."""
+    chains = []
+    for si in shapes:
+        x, y, w = titer_model(si, seed)
+        n = y.size
+        for r in range(reps):
+            rng = np.random.default_rng(50_000 + 1000 * si + r + seed)
+            idx = rng.integers(0, n, n)
+            kw2 = dict(kw)
+            kw2.setdefault("seed", 12345 + len(chains))
+            chains.append(fwbart_chain(x[idx], y[idx], w[idx], **kw2))
+    return chains
+
+
+def friedman_large(nchains=16, n=65536, p=32, seed=0, **kw) -> list:
+    x, y, w = friedman_data(n, p, seed, weights=False)
+    out = []
+    for c in range(nchains):
+        kw2 = dict(kw)
+        kw2.setdefault("seed", 777 + c)
+        kw2.setdefault("numcut", 255)
+        out.append(fwbart_chain(x, y, None, **kw2))
+    return out

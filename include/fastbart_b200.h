@@ -1,0 +1,158 @@
+/*
+ * fastbart_b200.h -- C ABI of the B200 implementation of fastbart's hot path.
+ *
+ * One shared library (libfastbart_b200.so) replaces the native side of the reference R package:
+ *   - the sampler call that src/glue.cpp:26-27 makes into bart_fit_cpu (src/bart_kernel.h:63-66) and the output
+ *     assembly around it (src/glue.cpp:29-61);
+ *   - compile_trees_cpp / predict_draw_cpp (src/predict.cpp:11-73);
+ *   - the batch GPU prototype's fit list (gpu/bart_gpu.cu:326-404) via fb_fit_batch.
+ *
+ * Conventions: plain C types; every buffer is owned by the caller; sizes are element counts.  Functions return an
+ * fb_status; on failure fb_last_error() returns a message for the calling thread.  Calls are thread-safe as long as
+ * different threads use different fb_batch / fb_compiled objects.  Results are bit-for-bit deterministic for a given
+ * input and seed.  The product never falls back to a CPU path: without a usable CUDA device every compute entry point
+ * returns FB_ERR_CUDA.
+ */
+#ifndef FASTBART_B200_H
+#define FASTBART_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef enum fb_status {
+  FB_OK = 0,
+  FB_ERR_ARG = 1,     /* null pointer or invalid argument */
+  FB_ERR_LIMIT = 2,   /* n > 65536, p > 32, ntree > 200, numcut > 255, ... (R/fwbart.R:11-17 falls back to BART) */
+  FB_ERR_CUDA = 3,    /* no device, out of device memory, launch or runtime error */
+  FB_ERR_PARSE = 4,   /* malformed tree text */
+  FB_ERR_SHAPE = 5,   /* predict: newdata has the wrong number of columns (src/predict.cpp:51) */
+  FB_ERR_RANGE = 6    /* predict: draw out of range (src/predict.cpp:52) */
+} fb_status;
+
+#define FB_NODES 64   /* node slots per tree in the packed tree format (src/bart_kernel.h:23) */
+
+/* Message describing the last failure on the calling thread ("" if none). */
+const char* fb_last_error(void);
+/* Library version string. */
+const char* fb_version(void);
+
+/* ------------------------------------------------------------------------------------------------ sampler */
+
+/* One chain (fit).  Field meanings follow fbart_cpp's arguments (src/glue.cpp:10-12, R/fwbart.R:31-32,
+ * R/fpbart.R:24-26). */
+typedef struct fb_chain {
+  int n, p, ntree;          /* rows (<= 65536), predictors (<= 32), trees (<= 200) */
+  const uint8_t* q;         /* [p][n] cutpoint codes: x < cutpoints[v][c]  <=>  q <= c */
+  const double* y;          /* [n] centred y (fwbart); ignored when probit */
+  const double* wt;         /* [n] 1/w^2 (fwbart); NULL means all ones */
+  const int* ybin;          /* [n] 0/1 outcomes (fpbart); NULL unless probit */
+  const int* numcut;        /* [p] number of cutpoints of each predictor (1..255) */
+  const double* pgtab;      /* [64] base / (1 + depth)^power */
+  double tau, lambda, nu, sigest, offset;  /* offset = binaryOffset (fpbart) */
+  uint64_t seed;            /* Philox key of the chain */
+  int probit;               /* 0: fwbart (weighted continuous), 1: fpbart (probit; sigma fixed at 1) */
+  int fx_shift, rss_shift;  /* fixed-point scales 2^fx_shift / 2^rss_shift of the exact sums; 0 = automatic */
+} fb_chain;
+
+typedef struct fb_options {
+  int nskip, ndpost;        /* burn-in and kept sweeps (shared by all chains of a batch) */
+  int threads;              /* threads per CTA; 0 = automatic */
+  int sweeps_per_launch;    /* 0 = the whole MCMC in one launch; k > 0 = launches of k sweeps */
+  int device;               /* CUDA device ordinal */
+} fb_options;
+
+/* Caller-owned host outputs of one chain; a NULL pointer skips that copy. */
+typedef struct fb_chain_out {
+  double* sigma;            /* [nskip + ndpost] every sigma draw (sigest for probit) */
+  double* yhat_mean;        /* [n] posterior mean of f over kept draws, without fmean / binaryOffset */
+  double* yhat;             /* [ndpost][n] f of every kept draw: FP64 sum of leaf values in tree order */
+  uint64_t* trees;          /* [ndpost][ntree][64] packed nodes (src/bart_kernel.cpp:559-571 format) */
+  int moves[3];             /* births, deaths, node-cap hits (src/glue.cpp:61 "moves") */
+  int rtnorm_caps;          /* truncated-normal draws that reached their iteration cap (probit) */
+} fb_chain_out;
+
+/* Runs every chain's full MCMC (nskip + ndpost sweeps) in one batch on the device and copies the outputs back.
+ * Replaces the fit call of src/glue.cpp:26-27 (bart_fit_cpu, src/bart_kernel.h:63-66) and the batch runner of
+ * gpu/bart_gpu.cu:366-390. */
+fb_status fb_fit_batch(const fb_chain* chains, int nchains, const fb_options* opt, fb_chain_out* outs);
+
+/* Staged use of the same sampler: inputs are uploaded once, fb_batch_run() repeats the full MCMC from the initial
+ * state on the device (results are identical every run), fb_batch_download() copies the outputs of the last run. */
+typedef struct fb_batch fb_batch;
+fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options* opt, fb_batch** out);
+fb_status fb_batch_run(fb_batch* b, void* cuda_stream);        /* enqueues on cuda_stream (NULL: default stream) */
+fb_status fb_batch_sync(fb_batch* b);
+fb_status fb_batch_download(fb_batch* b, fb_chain_out* outs);
+/* number of sampler kernel launches per fb_batch_run, and the dynamic shared memory / threads / grid of each */
+fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes);
+void fb_batch_destroy(fb_batch* b);
+
+/* fbart_cpp (src/glue.cpp:10-62) with R's memory layouts: q is the n x p integer code matrix (column-major), yhat is
+ * ndpost x n and varcount ndpost x p (column-major, as Rcpp::NumericMatrix / IntegerMatrix).  trees_text receives
+ * BART's tree text when non-NULL; *text_len always receives its length (call once with trees_text = NULL to size the
+ * buffer, which must hold text_len + 1 bytes).  Outputs may be NULL.  seed is the chain's Philox key (the R
+ * generator of use_r_rng = 1 is not available on the device). */
+fb_status fb_fbart(const int* q, int n, int p, const double* y, const double* wt, const int* ybin, const int* numcut,
+                   const double* pgtab, int ntree, int nskip, int ndpost, double tau, double lambda, double nu,
+                   double sigest, uint64_t seed, int probit, double offset, double* sigma, double* yhat_train_mean,
+                   double* yhat_train, int* varcount, char* trees_text, size_t text_cap, size_t* text_len, int* moves);
+
+/* BART's tree text of packed draws (src/glue.cpp:32-50): header "ndpost ntree p", then per draw and tree the node
+ * count and pre-order "id v c theta" lines (root id 1, children 2id / 2id+1, 10 significant digits).  Writes at most
+ * cap bytes (NUL-terminated when cap > 0) and returns the full length. */
+size_t fb_trees_text(const uint64_t* trees, int ndpost, int ntree, int p, char* buf, size_t cap);
+/* varcount[dr][v] = number of internal nodes splitting on v in draw dr (src/glue.cpp:49). */
+fb_status fb_varcount(const uint64_t* trees, int ndpost, int ntree, int p, int* varcount);
+
+/* ------------------------------------------------------------------------------------------------ evaluator */
+
+/* compile_trees_cpp (src/predict.cpp:12-45): parses tree text once into flat breadth-first node arrays (children
+ * adjacent, cut = cutpoints[v][c]) and uploads them to the device.  cutpoints[v] has ncut[v] values. */
+typedef struct fb_compiled fb_compiled;
+fb_status fb_compile_trees(const char* text, size_t len, const double* const* cutpoints, const int* ncut, int ncol,
+                           int device, fb_compiled** out);
+fb_status fb_compiled_info(const fb_compiled* ct, int* ndpost, int* ntree, int* p, int* nnodes);
+/* Copies the host arrays of compile_trees_cpp's result list (var, child, cut, theta [nnodes]; root [ndpost*ntree]). */
+fb_status fb_compiled_arrays(const fb_compiled* ct, int* var, int* child, double* cut, double* theta, int* root);
+void fb_compiled_free(fb_compiled* ct);
+
+/* predict_draw_cpp (src/predict.cpp:49-73): f[i] = sum over trees, in tree order, of the leaf value reached by row i
+ * (left when x < cut), plus mu; draw is 1-based.  cols[v] are host columns of n doubles.  Bit-identical to the
+ * reference loop. */
+fb_status fb_predict_draw(const fb_compiled* ct, const double* const* cols, int ncol, int n, int draw, double mu,
+                          double* out);
+/* Bulk form on device memory: x_dev is [ncol][ld] (column v at x_dev + v*ld), out_dev receives ndraws rows of n
+ * values at out_dev + d*ldo, for draws draw0 .. draw0+ndraws-1 (1-based).  Enqueued on cuda_stream. */
+fb_status fb_predict_draws_device(const fb_compiled* ct, const double* x_dev, int ncol, int n, int ld, int draw0,
+                                  int ndraws, double mu, double* out_dev, int ldo, void* cuda_stream);
+
+/* ------------------------------------------------------------------------------------------------ diagnostics */
+
+/* One fused per-tree data pass on explicit state (the pass of src/bart_kernel.cpp:131-213), run by the same device
+ * code as the sampler.  Host buffers of n rows: leaf_prev and r are updated in place; out receives 70 int64 values:
+ * S1 (sum of fx(w*R)) per leaf slot [64], the birth split sums sL0 sL1 sR0 sR1, and the counts nL nR. */
+typedef struct fb_pass_state {
+  int n, apply, stats, fx_shift, threads;
+  int pmode, pnx, pc, pL, pR, pl, pr;   /* previous tree's move */
+  int cmode, cnx, cc;                   /* current tree's proposal */
+  uint64_t leafmask;                    /* leaf slots of the current tree */
+  uint8_t* leaf_prev; const uint8_t* leaf_cur; const uint8_t* qprev; const uint8_t* qcur;
+  float* r; const float* w;
+  const float* tho; const float* thn; const float* thc;   /* [64] each */
+} fb_pass_state;
+fb_status fb_debug_tree_pass(const fb_pass_state* s, int64_t* out);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,105 @@
+/*
+ * fb_oracle.h -- CPU oracle for fastbart_b200.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker: tests/, __graft_entry__.smoke() and the cpu_baseline leg
+ * of bench.py load it to compute the expected answer on the CPU.  The product (fastbart_b200/, libfastbart_b200.so)
+ * never links, loads or calls it.
+ *
+ * It restates, in plain C, the reference's algorithms for the hot path:
+ *
+ *   - the sampler of src/bart_kernel.cpp:304-580 (bart_fit_cpu), in two arithmetic modes:
+ *       ORC_MODE_REF  the reference's own arithmetic: xoshiro128** RNG (bart_kernel.cpp:53-83), FP64 row sums in
+ *                     KL = 16 lanes summed lane by lane (bart_kernel.cpp:131-213).  Bit-exact to bart_fit_cpu built
+ *                     with -DFAST_CPU and run with bart_set_rng(NULL, ...) (the internal generator), which pins this
+ *                     restatement to the reference itself (oracle/_ref).
+ *       ORC_MODE_DEV  the arithmetic of the B200 kernels: counter-based Philox4x32-10 RNG, FP32 row residuals, exact
+ *                     int64 fixed-point sums, FP64 control math with this project's own log/exp (atanh-series log,
+ *                     Taylor exp with Cody-Waite reduction), polar-method normals, FP64 tree-order refresh of
+ *                     y - sum(trees) once per sweep.  The CUDA sampler must reproduce this mode bit for bit.
+ *   - the per-tree fused data pass (bart_kernel.cpp:131-213 semantics, gpu/bart_batch.cu:184-227 fixed-point
+ *     semantics) on explicit state, in DEV arithmetic (orc_pass_dev);
+ *   - compile_trees_cpp / predict_draw_cpp of src/predict.cpp:11-73 without Rcpp;
+ *   - the BART tree-text writer, varcount and yhat.train re-sum of src/glue.cpp:29-57.
+ */
+#ifndef FB_ORACLE_H
+#define FB_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#define ORC_NODES 64      /* node slots per tree (bart_kernel.h:23) */
+#define ORC_MAXDEPTH 24   /* bart_kernel.h:33 */
+#define ORC_PMAX 32       /* bart_kernel.h:20 */
+#define ORC_MMAX 200      /* bart_kernel.h:21 */
+#define ORC_KL 16         /* lanes of the reference CPU build (bart_kernel.h:26) */
+
+enum { ORC_MODE_REF = 0, ORC_MODE_DEV = 1 };
+
+/* Philox counter tags (word 3 of the counter) used by the DEV arithmetic. */
+enum { ORC_TAG_PROP = 1, ORC_TAG_MH = 2, ORC_TAG_MU = 3, ORC_TAG_SIG_N = 4, ORC_TAG_SIG_U = 5, ORC_TAG_Z_N = 6,
+       ORC_TAG_Z_E = 7 };
+#define ORC_INIT_SWEEP 0xFFFFFFFFu
+
+typedef struct {
+  int n, p, m, nskip, ndpost;
+  const uint8_t* q;       /* [p][n] cutpoint codes: x < xi[v][c]  <=>  q <= c */
+  const double* y;        /* [n] centred y (wbart); unused when probit */
+  const double* wt;       /* [n] 1/w^2 (wbart); NULL means all ones */
+  const int* ybin;        /* [n] 0/1 outcomes (probit), else NULL */
+  const int* numcut;      /* [p] */
+  const double* pgtab;    /* [64] base/(1+d)^power */
+  double tau, lambda, nu, sigest, offset;
+  uint64_t seed;          /* REF: low 32 bits are bart_fit_cpu's seed; DEV: the Philox key */
+  int probit;
+  int fx_shift;           /* DEV: w and w*r are summed as llrint(x * 2^fx_shift) */
+  int rss_shift;          /* DEV: w*e^2 is summed as llrint(x * 2^rss_shift) */
+} orc_chain;
+
+typedef struct {
+  double* sigma;          /* [nskip+ndpost] (REF: float-rounded like sigma_out) */
+  double* fmean;          /* [n] posterior mean of f (REF: float TM/ndpost like trmean_out) */
+  double* yhat;           /* [ndpost][n] FP64 tree-order sum of each kept draw (glue.cpp:52-56); may be NULL */
+  uint64_t* trees;        /* [ndpost][m][64] packed nodes (bart_kernel.cpp:559-571); may be NULL */
+  int moves[3];           /* births, deaths, node-cap hits */
+  int rtnorm_caps;        /* DEV: truncated-normal draws that hit their iteration cap */
+} orc_out;
+
+/* Whole-chain sampler.  Returns 0 on success, <0 on a bad shape. */
+int orc_fit(const orc_chain* c, int mode, orc_out* o);
+
+/* ---------------------------------------------------------------- per-tree pass on explicit state (DEV arithmetic) */
+typedef struct { int mode, nx, v, c, L, R, l, r; } orc_upd;   /* previous tree's accepted move (0 none, 1 birth, 2 death) */
+typedef struct { int mode, nx, v, c; } orc_prop;              /* current tree's proposal (0 none, 1 birth, 2 death) */
+typedef struct {
+  int64_t S0[ORC_NODES], S1[ORC_NODES];                       /* per leaf slot: sum fx(w), sum fx(w*R) */
+  int64_t sL0, sL1, sR0, sR1;                                 /* birth split sums */
+  int nL, nR;
+} orc_stats;
+
+void orc_pass_dev(int n, uint8_t* leaf_prev, const uint8_t* leaf_cur, float* r, const float* w,
+                  const uint8_t* qprev, const uint8_t* qcur, const orc_upd* pu, const float* tho, const float* thn,
+                  int apply, const orc_prop* cp, const float* thc, int fx_shift, orc_stats* st);
+
+/* ---------------------------------------------------------------- DEV arithmetic primitives (exported for tests) */
+void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+double orc_log(double x);
+double orc_exp(double x);
+double orc_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag);
+double orc_gamma(uint64_t seed, uint32_t it, double a);
+double orc_rtnorm(uint64_t seed, uint32_t row, uint32_t it, double mean, double tau, int* capped);
+
+/* ---------------------------------------------------------------- evaluator (src/predict.cpp) */
+typedef struct {
+  int ndpost, ntree, p, nnodes;
+  int* var; int* child; double* cut; double* theta; int* root;
+} orc_ct;
+int orc_compile_trees(const char* text, const double* const* xi, const int* ncut, int ncol, orc_ct* out);
+void orc_ct_free(orc_ct* ct);
+int orc_predict_draw(const orc_ct* ct, const double* const* cols, int ncol, int n, int draw1, double mu, double* out);
+
+/* ---------------------------------------------------------------- output assembly (src/glue.cpp:29-57) */
+/* Writes BART tree text into buf (if non-NULL, up to cap bytes) and returns the full length (excluding NUL). */
+size_t orc_trees_text(const uint64_t* trees, int ndpost, int m, int p, char* buf, size_t cap);
+void orc_varcount(const uint64_t* trees, int ndpost, int m, int p, int* varcount /* [ndpost][p] */);
+void orc_yhat_from_trees(const uint64_t* trees, int ndpost, int m, const uint8_t* q, int n, double* yhat /* [ndpost][n] */);
+
+#endif

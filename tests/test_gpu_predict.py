@@ -1,0 +1,55 @@
+"""GPU parity of compile_trees / predict_draw: bit-exact against the oracle's restatement of src/predict.cpp."""
+import numpy as np
+import pytest
+
+import fastbart_b200 as F
+from fastbart_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def test_predict_draw_bit_exact_and_errors(orc):
+    x, y = W.hazard_data(3000, 4)
+    ch = W.fpbart_chain(x, y, ntree=12, nskip=20, ndpost=8, seed=3)
+    g = F.fit_batch([ch], 20, 8)[0]
+    text = F.trees_text(g["trees"], 3)
+    assert text == orc.trees_text(g["trees"], 3)
+    cps = ch["xi"]
+    ct = F.CompiledTrees(text, cps, mu=ch["offset"])
+    ref = orc.compile_trees(text, cps)
+    arr = ct.arrays()
+    for k in ("var", "child", "cut", "theta", "root"):
+        assert np.array_equal(arr[k], getattr(ref, k)), k
+    xn, _ = W.hazard_data(5000, 99)
+    for d in (1, 4, 8):
+        f = F.predict_draw(ct, xn, d)
+        o = orc.predict_draw(ref, [xn[:, v] for v in range(3)], d, ch["offset"])
+        assert np.array_equal(f, o)
+    with pytest.raises(F.FastbartError, match="out of range"):
+        F.predict_draw(ct, xn, 9)
+    with pytest.raises(F.FastbartError, match="columns"):
+        F.predict_draw(ct, xn[:, :2], 1)
+
+
+def test_fwbart_object_and_predict_reproduces_yhat():
+    x, y, w = W.friedman_data(800, 6, 12)
+    fit = F.fwbart(x, y, w=w, ntree=30, nskip=50, ndpost=20, seed=5)
+    assert fit.cls == "wbart"
+    assert fit["yhat.train"].shape == (20, 800) and fit["sigma"].shape == (70,)
+    assert fit["varcount"].shape == (20, 6)
+    ct = F.compile_trees(fit)
+    for d in (1, 20):
+        f = F.predict_draw(ct, x, d)
+        assert np.max(np.abs(f - fit["yhat.train"][d - 1])) < 1e-8
+    assert np.corrcoef(fit["yhat.train.mean"], W.friedman(x))[0, 1] > 0.95
+
+
+def test_fpbart_object():
+    x, y = W.hazard_data(2000, 1)
+    fit = F.fpbart(x, y, ntree=20, nskip=50, ndpost=20, seed=9)
+    assert fit.cls == "pbart"
+    assert fit["prob.train"].shape == (20, 2000)
+    assert abs(fit["prob.train.mean"].mean() - y.mean()) < 0.05
+    ct = F.compile_trees(fit)
+    f = F.predict_draw(ct, x, 3)
+    assert np.max(np.abs(f - fit["yhat.train"][2])) < 1e-8

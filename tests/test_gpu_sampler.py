@@ -1,0 +1,133 @@
+"""GPU parity of the sampler: the fused per-tree pass and whole chains are bit-exact against the oracle's DEV
+arithmetic on identical state; statistical agreement with the reference sampler (oracle/_ref)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import fastbart_b200 as F
+from fastbart_b200 import _lib, workloads as W
+from fastbart_b200.api import fit_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_pass(n, lp, lc, r, w, qp, qc, upd, th, prop, apply, stats, leafmask, S, threads):
+    st = _lib.PassState()
+    st.n, st.apply, st.stats, st.fx_shift, st.threads = n, apply, stats, S, threads
+    st.pmode, st.pnx, st.pc, st.pL, st.pR, st.pl, st.pr = (upd[k] for k in ("mode", "nx", "c", "L", "R", "l", "r"))
+    st.cmode, st.cnx, st.cc = prop["mode"], prop["nx"], prop["c"]
+    st.leafmask = int(leafmask)
+    st.leaf_prev, st.leaf_cur, st.qprev, st.qcur = lp.ctypes.data, lc.ctypes.data, qp.ctypes.data, qc.ctypes.data
+    st.r, st.w = r.ctypes.data, w.ctypes.data
+    st.tho, st.thn, st.thc = th[0].ctypes.data, th[1].ctypes.data, th[2].ctypes.data
+    out = np.zeros(70, dtype=np.int64)
+    _lib.check(_lib.lib().fb_debug_tree_pass(C.byref(st), out.ctypes.data))
+    return out
+
+
+@pytest.mark.parametrize("n,nleaf,pmode,cmode,threads", [
+    (1, 1, 0, 0, 32), (7, 2, 1, 1, 64), (1000, 1, 0, 1, 256), (1000, 3, 1, 1, 256), (4573, 5, 2, 1, 256),
+    (4573, 8, 1, 2, 512), (3091, 9, 1, 1, 128), (20000, 17, 2, 1, 512), (65536, 32, 1, 1, 512),
+    (24576, 2, 2, 0, 512)])
+def test_tree_pass_bit_exact(orc, n, nleaf, pmode, cmode, threads):
+    rng = np.random.default_rng(n * 7 + nleaf)
+    slots = np.sort(rng.choice(np.arange(64), size=nleaf, replace=False)).astype(np.uint8)
+    lc = rng.choice(slots, n).astype(np.uint8)
+    lp = rng.choice(slots, n).astype(np.uint8)
+    r = rng.normal(0, 3, n).astype(np.float32)
+    w = rng.gamma(4, 0.25, n).astype(np.float32)
+    qp = rng.integers(0, 100, n).astype(np.uint8)
+    qc = rng.integers(0, 100, n).astype(np.uint8)
+    th = [rng.normal(0, 1, 64).astype(np.float32) for _ in range(3)]
+    upd = dict(mode=pmode, nx=int(lp[0]), v=0, c=40, L=int(rng.integers(1, 64)), R=int(rng.integers(1, 64)),
+               l=int(lp[0]), r=int(lp[-1]))
+    prop = dict(mode=cmode, nx=int(lc[0]), v=0, c=50)
+    S = 30
+    leafmask = sum(1 << int(s) for s in slots)
+    lp_o, r_o = lp.copy(), r.copy()
+    ref = orc.pass_dev(n, lp_o, lc, r_o, w, qp, qc, upd, th[0], th[1], 1, prop, th[2], S)
+    lp_g, r_g = lp.copy(), r.copy()
+    out = _gpu_pass(n, lp_g, lc, r_g, w, qp, qc, upd, th, prop, 1, 1, leafmask, S, threads)
+    assert np.array_equal(lp_g, lp_o)
+    assert np.array_equal(r_g.view(np.uint32), r_o.view(np.uint32))
+    for s in slots:
+        assert out[s] == ref["S1"][s], s
+    if cmode == 1:
+        assert np.array_equal(out[64:68], ref["split"])
+        assert out[68] == ref["nL"] and out[69] == ref["nR"]
+
+
+def _compare(a, b, keys=("sigma", "yhat_mean", "yhat", "trees", "moves")):
+    m = {"yhat_mean": "fmean"}
+    for k in keys:
+        x, y = np.asarray(a[k]), np.asarray(b[k] if k in b else b[m[k]])
+        assert x.shape == y.shape, k
+        assert np.array_equal(x, y), f"{k}: first mismatch at {np.argwhere(x != y)[:3]}"
+
+
+def test_chain_bit_exact_wbart(orc):
+    ch = W.fwbart_friedman(n=300, p=5, seed=3, ntree=20, nskip=40, ndpost=20)
+    g = fit_batch([ch], 40, 20)[0]
+    o = orc.fit(ch, orc.MODE_DEV)
+    _compare(g, o)
+
+
+def test_chain_bit_exact_pbart(orc):
+    ch = W.fpbart_hazard(n=1000, seed=2, ntree=10, nskip=30, ndpost=10)
+    g = fit_batch([ch], 30, 10)[0]
+    o = orc.fit(ch, orc.MODE_DEV)
+    _compare(g, o)
+    assert g["rtnorm_caps"] == o["rtnorm_caps"]
+
+
+def test_batch_uneven_chains_bit_exact(orc):
+    """Chains of uneven n, p and ntree, probit and weighted, in one launch; also ragged n (not a multiple of 4)."""
+    chains = [W.fwbart_friedman(n=n, p=p, seed=s, ntree=m, nskip=15, ndpost=6)
+              for n, p, m, s in [(37, 3, 7, 1), (513, 8, 30, 2), (1001, 4, 12, 3), (64, 2, 3, 4)]]
+    chains.append(W.fpbart_hazard(n=777, seed=9, ntree=9, nskip=15, ndpost=6))
+    outs = fit_batch(chains, 15, 6)
+    for ch, g in zip(chains, outs):
+        _compare(g, orc.fit(ch, orc.MODE_DEV))
+
+
+@pytest.mark.parametrize("threads,spl", [(64, 7), (512, 0)])
+def test_launch_shape_does_not_change_results(orc, threads, spl):
+    ch = W.fwbart_friedman(n=700, p=6, seed=21, ntree=25, nskip=20, ndpost=10)
+    base = fit_batch([ch], 20, 10)[0]
+    other = fit_batch([ch], 20, 10, threads=threads, sweeps_per_launch=spl)[0]
+    _compare(other, base, keys=("sigma", "yhat_mean", "yhat", "trees", "moves"))
+
+
+def test_staged_batch_repeats_identically():
+    chains = W.titer_bootstrap(reps=2, shapes=[0, 5], nskip=10, ndpost=5, ntree=50)
+    b = F.Batch(chains, 10, 5)
+    b.run(); b.sync()
+    a = b.download()
+    b.run(); b.sync()
+    c = b.download()
+    for x, y in zip(a, c):
+        _compare(x, y)
+    b.close()
+
+
+def test_probit_large_n_rows_in_global(orc):
+    """n = 24,576 person-weeks (shared memory holds the rows) and n = 40,000 (rows stay in global memory)."""
+    for n in (24576, 40000):
+        ch = W.fpbart_hazard(n=n, seed=5, ntree=6, nskip=4, ndpost=3)
+        g = fit_batch([ch], 4, 3)[0]
+        _compare(g, orc.fit(ch, orc.MODE_DEV))
+
+
+def test_statistical_agreement_with_reference(orc):
+    """Whole chains: posterior-mean f correlation >= 0.99 with the reference sampler and mean sigma within 2%."""
+    if not orc.ref_available():
+        pytest.skip("reference library not built")
+    x, y, w = W.friedman_data(2000, 10, 31)
+    ch = W.fwbart_chain(x, y, w, ntree=100, nskip=500, ndpost=200, seed=77)
+    g = fit_batch([ch], 500, 200)[0]
+    r = orc.ref_fit(ch)
+    corr = np.corrcoef(g["yhat_mean"], r["fmean"])[0, 1]
+    sg, sr = g["sigma"][500:].mean(), r["sigma"][500:].mean()
+    assert corr >= 0.99, corr
+    assert abs(sg / sr - 1) < 0.02, (sg, sr)

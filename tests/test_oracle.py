@@ -1,0 +1,142 @@
+"""CPU tests of the oracle: pinned to the reference's own outputs (golden fixtures made by oracle/_ref) and to the
+published known-answer vector of Philox4x32-10; sanity of the DEV arithmetic and of the evaluator restatement."""
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import make_golden  # noqa: E402
+
+from fastbart_b200 import workloads as W  # noqa: E402
+
+
+@pytest.mark.parametrize("name", sorted(make_golden.CASES))
+def test_ref_mode_matches_reference_golden(orc, name):
+    """The oracle's REF mode reproduces bart_fit_cpu's outputs bit for bit (golden made by the reference itself)."""
+    ch, ref = make_golden.load(name)
+    out = orc.fit(ch, orc.MODE_REF)
+    assert np.array_equal(out["sigma"], ref["sigma"])
+    assert np.array_equal(out["fmean"], ref["fmean"])
+    assert np.array_equal(out["trees"], ref["trees"])
+    assert np.array_equal(out["moves"], ref["moves"])
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+@pytest.mark.parametrize("probit", [0, 1])
+def test_ref_mode_matches_reference_library(orc, seed, probit):
+    """Live comparison with oracle/_ref/libbartref.so when the reference was built here."""
+    if not orc.ref_available():
+        pytest.skip("reference library not built (needs the reference sources)")
+    if probit:
+        ch = W.fpbart_hazard(n=333, seed=seed, ntree=8, nskip=25, ndpost=6)
+    else:
+        ch = W.fwbart_friedman(n=257, p=6, seed=seed, ntree=15, nskip=25, ndpost=8)
+    a, b = orc.fit(ch, orc.MODE_REF), orc.ref_fit(ch)
+    for k in ("sigma", "fmean", "trees", "moves"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_philox_known_answer(orc):
+    # Random123 known-answer vector of philox4x32-10: counter 0, key 0
+    assert orc.philox([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+
+
+def test_log_exp_accuracy(orc):
+    xs = np.exp(np.linspace(-740, 700, 4001))
+    for x in xs:
+        if x != 1.0:
+            assert abs(orc.log(x) - math.log(x)) <= 4e-16 * abs(math.log(x)) + 1e-300
+    assert orc.log(1.0) == 0.0
+    assert orc.log(5e-324) == pytest.approx(math.log(5e-324), rel=1e-15)
+    for x in np.linspace(-745, 709, 4001):
+        assert abs(orc.exp(x) - math.exp(x)) <= 2e-15 * math.exp(x) + 1e-323
+    assert orc.exp(-800.0) == 0.0 and math.isinf(orc.exp(710.0))
+
+
+def test_normal_gamma_rtnorm_moments(orc):
+    z = np.array([orc.normal(99, (s << 8), 7, 3, 3) for s in range(20000)])
+    assert abs(z.mean()) < 0.03 and abs(z.std() - 1) < 0.03
+    g = np.array([orc.gamma(5 + k, k, 30.0) for k in range(4000)])
+    assert abs(g.mean() - 30.0) < 0.4 and abs(g.var() - 30.0) < 3.0
+    t = np.array([orc.rtnorm(3, i, 0, 0.0, 1.5)[0] for i in range(4000)])
+    assert t.min() > 1.5
+    ref = 0.0 + math.exp(-1.5**2 / 2) / math.sqrt(2 * math.pi) / (0.5 * math.erfc(1.5 / math.sqrt(2)))
+    assert abs(t.mean() - ref) < 0.03
+
+
+def _random_pass_state(rng, n, nleaf, pmode):
+    slots = np.sort(rng.choice(np.arange(64), size=nleaf, replace=False)).astype(np.uint8)
+    lc = rng.choice(slots, n).astype(np.uint8)
+    lp = rng.integers(0, 64, n).astype(np.uint8)
+    r = rng.normal(0, 3, n).astype(np.float32)
+    w = rng.gamma(4, 0.25, n).astype(np.float32)
+    qp = rng.integers(0, 50, n).astype(np.uint8)
+    qc = rng.integers(0, 50, n).astype(np.uint8)
+    th = [rng.normal(0, 1, 64).astype(np.float32) for _ in range(3)]
+    upd = dict(mode=pmode, nx=int(lp[0]), v=0, c=25, L=int(rng.integers(1, 64)), R=int(rng.integers(1, 64)),
+               l=int(lp[1]), r=int(lp[2]))
+    prop = dict(mode=1, nx=int(slots[0]), v=0, c=20)
+    return slots, lc, lp, r, w, qp, qc, th, upd, prop
+
+
+def test_pass_dev_sums_are_exact(orc):
+    """DEV pass: int64 sums equal brute-force sums of the per-row fixed-point terms."""
+    rng = np.random.default_rng(0)
+    n, S = 1000, 30
+    slots, lc, lp, r, w, qp, qc, th, upd, prop = _random_pass_state(rng, n, 5, 1)
+    lp0, r0 = lp.copy(), r.copy()
+    st = orc.pass_dev(n, lp, lc, r, w, qp, qc, upd, th[0], th[1], 1, prop, th[2], S)
+    # recompute in numpy
+    lf = lp0.astype(int)
+    lf2 = lf.copy()
+    sel = lf == upd["nx"]
+    lf2[sel] = np.where(qp[sel] <= upd["c"], upd["L"], upd["R"])
+    rr = ((r0 + th[0][lf]).astype(np.float32) - th[1][lf2]).astype(np.float32)
+    assert np.array_equal(lp, lf2.astype(np.uint8)) and np.array_equal(r, rr)
+    R = (rr + th[2][lc]).astype(np.float32)
+    wr = (w * R).astype(np.float32)
+    fx = np.rint((wr * np.float32(2.0**S)).astype(np.float32).astype(np.float64)).astype(np.int64)
+    for s in slots:
+        assert st["S1"][s] == fx[lc == s].sum()
+    inx = lc == prop["nx"]
+    left = inx & (qc <= prop["c"])
+    assert st["nL"] == left.sum() and st["nR"] == (inx & ~left).sum()
+    assert st["split"][1] == fx[left].sum() and st["split"][3] == fx[inx & ~left].sum()
+
+
+def test_dev_mode_is_deterministic_and_sane(orc):
+    ch = W.fwbart_friedman(n=400, p=5, seed=4, ntree=20, nskip=60, ndpost=30)
+    a = orc.fit(ch, orc.MODE_DEV)
+    b = orc.fit(ch, orc.MODE_DEV)
+    for k in ("sigma", "fmean", "yhat", "trees", "moves"):
+        assert np.array_equal(a[k], b[k])
+    # yhat from the FP64 refresh equals glue.cpp's re-traversal of the packed kept trees
+    assert np.array_equal(a["yhat"], orc.yhat_from_trees(a["trees"], ch["q"]))
+    assert np.allclose(a["fmean"], a["yhat"].mean(axis=0), atol=1e-12)
+    x, y, w = W.friedman_data(400, 5, 4)
+    assert np.corrcoef(a["fmean"] + ch["fmean"], W.friedman(x))[0, 1] > 0.95
+
+
+def test_text_compile_predict_roundtrip(orc):
+    """Tree text -> compile_trees -> predict_draw on the training x reproduces yhat.train to 1e-8 (10-digit text)."""
+    x, y, w = W.friedman_data(300, 4, 8)
+    ch = W.fwbart_chain(x, y, w, ntree=10, nskip=20, ndpost=5, numcut=30, seed=5)
+    a = orc.fit(ch, orc.MODE_DEV)
+    text = orc.trees_text(a["trees"], 4)
+    assert text.startswith("5 10 4\n")
+    ct = orc.compile_trees(text, ch["xi"])
+    cols = [x[:, v] for v in range(4)]
+    for d in range(1, 6):
+        f = orc.predict_draw(ct, cols, d, 0.0)
+        assert np.max(np.abs(f - a["yhat"][d - 1])) < 1e-8
+    with pytest.raises(ValueError, match="out of range"):
+        orc.predict_draw(ct, cols, 6, 0.0)
+    with pytest.raises(ValueError, match="columns"):
+        orc.predict_draw(ct, cols[:3], 1, 0.0)
+    vc = orc.varcount(a["trees"], 4)
+    internal = np.array([[((a["trees"][d, j] >> np.uint64(16)) & np.uint64(255)) != 0 for j in range(10)]
+                         for d in range(5)]).reshape(5, -1).sum(axis=1)
+    assert np.array_equal(vc.sum(axis=1), internal)
