@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the batched BART sampler on B200: chain-sweeps/s (and ESS/s) of the 96-chain titer bootstrap workload.
+
+Workload (one "step"): 96 fwbart chains of uneven size run to completion in one batch -- 6 model shapes
+(n 3,091-4,573, p 15-19) x 16 multinomial bootstrap resamples, ntree 200, nskip 1000, ndpost 100 (1,100 sweeps each),
+seeded synthetic data with the shapes of the reference's titer models.  Every step runs the whole MCMC on the device
+from the initial state, producing all outputs (sigma draws, yhat.train draws, posterior mean, kept trees).
+
+  python bench.py [--gpus N --steps K --warmup W]          this implementation (one rank per GPU under torchrun)
+  python bench.py --impl reference [--steps K --warmup W]   the reference sampler (bart_fit_cpu, built from source
+                                                            into oracle/_ref) on the host cores, one chain per core
+
+Timing: W untimed warm-up steps; K timed steps, each preceded (outside its event pair) by a write of 512 MiB to flush
+L2; CUDA events on the launching stream; max over ranks.  Multi-GPU: every rank runs its own 96-chain batch (different
+seeds), no collective on the data path ("weak" scaling); value = all ranks' chain-sweeps / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "chain-sweeps/s (96 batched fwbart chains, titer bootstrap)"
+UNIT = "chain-sweeps/s"
+BYTES_PER_ROW_TREE = 16   # algorithmic bytes per row-tree visit of the fused pass (leaf ids 3, residual 8, w 4, code 1)
+NSKIP, NDPOST, NTREE = 1000, 100, 200
+WORKLOAD_NAME = "titer_bootstrap_96"
+
+
+def workload(rank: int = 0, reps: int = 16, nskip=NSKIP, ndpost=NDPOST):
+    from fastbart_b200 import workloads as W
+    return W.titer_bootstrap(reps=reps, seed=rank, nskip=nskip, ndpost=ndpost, ntree=NTREE)
+
+
+def set_workload(name: str):
+    """'titer96' (the benchmark) or 'small' (6 chains, one per shape, 40 sweeps: the profiling case)."""
+    global NSKIP, NDPOST, WORKLOAD_NAME, workload
+    if name == "small":
+        NSKIP, NDPOST, WORKLOAD_NAME = 30, 10, "titer_small_6x40"
+        base = workload
+
+        def small(rank: int = 0, reps: int = 1, nskip=None, ndpost=None):
+            return base(rank, 1, NSKIP, NDPOST)
+        workload = small
+
+
+# ------------------------------------------------------------------------------------------------ CPU reference
+def _ref_worker(args):
+    ch, sweeps = args
+    from oracle import oracle as O
+    ch = dict(ch)
+    ch["nskip"], ch["ndpost"] = sweeps - 10, 10
+    t = time.perf_counter()
+    if O.ref_available():
+        O.ref_fit(ch)
+        kind = "reference"
+    else:
+        O.fit(ch, O.MODE_REF)
+        kind = "port"
+    return time.perf_counter() - t, kind
+
+
+def _full_ref_chain(ch):
+    from oracle import oracle as O
+    if O.ref_available():
+        return O.ref_fit(ch)["fmean"]
+    return O.fit(ch, O.MODE_REF)["fmean"]
+
+
+def cpu_sample_plan(ncores: int):
+    sweeps = 300 if ncores <= 8 else max(40, 2400 // ncores)
+    return sweeps
+
+
+def run_cpu_sample(pool, chains, ncores, sweeps):
+    tasks = [(chains[k % len(chains)], sweeps) for k in range(ncores)]
+    t = time.perf_counter()
+    res = pool.map(_ref_worker, tasks)
+    wall = time.perf_counter() - t
+    return ncores * sweeps / wall, res[0][1], wall
+
+
+# ------------------------------------------------------------------------------------------------ clocks
+class Clocks:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.lines = index, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        load = [s for s in sm if mx and s > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per full-size launch from the committed ncu summary (scaled from a small capture), or None."""
+    p = os.path.join(ROOT, "profiles", "sampler_kernel_titer96.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch_full:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------------------------------------ reference arm
+def bench_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    chains = workload(0)
+    ncores = os.cpu_count() or 1
+    sweeps = cpu_sample_plan(ncores)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(ncores) as pool:
+        for _ in range(args.warmup):
+            run_cpu_sample(pool, chains, ncores, sweeps)
+        vals, kind, walls = [], "reference", []
+        for _ in range(args.steps):
+            v, kind, wall = run_cpu_sample(pool, chains, ncores, sweeps)
+            vals.append(v); walls.append(wall)
+    tot = sum(walls)
+    value = ncores * sweeps * args.steps / tot
+    sample = f"{ncores} chains of the 96 (one per core), {sweeps} sweeps each, per step"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "chains": 96, "ntree": NTREE, "nskip": NSKIP,
+                       "ndpost": NDPOST},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------ our arm
+def bench_ours(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    chains = workload(rank)
+    S = NSKIP + NDPOST
+
+    # CPU baseline before any CUDA work (the pool is spawned here, rank 0, N = 1 only)
+    cpu = None
+    full_ref = None
+    pool = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ncores = os.cpu_count() or 1
+        sweeps = cpu_sample_plan(ncores)
+        pool = mp.get_context("spawn").Pool(ncores)
+        v, kind, wall = run_cpu_sample(pool, chains, ncores, sweeps)
+        cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": kind,
+               "sample": f"{ncores} of the 96 chains, one per core, {sweeps} sweeps each ({wall:.1f} s wall)"}
+        full_ref = pool.apply_async(_full_ref_chain, (chains[0],))   # agreement check of chain 0, full length
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    import fastbart_b200 as F
+    from fastbart_b200 import diagnostics
+
+    b = F.Batch(chains, NSKIP, NDPOST, threads=args.threads, device=local)
+    info = b.launch_info()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        flush.zero_()
+        b.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        b.run(stream.cuda_stream)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(c) for a, c in evs]
+    tot_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    units = len(chains) * S * args.steps * world
+    value = units / (tot_ms / 1000.0)
+
+    # outputs of the last run: ESS of sigma and f (Geyer initial monotone sequence)
+    outs = b.download()
+    ess_s, ess_f = [], []
+    for o in outs:
+        e = diagnostics.chain_ess(o["sigma"][NSKIP:], o["yhat"])
+        ess_s.append(e["sigma"]); ess_f.append(e["f_median"])
+    per_step_s = tot_ms / 1000.0 / args.steps
+    ess_line = {"sigma_per_s": sum(ess_s) * world / per_step_s, "f_median_per_s": sum(ess_f) * world / per_step_s,
+                "sigma_mean_ess": float(np.mean(ess_s)), "f_median_ess": float(np.mean(ess_f)), "kept": NDPOST}
+    b.close()
+
+    # roofline of the sampler kernel (one launch per step)
+    alg = BYTES_PER_ROW_TREE * sum(np.asarray(c["q"]).shape[1] * (c["ntree"] + 1) for c in chains) * S
+    launch_s = per_step_s / info["launches"]
+    achieved = alg / launch_s / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profiled_traffic()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": peak_kind,
+            "note": "algorithmic bytes 16 B per row-tree visit; the kernel is bound by serial control latency"}
+
+    # end to end through the public C ABI with host buffers (pinned), every step: H2D inputs, MCMC, D2H outputs
+    e2e = None
+    if not args.no_e2e:
+        from fastbart_b200 import api
+        import ctypes as C
+        from fastbart_b200 import _lib
+
+        def pinned(shape, dtype):
+            shape = (shape,) if isinstance(shape, (int, np.integer)) else tuple(shape)
+            dt = np.dtype(dtype)
+            t = torch.empty(int(np.prod(shape)) * dt.itemsize, dtype=torch.uint8, pin_memory=True)
+            return t.numpy().view(dt).reshape(shape)
+
+        keep: list = []
+        pin_chains = []
+        for c in chains:
+            d = dict(c)
+            for k in ("q", "y", "wt"):
+                a = np.asarray(c[k])
+                p_ = pinned(a.shape, a.dtype)
+                p_[...] = a
+                d[k] = p_
+            pin_chains.append(d)
+        arr = (_lib.Chain * len(pin_chains))(*[api._as_chain(c, keep) for c in pin_chains])
+        outs_p = [api._alloc_out(c, NSKIP, NDPOST, True, alloc=pinned) for c in pin_chains]
+        oarr = (_lib.ChainOut * len(outs_p))(*[s_ for _, s_ in outs_p])
+        opt = _lib.Options(NSKIP, NDPOST, args.threads, 0, local)
+        h2d = sum(np.asarray(c["q"]).nbytes + 8 * len(c["y"]) + 4 * len(c["y"]) + len(c["y"]) for c in chains)
+        h2d += len(chains) * 1024
+        d2h = sum(8 * S + 8 * len(c["y"]) * (1 + NDPOST) + 8 * NDPOST * NTREE * 64 for c in chains)
+        times = []
+        for k in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            _lib.check(_lib.lib().fb_fit_batch(arr, len(pin_chains), C.byref(opt), oarr))
+            torch.cuda.synchronize()
+            if k > 0:
+                times.append(time.perf_counter() - t1)
+        e2e_s = max(times) if world == 1 else times[-1]
+        if world > 1:
+            t = torch.tensor([sum(times)], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item()) / len(times)
+        else:
+            e2e_s = sum(times) / len(times)
+        e2e = {"value": len(chains) * S * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": len(times), "ms_per_step": 1000 * e2e_s,
+               "api": "fb_fit_batch (host buffers; allocation, H2D, MCMC, D2H of sigma/yhat/yhat_mean/trees)"}
+
+    r_f = None
+    if full_ref is not None:
+        fm = full_ref.get(timeout=600)
+        r_f = float(np.corrcoef(outs[0]["yhat_mean"], fm)[0, 1])
+        pool.close()
+    if pool is not None:
+        pool.terminate()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64-fixed+f32+f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD_NAME, "chains_per_gpu": len(chains), "ntree": NTREE,
+                           "nskip": NSKIP, "ndpost": NDPOST, "n_range": [3091, 4573], "p_range": [15, 19],
+                           "l2": "flushed (512 MiB write) before every timed step", "threads": info["threads"],
+                           "grid": info["grid"], "smem_bytes": info["smem"]},
+                "e2e": e2e, "gpu_launches": args.steps * info["launches"], "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clk, "ess_per_s": ess_line, "r_f_vs_reference_chain0": r_f, "wall_s": wall}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="titer96", choices=["titer96", "small"])
+    args = ap.parse_args()
+    set_workload(args.workload)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return bench_reference(args)
+    return bench_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

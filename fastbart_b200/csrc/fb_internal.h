@@ -11,6 +11,7 @@ constexpr int NMAX = 65536;    // rows per chain (src/bart_kernel.h:16)
 constexpr int MAXDEPTH = 24;   // src/bart_kernel.h:33
 constexpr int NB_MAX = 8;      // per-thread register bins of the fused pass; leaves beyond use shared atomics
 constexpr int MAX_THREADS = 512;
+constexpr int MIN_THREADS = 64;   // warp 0 is the control warp; at least one row warp
 
 // Topology of one tree: 64 node slots (leaf values are kept apart, in th[]).  464 bytes, 16-byte multiple.
 struct DTree {
@@ -54,6 +55,7 @@ struct DBufs {
   const float* win;
   const int8_t* ybin;
   float* rsave;
+  float* wsave;
   uint8_t* leaf;
   DTree* trees;
   long long* s0;
@@ -87,6 +89,7 @@ struct DPassArgs {
   const uint8_t* qcur;           // [n_pad]
   float* r;                      // [n_pad] in/out
   const float* w;                // [n_pad]
+  float* wscratch;               // [n_pad] scaled weights when rows stay in global memory
   const float* tho;              // [64]
   const float* thn;              // [64]
   const float* thc;              // [64]

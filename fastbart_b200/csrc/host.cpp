@@ -116,8 +116,8 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   *out = nullptr;
   if (!chains || nchains < 1 || !opt) return fail(FB_ERR_ARG, "chains, nchains >= 1 and opt are required");
   if (opt->nskip < 0 || opt->ndpost < 1) return fail(FB_ERR_ARG, "nskip must be >= 0 and ndpost >= 1");
-  if (opt->threads != 0 && (opt->threads < 32 || opt->threads > MAX_THREADS || opt->threads % 32))
-    return fail(FB_ERR_ARG, "threads must be a multiple of 32 in 32..%d", MAX_THREADS);
+  if (opt->threads != 0 && (opt->threads < MIN_THREADS || opt->threads > MAX_THREADS || opt->threads % 32))
+    return fail(FB_ERR_ARG, "threads must be a multiple of 32 in %d..%d", MIN_THREADS, MAX_THREADS);
   for (int k = 0; k < nchains; k++) {
     fb_status s = check_chain(chains[k], k);
     if (s != FB_OK) return s;
@@ -167,8 +167,9 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   // launch shape
   int T = opt->threads;
   if (T == 0) {
-    const int groups = n_pad_max / 4;
-    T = groups >= 4096 ? 512 : 256;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
+    T = nchains <= nsm ? 512 : 256;   // one chain per SM: widest CTA; more chains than SMs: two CTAs per SM
   }
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt->device) != cudaSuccess) optin = 232448;
@@ -189,12 +190,13 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
     if (s == FB_OK) b->allocs.push_back((void*)*p);
     return s;
   };
-  DChain* dch; DState* dst; uint8_t* dq; double* dyin; double* dyw; float* dw; int8_t* dyb; float* drs; uint8_t* dleaf;
+  DChain* dch; DState* dst; uint8_t* dq; double* dyin; double* dyw; float* dw; int8_t* dyb; float* drs; float* dws;
+  uint8_t* dleaf;
   DTree* dtr; long long* ds0; float* dth; double* dtm; double* dsig; double* dyh; unsigned long long* dto; int* dord;
   int* dqueue;
   fb_status s = FB_OK;
   if ((s = A(&dch, nchains)) || (s = A(&dst, nchains)) || (s = A(&dq, b->qbytes)) || (s = A(&dyin, b->rows)) ||
-      (s = A(&dyw, b->rows)) || (s = A(&dw, b->rows)) || (s = A(&dyb, b->rows)) || (s = A(&drs, b->rows)) ||
+      (s = A(&dyw, b->rows)) || (s = A(&dw, b->rows)) || (s = A(&dyb, b->rows)) || (s = A(&drs, b->rows)) || (s = A(&dws, b->rows)) ||
       (s = A(&dleaf, b->leafbytes)) || (s = A(&dtr, b->ntrees)) || (s = A(&ds0, b->ntrees * NODES)) ||
       (s = A(&dth, b->ntrees * NODES)) || (s = A(&dtm, b->rows)) || (s = A(&dsig, b->nsig)) ||
       (s = A(&dyh, b->nyhat)) || (s = A(&dto, b->ntout)) || (s = A(&dord, nchains)) || (s = A(&dqueue, 1))) {
@@ -225,7 +227,7 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   CK(cudaMemcpy(dw, hw.data(), hw.size() * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dyb, hyb.data(), hyb.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dord, b->order.data(), sizeof(int) * nchains, cudaMemcpyHostToDevice));
-  d.chains = dch; d.states = dst; d.q = dq; d.yin = dyin; d.ywork = dyw; d.win = dw; d.ybin = dyb; d.rsave = drs;
+  d.chains = dch; d.states = dst; d.q = dq; d.yin = dyin; d.ywork = dyw; d.win = dw; d.ybin = dyb; d.rsave = drs; d.wsave = dws;
   d.leaf = dleaf; d.trees = dtr; d.s0 = ds0; d.th = dth; d.tm = dtm; d.sigma_out = dsig; d.yhat_out = dyh;
   d.trees_out = dto; d.order = dord; d.queue = dqueue; d.nchains = nchains; d.m_max = m_max;
   d.n_pad_max = n_pad_max; d.rows_in_smem = rows_in_smem;
@@ -610,7 +612,8 @@ fb_status fb_debug_tree_pass(const fb_pass_state* s, int64_t* out) {
   if (!s || !out || !s->r || !s->w || !s->tho || !s->thn || !s->thc) return fail(FB_ERR_ARG, "missing argument");
   if (s->n < 1 || s->n > NMAX) return fail(FB_ERR_LIMIT, "n must be in 1..%d", NMAX);
   const int T = s->threads ? s->threads : 256;
-  if (T < 32 || T > MAX_THREADS || T % 32) return fail(FB_ERR_ARG, "threads must be a multiple of 32 in 32..%d", MAX_THREADS);
+  if (T < MIN_THREADS || T > MAX_THREADS || T % 32)
+    return fail(FB_ERR_ARG, "threads must be a multiple of 32 in %d..%d", MIN_THREADS, MAX_THREADS);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
   const int n = s->n, n_pad = (int)round_up(n, 16);
@@ -626,7 +629,7 @@ fb_status fb_debug_tree_pass(const fb_pass_state* s, int64_t* out) {
   float* dfl = nullptr;
   long long* dout = nullptr;
   CK(cudaMalloc(&dbytes, (size_t)n_pad * 4));
-  CK(cudaMalloc(&dfl, sizeof(float) * ((size_t)n_pad * 2 + 3 * NODES)));
+  CK(cudaMalloc(&dfl, sizeof(float) * ((size_t)n_pad * 3 + 3 * NODES)));
   CK(cudaMalloc(&dout, sizeof(long long) * 70));
   CK(cudaMemcpy(dbytes, lp.data(), n_pad, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dbytes + n_pad, lc.data(), n_pad, cudaMemcpyHostToDevice));
@@ -644,7 +647,7 @@ fb_status fb_debug_tree_pass(const fb_pass_state* s, int64_t* out) {
   a.cmode = s->cmode; a.cnx = s->cnx; a.cc = s->cc; a.fx_shift = s->fx_shift; a.leafmask = s->leafmask;
   a.leaf_prev = dbytes; a.leaf_cur = dbytes + n_pad; a.qprev = dbytes + 2 * n_pad; a.qcur = dbytes + 3 * n_pad;
   a.r = dfl; a.w = dfl + n_pad; a.tho = dfl + 2 * n_pad; a.thn = dfl + 2 * n_pad + NODES;
-  a.thc = dfl + 2 * n_pad + 2 * NODES; a.out = dout;
+  a.thc = dfl + 2 * n_pad + 2 * NODES; a.wscratch = dfl + 2 * n_pad + 3 * NODES; a.out = dout;
   fb_status st = FB_OK;
   if (launch_debug_pass(a, T, nullptr) != 0) st = fail(FB_ERR_CUDA, "debug pass launch failed");
   if (st == FB_OK && cudaDeviceSynchronize() != cudaSuccess) st = fail(FB_ERR_CUDA, "debug pass failed: %s", cudaGetErrorString(cudaGetLastError()));

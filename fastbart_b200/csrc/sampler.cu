@@ -6,18 +6,20 @@
 // Layout and execution
 //   * One CTA runs one chain at a time; CTAs pull chains from a device work queue (atomic counter over a host-sorted
 //     order, largest n*ntree first), so chains of uneven n, p and ntree share one launch.
-//   * Every thread owns fixed groups of 4 consecutive rows (group g = tid + k*T) for the whole run, so per-row state
-//     never moves between threads: FP32 residuals r and weights w sit in shared memory (float4 per group), leaf ids
-//     [ntree][n] and cutpoint codes [p][n] stream from L2 as one 32-bit word per group (4 rows).
-//   * Per sweep: (1) all m proposals are drawn in parallel, one thread per tree (a proposal depends only on its own
-//     tree and on counter-based random numbers); (2) for each tree j, ONE fused pass over the rows applies tree j-1's
-//     accepted move and new leaf values, and accumulates tree j's per-leaf sums and the birth split sums as exact
-//     int64 fixed point (order independent, so bit-exact); warp sums use redux.sync on three 21-bit limbs; then one
-//     warp runs Metropolis-Hastings, the tree update and the leaf mu draws in FP64, lanes in parallel over leaves;
-//     (3) an end-of-sweep pass refreshes every row's fit as an FP64 tree-order sum of leaf values (which is also the
-//     draw's yhat.train), redraws the probit latent z, and accumulates rss for the sigma draw.
-//   * sum(w) per leaf is maintained exactly per tree (root: sum of all rows; birth: the split sums; death: the sum of
-//     the two children), so the pass reduces only sum(w * R).
+//   * Warp 0 is the control warp; warps 1.. stream the rows.  Rows live in shared memory (FP32 residual r and the
+//     weight pre-scaled to fixed point, ws = w * 2^S, one float4 per group of 4 rows); leaf ids [ntree][n] and
+//     cutpoint codes [p][n] stream from L2 as one 32-bit word per group.
+//   * Per sweep: (1) all proposals are drawn in parallel, one thread per tree (a proposal depends only on its own
+//     tree and on counter-based random numbers); (2) for each tree j the row warps make ONE fused pass that applies
+//     tree j-1's accepted move (leaf ids updated four at a time with byte-SIMD compares, r -= delta from a 64-entry
+//     table) and accumulates tree j's per-leaf sum of fx(w*R) into per-thread shared-memory bins plus the birth split
+//     sums, all exact int64 (order independent, hence bit-exact); warp sums use redux.sync on three 21-bit limbs.
+//     Meanwhile the control warp prefetches tree j's topology (cp.async) and draws the leaf-mu normals of every slot
+//     that can be a leaf after the move.  Then the control warp runs Metropolis-Hastings, the tree update and the mu
+//     draws in FP64, lanes in parallel; (3) an end-of-sweep pass refreshes every row's fit as an FP64 tree-order sum
+//     of leaf values (which is also the draw's yhat.train), redraws the probit latent z, and sums rss for sigma.
+//   * sum(w) per leaf is maintained exactly per tree (root: all rows; birth: the split sums; death: the two
+//     children), so the pass reduces only sum(fx(w * R)).
 //   * Random numbers: Philox4x32-10 keyed by the chain seed, counter = (draw index, tree or row, sweep, purpose).
 //   * All control arithmetic is IEEE FP64 through fb_math.cuh; the file is compiled with -fmad=false.  The oracle's
 //     DEV mode (oracle/fb_oracle.c) restates exactly this arithmetic on the CPU.
@@ -30,6 +32,8 @@
 
 namespace fb {
 
+constexpr int NBS = NB_MAX;   // per-thread shared-memory bins (compact leaf index < NBS); beyond: shared atomics
+
 struct Prop {                 // proposal of one tree for the current sweep
   double logpr, lu;
   uint8_t mode, nx, v, c, l, r, pad0, pad1;
@@ -37,6 +41,7 @@ struct Prop {                 // proposal of one tree for the current sweep
 struct Masks { unsigned long long used, leaf; };
 struct Ctl {                  // CTA-shared control state
   int pmode, pnx, pv, pc, pL, pR, pl, pr;   // tree j-1's applied move
+  float DL, DR;                             // apply deltas of a birth's left / right rows
   int nleaf;                                // leaves of tree j
   int births, deaths, caps, rtcaps;
   int chain;
@@ -61,6 +66,9 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+__device__ __forceinline__ uint32_t bcast4(int v) { return (uint32_t)v * 0x01010101u; }
+__device__ __forceinline__ int byte_of(uint32_t w, int e) { return (int)((w >> (8 * e)) & 255u); }
+
 // ------------------------------------------------------------------------------------------------ fused row pass
 struct PassU {
   uint8_t* leaf_prev;
@@ -68,112 +76,102 @@ struct PassU {
   const uint8_t* qprev;
   const uint8_t* qcur;
   float* r;
-  const float* w;
-  const float* tho;
-  const float* thn;
-  const float* thc;
-  const uint8_t* cmap;
-  int n, ngroups;
+  const float* ws;
+  const float* D;       // [64] apply deltas
+  const float2* tc;     // [64] {theta of tree j, compact leaf index as int bits}
+  long long* bins;      // [NBS][RT]
+  unsigned long long* ovb;
+  long long* wpart;     // [NWR][NBS]
+  long long* wsplit;    // [NWR][4]
+  int* wcnt;            // [NWR][2]
+  float DL, DR;
+  int n, ngroups, rt, RT, rwarp, nleaf;
   int apply, pmode, pnx, pc, pL, pR, pl, pr;
-  int stats, cmode, cnx, cc;
-  float scale;
+  int cmode, cnx, cc;
 };
 
-// Applies tree j-1's move to its leaf ids and to r, and accumulates tree j's statistics.  Per-warp results go to
-// wpart[warp][b] (sum fx(w*R) of compact leaf b < NB), wsplit[warp][4] and wcnt[warp][2]; leaves with compact index
-// >= NB (trees with more than NB leaves) are added to ovb[slot] with shared atomics.  Integer sums: the result does
-// not depend on the thread or row order.  (src/bart_kernel.cpp:164-201 semantics; gpu/bart_batch.cu:184-227
-// fixed-point semantics.)
-template <int NB>
-__device__ __forceinline__ void pass_rows(const PassU& P, int nleaf, long long* wpart, long long* wsplit, int* wcnt,
-                                          unsigned long long* ovb) {
-  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
-  long long acc[NB];
-#pragma unroll
-  for (int b = 0; b < NB; b++) acc[b] = 0;
+// Applies tree j-1's move to its leaf ids and to r, accumulates tree j's statistics (src/bart_kernel.cpp:164-201
+// semantics; gpu/bart_batch.cu:184-227 fixed-point semantics).  Called by the row warps only; every lane of a row
+// warp must call it (warp-wide reductions at the end).
+__device__ __forceinline__ void pass_rows(const PassU& P) {
+  const int lane = threadIdx.x & 31;
+  long long* mybins = P.bins + P.rt;
   long long sl0 = 0, sl1 = 0, sr0 = 0, sr1 = 0;
   int nl = 0, nr = 0;
-  for (int g = tid; g < P.ngroups; g += T) {
+  const uint32_t pnx4 = bcast4(P.pnx), pc4 = bcast4(P.pc), pl4 = bcast4(P.pl), pr4 = bcast4(P.pr);
+  const uint32_t pL4 = bcast4(P.pL), pR4 = bcast4(P.pR), cnx4 = bcast4(P.cnx), cc4 = bcast4(P.cc);
+  for (int g = P.rt; g < P.ngroups; g += P.RT) {
+    const uint32_t lc4 = *reinterpret_cast<const uint32_t*>(P.leaf_cur + 4 * g);
     const uint32_t lp4 = P.apply ? *reinterpret_cast<const uint32_t*>(P.leaf_prev + 4 * g) : 0u;
-    const uint32_t lc4 = P.stats ? *reinterpret_cast<const uint32_t*>(P.leaf_cur + 4 * g) : 0u;
     const uint32_t qp4 = (P.apply && P.pmode == 1) ? __ldg(reinterpret_cast<const uint32_t*>(P.qprev + 4 * g)) : 0u;
-    const uint32_t qc4 = (P.stats && P.cmode == 1) ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
+    const uint32_t qc4 = P.cmode == 1 ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
     const float4 r4 = reinterpret_cast<const float4*>(P.r)[g];
-    const float4 w4 = reinterpret_cast<const float4*>(P.w)[g];
+    const float4 w4 = reinterpret_cast<const float4*>(P.ws)[g];
     float rr[4] = {r4.x, r4.y, r4.z, r4.w};
     const float ww[4] = {w4.x, w4.y, w4.z, w4.w};
-    uint32_t lpn = lp4;
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      float ri = rr[e];
-      if (P.apply) {
-        const int lf = (int)((lp4 >> (8 * e)) & 255u);
-        int lf2 = lf;
-        if (P.pmode == 1) {
-          if (lf == P.pnx) lf2 = (int)((qp4 >> (8 * e)) & 255u) <= P.pc ? P.pL : P.pR;
-        } else if (P.pmode == 2) {
-          if (lf == P.pl || lf == P.pr) lf2 = P.pnx;
-        }
-        const float t1 = __fadd_rn(ri, P.tho[lf]);
-        ri = __fsub_rn(t1, P.thn[lf2]);
-        lpn = (lpn & ~(0xFFu << (8 * e))) | ((uint32_t)lf2 << (8 * e));
-        rr[e] = ri;
-      }
-      if (P.stats) {
-        const int lc = (int)((lc4 >> (8 * e)) & 255u);
-        const float R = __fadd_rn(ri, P.thc[lc]);
-        const float wr = __fmul_rn(ww[e], R);
-        const long long wrfx = __float2ll_rn(__fmul_rn(wr, P.scale));
-        const int ci = P.cmap[lc];
-        if (ci >= NB) atomicAdd(&ovb[lc], (unsigned long long)wrfx);
-#pragma unroll
-        for (int b = 0; b < NB; b++) acc[b] += (ci == b) ? wrfx : 0ll;
-        if (P.cmode == 1 && lc == P.cnx && 4 * g + e < P.n) {
-          const long long wfx = __float2ll_rn(__fmul_rn(ww[e], P.scale));
-          if ((int)((qc4 >> (8 * e)) & 255u) <= P.cc) { nl++; sl0 += wfx; sl1 += wrfx; }
-          else { nr++; sr0 += wfx; sr1 += wrfx; }
-        }
-      }
-    }
     if (P.apply) {
+      uint32_t lpn = lp4, mv = 0u, side = 0u;
+      if (P.pmode == 1) {
+        mv = __vcmpeq4(lp4, pnx4);
+        side = __vcmpleu4(qp4, pc4);                       // 0xFF where the row goes left
+        lpn = (lp4 & ~mv) | (mv & ((side & pL4) | (~side & pR4)));
+      } else if (P.pmode == 2) {
+        const uint32_t md = __vcmpeq4(lp4, pl4) | __vcmpeq4(lp4, pr4);
+        lpn = (lp4 & ~md) | (md & pnx4);                   // death deltas come from the table
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        float delta = P.D[byte_of(lp4, e)];
+        if (byte_of(mv, e)) delta = byte_of(side, e) ? P.DL : P.DR;
+        rr[e] = __fsub_rn(rr[e], delta);
+      }
       reinterpret_cast<float4*>(P.r)[g] = make_float4(rr[0], rr[1], rr[2], rr[3]);
       if (lpn != lp4) *reinterpret_cast<uint32_t*>(P.leaf_prev + 4 * g) = lpn;
     }
-  }
-  if (P.stats) {
+    long long wr[4];
 #pragma unroll
-    for (int b = 0; b < NB; b++) {
-      if (b < nleaf) {
-        const long long s = warp_sum64(acc[b]);
-        if (lane == 0) wpart[warp * NB_MAX + b] = s;
-      }
+    for (int e = 0; e < 4; e++) {
+      const int lc = byte_of(lc4, e);
+      const float2 t = P.tc[lc];
+      const float R = __fadd_rn(rr[e], t.x);
+      wr[e] = __float2ll_rn(__fmul_rn(ww[e], R));
+      const int ci = __float_as_int(t.y);
+      if (ci < NBS) mybins[ci * P.RT] += wr[e];
+      else atomicAdd(&P.ovb[lc], (unsigned long long)wr[e]);
     }
     if (P.cmode == 1) {
-      const long long a0 = warp_sum64(sl0), a1 = warp_sum64(sl1), a2 = warp_sum64(sr0), a3 = warp_sum64(sr1);
-      const int c0 = __reduce_add_sync(0xffffffffu, nl), c1 = __reduce_add_sync(0xffffffffu, nr);
-      if (lane == 0) {
-        wsplit[warp * 4 + 0] = a0; wsplit[warp * 4 + 1] = a1; wsplit[warp * 4 + 2] = a2; wsplit[warp * 4 + 3] = a3;
-        wcnt[warp * 2 + 0] = c0; wcnt[warp * 2 + 1] = c1;
+      uint32_t inx = __vcmpeq4(lc4, cnx4);
+      const int left = P.n - 4 * g;
+      if (left < 4) inx &= (1u << (8 * (left > 0 ? left : 0))) - 1u;   // rows beyond n are padding
+      if (inx) {
+        const uint32_t lq = __vcmpleu4(qc4, cc4);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          if (byte_of(inx, e)) {
+            const long long wfx = __float2ll_rn(ww[e]);
+            if (byte_of(lq, e)) { nl++; sl0 += wfx; sl1 += wr[e]; }
+            else { nr++; sr0 += wfx; sr1 += wr[e]; }
+          }
+        }
       }
     }
   }
-}
-
-__device__ __forceinline__ void pass_dispatch(const PassU& P, int nleaf, long long* wpart, long long* wsplit,
-                                              int* wcnt, unsigned long long* ovb) {
-  if (nleaf <= 2) pass_rows<2>(P, nleaf, wpart, wsplit, wcnt, ovb);
-  else if (nleaf <= 4) pass_rows<4>(P, nleaf, wpart, wsplit, wcnt, ovb);
-  else pass_rows<8>(P, nleaf, wpart, wsplit, wcnt, ovb);
-}
-
-__device__ __forceinline__ int nb_for(int nleaf) { return nleaf <= 2 ? 2 : (nleaf <= 4 ? 4 : 8); }
-
-// compact index of each leaf slot (0..L-1 in slot order), 255 for other slots
-__device__ __forceinline__ void build_cmap(unsigned long long lm, uint8_t* cmap, int lane) {
-  for (int s = lane; s < NODES; s += 32) {
-    const bool isl = (lm >> s) & 1ull;
-    const int ci = __popcll(lm & ((1ull << s) - 1ull));
-    cmap[s] = isl ? (uint8_t)ci : (uint8_t)255;
+  // per-warp reductions of the private bins (and reset them for the next pass)
+  const int nb = P.nleaf < NBS ? P.nleaf : NBS;
+  for (int b = 0; b < nb; b++) {
+    const long long v = mybins[b * P.RT];
+    mybins[b * P.RT] = 0;
+    const long long s = warp_sum64(v);
+    if (lane == 0) P.wpart[P.rwarp * NBS + b] = s;
+  }
+  if (P.cmode == 1) {
+    const long long a0 = warp_sum64(sl0), a1 = warp_sum64(sl1), a2 = warp_sum64(sr0), a3 = warp_sum64(sr1);
+    const int c0 = __reduce_add_sync(0xffffffffu, nl), c1 = __reduce_add_sync(0xffffffffu, nr);
+    if (lane == 0) {
+      P.wsplit[P.rwarp * 4 + 0] = a0; P.wsplit[P.rwarp * 4 + 1] = a1;
+      P.wsplit[P.rwarp * 4 + 2] = a2; P.wsplit[P.rwarp * 4 + 3] = a3;
+      P.wcnt[P.rwarp * 2 + 0] = c0; P.wcnt[P.rwarp * 2 + 1] = c1;
+    }
   }
 }
 
@@ -282,18 +280,21 @@ __device__ Prop propose(DTree* t, const DChain& C, int j, int it, Masks& mk) {
 
 // ------------------------------------------------------------------------------------------------ shared layout
 struct Smem {
-  float* r; float* w;           // [n_pad] (shared or global)
+  float* r; float* ws;          // [n_pad] (shared, or global when rows do not fit)
   float* th;                    // [m][64]
   Prop* prop;                   // [m]
   Masks* masks;                 // [m]
   DTree* tcur;                  // tree j (copy)
   long long* s0cur;             // [64]
   long long* s1;                // [64]
-  float* tho; float* thn;       // [64]
-  uint8_t* cmap;                // [64]
-  long long* wpart;             // [NW][8]
-  long long* wsplit;            // [NW][4]
-  int* wcnt;                    // [NW][2]
+  float* tho;                   // [64] leaf values of tree j before its mu draw
+  float* D;                     // [64] apply deltas of tree j-1's update
+  float2* tc;                   // [64] theta and compact leaf index of tree j
+  double* z;                    // [64] mu normals of tree j
+  long long* bins;              // [NBS][RT]
+  long long* wpart;             // [NWR][NBS]
+  long long* wsplit;            // [NWR][4]
+  int* wcnt;                    // [NWR][2]
   unsigned long long* ovb;      // [64]
   long long* red;               // [NW]
   Ctl* ctl;
@@ -302,10 +303,10 @@ struct Smem {
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_max, int rows_in_smem, size_t* off) {
-  const int NW = threads / 32;
+  const int NW = threads / 32, RT = threads - 32, NWR = NW - 1;
   size_t o = 0;
   off[0] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // r
-  off[1] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // w
+  off[1] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // ws
   off[2] = o; o += align_up((size_t)m_max * NODES * 4, 16);                  // th
   off[3] = o; o += align_up((size_t)m_max * sizeof(Prop), 16);               // prop
   off[4] = o; o += align_up((size_t)m_max * sizeof(Masks), 16);              // masks
@@ -313,24 +314,26 @@ __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_
   off[6] = o; o += NODES * 8;                                                // s0cur
   off[7] = o; o += NODES * 8;                                                // s1
   off[8] = o; o += NODES * 4;                                                // tho
-  off[9] = o; o += NODES * 4;                                                // thn
-  off[10] = o; o += NODES;                                                   // cmap
-  o = align_up(o, 16);
-  off[11] = o; o += (size_t)NW * NB_MAX * 8;                                 // wpart
-  off[12] = o; o += (size_t)NW * 4 * 8;                                      // wsplit
-  off[13] = o; o += align_up((size_t)NW * 2 * 4, 16);                        // wcnt
-  off[14] = o; o += NODES * 8;                                               // ovb
-  off[15] = o; o += (size_t)NW * 8;                                          // red
-  off[16] = o; o += align_up(sizeof(Ctl), 16);                               // ctl
+  off[9] = o; o += NODES * 4;                                                // D
+  off[10] = o; o += NODES * 8;                                               // tc
+  off[11] = o; o += NODES * 8;                                               // z
+  off[12] = o; o += (size_t)NBS * RT * 8;                                    // bins
+  off[13] = o; o += (size_t)NWR * NBS * 8;                                   // wpart
+  off[14] = o; o += (size_t)NWR * 4 * 8;                                     // wsplit
+  off[15] = o; o += align_up((size_t)NWR * 2 * 4, 16);                       // wcnt
+  off[16] = o; o += NODES * 8;                                               // ovb
+  off[17] = o; o += align_up((size_t)NW * 8, 16);                            // red
+  off[18] = o; o += align_up(sizeof(Ctl), 16);                               // ctl
   return o;
 }
+constexpr int NOFF = 19;
 
 __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max, int rows_in_smem) {
-  size_t off[17];
+  size_t off[NOFF];
   smem_layout(threads, m_max, n_pad_max, rows_in_smem, off);
   Smem S;
   S.r = reinterpret_cast<float*>(base + off[0]);
-  S.w = reinterpret_cast<float*>(base + off[1]);
+  S.ws = reinterpret_cast<float*>(base + off[1]);
   S.th = reinterpret_cast<float*>(base + off[2]);
   S.prop = reinterpret_cast<Prop*>(base + off[3]);
   S.masks = reinterpret_cast<Masks*>(base + off[4]);
@@ -338,14 +341,16 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.s0cur = reinterpret_cast<long long*>(base + off[6]);
   S.s1 = reinterpret_cast<long long*>(base + off[7]);
   S.tho = reinterpret_cast<float*>(base + off[8]);
-  S.thn = reinterpret_cast<float*>(base + off[9]);
-  S.cmap = reinterpret_cast<uint8_t*>(base + off[10]);
-  S.wpart = reinterpret_cast<long long*>(base + off[11]);
-  S.wsplit = reinterpret_cast<long long*>(base + off[12]);
-  S.wcnt = reinterpret_cast<int*>(base + off[13]);
-  S.ovb = reinterpret_cast<unsigned long long*>(base + off[14]);
-  S.red = reinterpret_cast<long long*>(base + off[15]);
-  S.ctl = reinterpret_cast<Ctl*>(base + off[16]);
+  S.D = reinterpret_cast<float*>(base + off[9]);
+  S.tc = reinterpret_cast<float2*>(base + off[10]);
+  S.z = reinterpret_cast<double*>(base + off[11]);
+  S.bins = reinterpret_cast<long long*>(base + off[12]);
+  S.wpart = reinterpret_cast<long long*>(base + off[13]);
+  S.wsplit = reinterpret_cast<long long*>(base + off[14]);
+  S.wcnt = reinterpret_cast<int*>(base + off[15]);
+  S.ovb = reinterpret_cast<unsigned long long*>(base + off[16]);
+  S.red = reinterpret_cast<long long*>(base + off[17]);
+  S.ctl = reinterpret_cast<Ctl*>(base + off[18]);
   return S;
 }
 
@@ -362,10 +367,22 @@ __device__ long long block_sum64(long long x, long long* red) {
   return t;
 }
 
+// theta / compact-index table of tree j (control warp)
+__device__ __forceinline__ void build_tc(const Smem& S, int j, int lane) {
+  const unsigned long long lm = S.masks[j].leaf & S.masks[j].used;
+  const float* thj = S.th + j * NODES;
+  for (int s = lane; s < NODES; s += 32) {
+    const int ci = ((lm >> s) & 1ull) ? __popcll(lm & ((1ull << s) - 1ull)) : 255;
+    S.tc[s] = make_float2(thj[s], __int_as_float(ci));
+  }
+  if (lane == 0) S.ctl->nleaf = __popcll(lm);
+}
+
 // ------------------------------------------------------------------------------------------------ one chain
 __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& S) {
   const DChain& C = B.chains[ci];
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, NW = T >> 5;
+  const int RT = T - 32, NWR = NW - 1;
   const int n = C.n, m = C.m, n_pad = C.n_pad, ngroups = n_pad / 4;
   const unsigned long long seed = C.seed;
   const double t2 = C.tau * C.tau, a_prior = 1.0 / t2;
@@ -379,9 +396,10 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   double* ywork = B.ywork + C.off_row;
   const float* wg = B.win + C.off_row;
   float* rg = B.rsave + C.off_row;
+  float* wsg = B.wsave + C.off_row;
   double* tm = B.tm + C.off_row;
   float* r = B.rows_in_smem ? S.r : rg;
-  const float* w = B.rows_in_smem ? S.w : wg;
+  float* ws = B.rows_in_smem ? S.ws : wsg;
   Ctl& ctl = *S.ctl;
   DState& st = B.states[ci];
 
@@ -391,7 +409,10 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     else { ctl.sigma = st.sigma; ctl.births = st.births; ctl.deaths = st.deaths; ctl.caps = st.caps; ctl.rtcaps = st.rtcaps; }
     ctl.pmode = 0;
   }
+  for (int k = tid; k < NBS * RT; k += T) S.bins[k] = 0;
+  for (int s = tid; s < NODES; s += T) S.ovb[s] = 0ull;
   __syncthreads();
+  for (int i = tid; i < n_pad; i += T) ws[i] = __fmul_rn(wg[i], scale);   // exact: power-of-two scaling
   if (it0 == 0) {
     int caps = 0;
     for (int i = tid; i < n_pad; i += T) {
@@ -404,7 +425,6 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       }
       ywork[i] = y;
       r[i] = (float)y;
-      if (B.rows_in_smem) S.w[i] = wg[i];
       tm[i] = 0.0;
     }
     if (caps) atomicAdd(&ctl.rtcaps, caps);
@@ -425,9 +445,8 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     }
     for (int k = tid; k < m * NODES; k += T) s0g[k] = (k % NODES == 0) ? swt : 0ll;
   } else {
-    for (int i = tid; i < n_pad; i += T) {
-      if (B.rows_in_smem) { S.r[i] = rg[i]; S.w[i] = wg[i]; }
-    }
+    if (B.rows_in_smem)
+      for (int i = tid; i < n_pad; i += T) S.r[i] = rg[i];
     for (int k = tid; k < m * NODES; k += T) S.th[k] = thg[k];
   }
   __syncthreads();
@@ -442,62 +461,72 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     }
     __syncthreads();
     if (warp == 0) {
-      const unsigned long long lm = S.masks[0].leaf & S.masks[0].used;
-      build_cmap(lm, S.cmap, lane);
-      if (lane == 0) { ctl.nleaf = __popcll(lm); ctl.pmode = 0; }
-      for (int s = lane; s < NODES; s += 32) S.ovb[s] = 0ull;
+      build_tc(S, 0, lane);
+      if (lane == 0) ctl.pmode = 0;
     }
     __syncthreads();
     // ---------------------------------------------------------------- (2) trees
     for (int j = 0; j < m; j++) {
-      // prefetch tree j's topology and leaf weights into shared memory while the rows stream
-      {
+      const Prop P = S.prop[j];
+      if (warp > 0) {
+        PassU U;
+        U.leaf_prev = j > 0 ? leaf + (long long)(j - 1) * n_pad : nullptr;
+        U.leaf_cur = leaf + (long long)j * n_pad;
+        U.qprev = q + (long long)ctl.pv * n_pad;
+        U.qcur = q + (long long)P.v * n_pad;
+        U.r = r; U.ws = ws; U.D = S.D; U.tc = S.tc; U.bins = S.bins; U.ovb = S.ovb;
+        U.wpart = S.wpart; U.wsplit = S.wsplit; U.wcnt = S.wcnt;
+        U.DL = ctl.DL; U.DR = ctl.DR;
+        U.n = n; U.ngroups = ngroups; U.rt = tid - 32; U.RT = RT; U.rwarp = warp - 1; U.nleaf = ctl.nleaf;
+        U.apply = j > 0; U.pmode = ctl.pmode; U.pnx = ctl.pnx; U.pc = ctl.pc; U.pL = ctl.pL; U.pR = ctl.pR;
+        U.pl = ctl.pl; U.pr = ctl.pr;
+        U.cmode = P.mode; U.cnx = P.nx; U.cc = P.c;
+        pass_rows(U);
+      } else {
+        // control warp during the pass: prefetch tree j, draw the normals of every slot that can be a leaf after
+        // this step's move (current leaves, the two slots a birth would take, the node a death would restore)
         constexpr int TW = (int)(sizeof(DTree) / 16), SW = NODES * 8 / 16;
-        for (int k = tid; k < TW + SW; k += T) {
+        for (int k = lane; k < TW + SW; k += 32) {
           if (k < TW) cp_async16(reinterpret_cast<unsigned char*>(S.tcur) + 16 * k, reinterpret_cast<const unsigned char*>(trees + j) + 16 * k);
           else cp_async16(reinterpret_cast<unsigned char*>(S.s0cur) + 16 * (k - TW), reinterpret_cast<const unsigned char*>(s0g + (long long)j * NODES) + 16 * (k - TW));
         }
+        const Masks mk = S.masks[j];
+        unsigned long long cand = mk.leaf & mk.used;
+        if (P.mode == 1) {
+          const int L = first_free(mk.used, -1), R = L >= 0 ? first_free(mk.used, L) : -1;
+          if (L >= 0 && R >= 0) cand |= (1ull << L) | (1ull << R);
+        } else if (P.mode == 2) {
+          cand |= 1ull << P.nx;
+        }
+        for (int s = lane; s < NODES; s += 32)
+          if ((cand >> s) & 1ull) S.z[s] = fbm::fb_normal(seed, (uint32_t)s << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
+        cp_async_wait_all();
       }
-      const Prop P = S.prop[j];
-      const int nleaf = ctl.nleaf;
-      PassU U;
-      U.leaf_prev = j > 0 ? leaf + (long long)(j - 1) * n_pad : nullptr;
-      U.leaf_cur = leaf + (long long)j * n_pad;
-      U.qprev = q + (long long)ctl.pv * n_pad;
-      U.qcur = q + (long long)P.v * n_pad;
-      U.r = r; U.w = w; U.tho = S.tho; U.thn = S.thn; U.thc = S.th + j * NODES; U.cmap = S.cmap;
-      U.n = n; U.ngroups = ngroups;
-      U.apply = j > 0; U.pmode = ctl.pmode; U.pnx = ctl.pnx; U.pc = ctl.pc; U.pL = ctl.pL; U.pR = ctl.pR;
-      U.pl = ctl.pl; U.pr = ctl.pr;
-      U.stats = 1; U.cmode = P.mode; U.cnx = P.nx; U.cc = P.c;
-      U.scale = scale;
-      pass_dispatch(U, nleaf, S.wpart, S.wsplit, S.wcnt, S.ovb);
-      cp_async_wait_all();
       __syncthreads();
       // ---------------------------------------------------------------- control: MH, tree update, mu draws
       if (warp == 0) {
+        const int nleaf = ctl.nleaf;
         const Masks mk = S.masks[j];
         unsigned long long used = mk.used, leafm = mk.leaf;
         const unsigned long long lm0 = used & leafm;
-        const int NBj = nb_for(nleaf);
         for (int s = lane; s < NODES; s += 32) {
           if ((lm0 >> s) & 1ull) {
-            const int ci2 = S.cmap[s];
+            const int ci2 = __float_as_int(S.tc[s].y);
             long long v = 0;
-            if (ci2 < NBj) { for (int w2 = 0; w2 < NW; w2++) v += S.wpart[w2 * NB_MAX + ci2]; }
+            if (ci2 < NBS) { for (int w2 = 0; w2 < NWR; w2++) v += S.wpart[w2 * NBS + ci2]; }
             else v = (long long)S.ovb[s];
             S.s1[s] = v;
           }
-          if (nleaf > NB_MAX) S.ovb[s] = 0ull;
+          if (nleaf > NBS) S.ovb[s] = 0ull;
         }
-        long long sL0 = 0, sL1 = 0, sR0 = 0, sR1 = 0;
-        int nL = 0, nR = 0;
-        if (P.mode == 1) {
-          for (int w2 = 0; w2 < NW; w2++) {
-            sL0 += S.wsplit[w2 * 4 + 0]; sL1 += S.wsplit[w2 * 4 + 1]; sR0 += S.wsplit[w2 * 4 + 2]; sR1 += S.wsplit[w2 * 4 + 3];
-            nL += S.wcnt[w2 * 2 + 0]; nR += S.wcnt[w2 * 2 + 1];
-          }
+        long long sv = 0;
+        if (P.mode == 1 && lane < 6) {
+          if (lane < 4) { for (int w2 = 0; w2 < NWR; w2++) sv += S.wsplit[w2 * 4 + lane]; }
+          else { for (int w2 = 0; w2 < NWR; w2++) sv += S.wcnt[w2 * 2 + lane - 4]; }
         }
+        const long long sL0 = __shfl_sync(0xffffffffu, sv, 0), sL1 = __shfl_sync(0xffffffffu, sv, 1);
+        const long long sR0 = __shfl_sync(0xffffffffu, sv, 2), sR1 = __shfl_sync(0xffffffffu, sv, 3);
+        const int nL = (int)__shfl_sync(0xffffffffu, sv, 4), nR = (int)__shfl_sync(0xffffffffu, sv, 5);
         __syncwarp();
         bool eval = false;
         double bl = 0, Ml = 0, br = 0, Mr = 0;
@@ -535,6 +564,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           R = L >= 0 ? first_free(used, L) : -1;
           if (L < 0 || R < 0) {
             if (lane == 0) ctl.caps++;
+            L = R = 0;
           } else {
             const int nx = P.nx;
             if (lane == 0) {
@@ -563,7 +593,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         }
         if (lane == 0) { t->used = used; t->leaf = leafm; S.masks[j].used = used; S.masks[j].leaf = leafm; }
         __syncwarp();
-        // leaf mu draws (DRMU), lanes in parallel over slots
+        // leaf mu draws (DRMU), lanes in parallel over slots; apply deltas D[s] = new - old
         const unsigned long long lm = used & leafm;
         float* thj = S.th + j * NODES;
         for (int s = lane; s < NODES; s += 32) {
@@ -572,13 +602,19 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           float nw = old;
           if ((lm >> s) & 1ull) {
             const double b = (double)S.s0cur[s] * sci * inv_s2, M = (double)S.s1[s] * sci * inv_s2;
-            const double z = fbm::fb_normal(seed, (uint32_t)s << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
-            nw = (float)(M / (a_prior + b) + z / sqrt(a_prior + b));
+            nw = (float)(M / (a_prior + b) + S.z[s] / sqrt(a_prior + b));
           }
           thj[s] = nw;
-          S.thn[s] = nw;
+          S.D[s] = __fsub_rn(nw, old);
         }
         __syncwarp();
+        if (lane == 0) {
+          float DL = 0.0f, DR = 0.0f;
+          if (nmode == 1) { DL = __fsub_rn(thj[L], S.tho[P.nx]); DR = __fsub_rn(thj[R], S.tho[P.nx]); }
+          else if (nmode == 2) { S.D[l] = __fsub_rn(thj[P.nx], S.tho[l]); S.D[rr] = __fsub_rn(thj[P.nx], S.tho[rr]); }
+          ctl.DL = DL; ctl.DR = DR;
+          ctl.pmode = nmode; ctl.pnx = P.nx; ctl.pv = P.v; ctl.pc = P.c; ctl.pL = L; ctl.pR = R; ctl.pl = l; ctl.pr = rr;
+        }
         // write tree j back
         {
           const uint32_t* src = reinterpret_cast<const uint32_t*>(t);
@@ -586,15 +622,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           for (int k = lane; k < (int)(sizeof(DTree) / 4); k += 32) dst[k] = src[k];
           for (int k = lane; k < NODES; k += 32) s0g[(long long)j * NODES + k] = S.s0cur[k];
         }
-        if (lane == 0) {
-          ctl.pmode = nmode; ctl.pnx = P.nx; ctl.pv = P.v; ctl.pc = P.c; ctl.pL = L; ctl.pR = R; ctl.pl = l; ctl.pr = rr;
-        }
-        // next tree's compact leaf map
-        if (j + 1 < m) {
-          const unsigned long long lmn = S.masks[j + 1].leaf & S.masks[j + 1].used;
-          build_cmap(lmn, S.cmap, lane);
-          if (lane == 0) ctl.nleaf = __popcll(lmn);
-        }
+        if (j + 1 < m) build_tc(S, j + 1, lane);
       }
       __syncthreads();
     }
@@ -604,31 +632,31 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     int caps = 0;
     long long rssfx = 0;
     {
-      const int pmode = ctl.pmode, pnx = ctl.pnx, pc = ctl.pc, pL = ctl.pL, pR = ctl.pR, pl = ctl.pl, pr = ctl.pr;
+      const int pmode = ctl.pmode;
+      const uint32_t pnx4 = bcast4(ctl.pnx), pc4 = bcast4(ctl.pc), pL4 = bcast4(ctl.pL), pR4 = bcast4(ctl.pR),
+                     pl4 = bcast4(ctl.pl), pr4 = bcast4(ctl.pr);
       uint8_t* lp = leaf + (long long)(m - 1) * n_pad;
       const uint8_t* qp = q + (long long)ctl.pv * n_pad;
       for (int g = tid; g < ngroups; g += T) {
         const uint32_t lp4 = *reinterpret_cast<const uint32_t*>(lp + 4 * g);
-        const uint32_t qp4 = pmode == 1 ? __ldg(reinterpret_cast<const uint32_t*>(qp + 4 * g)) : 0u;
         uint32_t lpn = lp4;
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const int lf = (int)((lp4 >> (8 * e)) & 255u);
-          int lf2 = lf;
-          if (pmode == 1) { if (lf == pnx) lf2 = (int)((qp4 >> (8 * e)) & 255u) <= pc ? pL : pR; }
-          else if (pmode == 2) { if (lf == pl || lf == pr) lf2 = pnx; }
-          lpn = (lpn & ~(0xFFu << (8 * e))) | ((uint32_t)lf2 << (8 * e));
+        if (pmode == 1) {
+          const uint32_t mv = __vcmpeq4(lp4, pnx4), side = __vcmpleu4(__ldg(reinterpret_cast<const uint32_t*>(qp + 4 * g)), pc4);
+          lpn = (lp4 & ~mv) | (mv & ((side & pL4) | (~side & pR4)));
+        } else if (pmode == 2) {
+          const uint32_t mv = __vcmpeq4(lp4, pl4) | __vcmpeq4(lp4, pr4);
+          lpn = (lp4 & ~mv) | (mv & pnx4);
         }
         if (lpn != lp4) *reinterpret_cast<uint32_t*>(lp + 4 * g) = lpn;
         // FP64 refresh: f = sum over trees, in tree order, of the row's leaf value
         double f0 = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
         int jj = 0;
-        for (; jj + 4 <= m - 1; jj += 4) {
-          uint32_t l4[4];
+        for (; jj + 16 <= m - 1; jj += 16) {
+          uint32_t l4[16];
 #pragma unroll
-          for (int u = 0; u < 4; u++) l4[u] = *reinterpret_cast<const uint32_t*>(leaf + (long long)(jj + u) * n_pad + 4 * g);
+          for (int u = 0; u < 16; u++) l4[u] = *reinterpret_cast<const uint32_t*>(leaf + (long long)(jj + u) * n_pad + 4 * g);
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
+          for (int u = 0; u < 16; u++) {
             const float* thj = S.th + (jj + u) * NODES;
             f0 += (double)thj[l4[u] & 255u]; f1 += (double)thj[(l4[u] >> 8) & 255u];
             f2 += (double)thj[(l4[u] >> 16) & 255u]; f3 += (double)thj[l4[u] >> 24];
@@ -641,6 +669,8 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           f2 += (double)thj[(l4 >> 16) & 255u]; f3 += (double)thj[l4 >> 24];
         }
         const double fe[4] = {f0, f1, f2, f3};
+        const float4 w4 = reinterpret_cast<const float4*>(ws)[g];
+        const float wwe[4] = {w4.x, w4.y, w4.z, w4.w};
         float rn[4];
 #pragma unroll
         for (int e = 0; e < 4; e++) {
@@ -657,7 +687,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
             const double ee = y - f;
             rn[e] = (float)ee;
             if (!C.probit) {
-              const double we = (double)w[i] * ee;
+              const double we = ((double)wwe[e] * sci) * ee;
               rssfx += __double2ll_rn(we * ee * rscale);
             }
             if (keep) {
@@ -718,7 +748,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it
 }
 
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem) {
-  size_t off[17];
+  size_t off[NOFF];
   return smem_layout(threads, m_max, n_pad_max, rows_in_smem, off);
 }
 
@@ -740,39 +770,62 @@ int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size
 }
 
 // ------------------------------------------------------------------------------------------------ diagnostics
+// One pass on explicit state, run by the same pass_rows() as the sampler: warp 0 builds the tables, warps 1.. stream.
 __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int tid = threadIdx.x, T = blockDim.x, NW = T >> 5;
+  const int tid = threadIdx.x, T = blockDim.x, NW = T >> 5, RT = T - 32, NWR = NW - 1, lane = tid & 31;
   const int rows_smem = a.rows_in_smem;
-  float* r = rows_smem ? reinterpret_cast<float*>(smem) : a.r;
-  float* w = rows_smem ? r + a.n_pad : const_cast<float*>(a.w);
-  float* th3 = reinterpret_cast<float*>(smem + (rows_smem ? (size_t)a.n_pad * 8 : 0));   // tho, thn, thc
-  uint8_t* cmap = reinterpret_cast<uint8_t*>(th3 + 3 * NODES);
-  long long* wpart = reinterpret_cast<long long*>(cmap + NODES);
-  long long* wsplit = wpart + NW * NB_MAX;
-  int* wcnt = reinterpret_cast<int*>(wsplit + NW * 4);
-  unsigned long long* ovb = reinterpret_cast<unsigned long long*>(wcnt + NW * 2);
-  if (rows_smem)
-    for (int i = tid; i < a.n_pad; i += T) { r[i] = a.r[i]; w[i] = a.w[i]; }
-  for (int s = tid; s < NODES; s += T) { th3[s] = a.tho[s]; th3[NODES + s] = a.thn[s]; th3[2 * NODES + s] = a.thc[s]; ovb[s] = 0; }
-  if (tid < 32) build_cmap(a.leafmask, cmap, tid);
+  unsigned char* p = smem;
+  float* r = rows_smem ? reinterpret_cast<float*>(p) : a.r;
+  float* ws = rows_smem ? reinterpret_cast<float*>(p) + a.n_pad : a.wscratch;
+  p += rows_smem ? (size_t)a.n_pad * 8 : 0;
+  float* D = reinterpret_cast<float*>(p); p += NODES * 4;
+  float2* tc = reinterpret_cast<float2*>(p); p += NODES * 8;
+  long long* bins = reinterpret_cast<long long*>(p); p += (size_t)NBS * RT * 8;
+  long long* wpart = reinterpret_cast<long long*>(p); p += (size_t)NWR * NBS * 8;
+  long long* wsplit = reinterpret_cast<long long*>(p); p += (size_t)NWR * 4 * 8;
+  int* wcnt = reinterpret_cast<int*>(p); p += align_up((size_t)NWR * 2 * 4, 16);
+  unsigned long long* ovb = reinterpret_cast<unsigned long long*>(p); p += NODES * 8;
+  float* dlr = reinterpret_cast<float*>(p);
+  const float scale = (float)pow2(a.fx_shift);
+  for (int i = tid; i < a.n_pad; i += T) {
+    if (rows_smem) r[i] = a.r[i];
+    ws[i] = __fmul_rn(a.w[i], scale);
+  }
+  for (int k = tid; k < NBS * RT; k += T) bins[k] = 0;
+  for (int s = tid; s < NODES; s += T) ovb[s] = 0;
+  if (tid < 32) {
+    const unsigned long long lm = a.leafmask;
+    for (int s = lane; s < NODES; s += 32) {
+      const int ci = ((lm >> s) & 1ull) ? __popcll(lm & ((1ull << s) - 1ull)) : 255;
+      tc[s] = make_float2(a.thc[s], __int_as_float(ci));
+      D[s] = __fsub_rn(a.thn[s], a.tho[s]);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      dlr[0] = dlr[1] = 0.0f;
+      if (a.pmode == 1) { dlr[0] = __fsub_rn(a.thn[a.pL], a.tho[a.pnx]); dlr[1] = __fsub_rn(a.thn[a.pR], a.tho[a.pnx]); }
+      else if (a.pmode == 2) { D[a.pl] = __fsub_rn(a.thn[a.pnx], a.tho[a.pl]); D[a.pr] = __fsub_rn(a.thn[a.pnx], a.tho[a.pr]); }
+    }
+  }
   __syncthreads();
   const int nleaf = __popcll(a.leafmask);
-  PassU U;
-  U.leaf_prev = a.leaf_prev; U.leaf_cur = a.leaf_cur; U.qprev = a.qprev; U.qcur = a.qcur;
-  U.r = r; U.w = w; U.tho = th3; U.thn = th3 + NODES; U.thc = th3 + 2 * NODES; U.cmap = cmap;
-  U.n = a.n; U.ngroups = a.n_pad / 4;
-  U.apply = a.apply; U.pmode = a.pmode; U.pnx = a.pnx; U.pc = a.pc; U.pL = a.pL; U.pR = a.pR; U.pl = a.pl; U.pr = a.pr;
-  U.stats = a.stats; U.cmode = a.cmode; U.cnx = a.cnx; U.cc = a.cc;
-  U.scale = (float)pow2(a.fx_shift);
-  pass_dispatch(U, nleaf, wpart, wsplit, wcnt, ovb);
+  if (tid >= 32) {
+    PassU U;
+    U.leaf_prev = a.leaf_prev; U.leaf_cur = a.leaf_cur; U.qprev = a.qprev; U.qcur = a.qcur;
+    U.r = r; U.ws = ws; U.D = D; U.tc = tc; U.bins = bins; U.ovb = ovb; U.wpart = wpart; U.wsplit = wsplit; U.wcnt = wcnt;
+    U.DL = dlr[0]; U.DR = dlr[1];
+    U.n = a.n; U.ngroups = a.n_pad / 4; U.rt = tid - 32; U.RT = RT; U.rwarp = (tid >> 5) - 1; U.nleaf = nleaf;
+    U.apply = a.apply; U.pmode = a.pmode; U.pnx = a.pnx; U.pc = a.pc; U.pL = a.pL; U.pR = a.pR; U.pl = a.pl; U.pr = a.pr;
+    U.cmode = a.stats ? a.cmode : 0; U.cnx = a.cnx; U.cc = a.cc;
+    pass_rows(U);
+  }
   __syncthreads();
-  const int NBj = nb_for(nleaf);
   for (int s = tid; s < NODES; s += T) {
     long long v = 0;
     if ((a.leafmask >> s) & 1ull) {
-      const int ci = cmap[s];
-      if (ci < NBj) { for (int w2 = 0; w2 < NW; w2++) v += wpart[w2 * NB_MAX + ci]; }
+      const int ci = __float_as_int(tc[s].y);
+      if (ci < NBS) { for (int w2 = 0; w2 < NWR; w2++) v += wpart[w2 * NBS + ci]; }
       else v = (long long)ovb[s];
     }
     a.out[s] = v;
@@ -781,7 +834,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
     long long x[4] = {0, 0, 0, 0};
     long long c[2] = {0, 0};
     if (a.stats && a.cmode == 1)
-      for (int w2 = 0; w2 < NW; w2++) {
+      for (int w2 = 0; w2 < NWR; w2++) {
         for (int k = 0; k < 4; k++) x[k] += wsplit[w2 * 4 + k];
         c[0] += wcnt[w2 * 2]; c[1] += wcnt[w2 * 2 + 1];
       }
@@ -793,8 +846,9 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
 }
 
 int launch_debug_pass(DPassArgs a, int threads, void* stream) {
-  const int NW = threads / 32;
-  const size_t rest = 3 * NODES * 4 + NODES + (size_t)NW * NB_MAX * 8 + (size_t)NW * 32 + (size_t)NW * 8 + NODES * 8 + 64;
+  const int NW = threads / 32, RT = threads - 32, NWR = NW - 1;
+  const size_t rest = NODES * 4 + NODES * 8 + (size_t)NBS * RT * 8 + (size_t)NWR * NBS * 8 + (size_t)NWR * 32 +
+                      align_up((size_t)NWR * 8, 16) + NODES * 8 + 16;
   a.rows_in_smem = (size_t)a.n_pad * 8 + rest <= 200 * 1024;
   const size_t smem = (a.rows_in_smem ? (size_t)a.n_pad * 8 : 0) + rest;
   if (cudaFuncSetAttribute(debug_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)

@@ -95,17 +95,18 @@ def fpbart_hazard(n=24576, seed=0, **kw) -> dict:
 
 
 def titer_model(shape_idx: int, seed=0):
-    """Base data of one titer-like model: half U(0,1), half integer 0..9 columns."""
+    """Base data of one titer-like model: half U(0,1), half integer 0..9 columns; y = a linear term on 4 columns
+    (coefficients N(0,1)) + sin(pi xa xb) on two U(0,1) columns + N(0, 0.5^2); weights w ~ Gamma(4, rate 4)."""
     n, p = TITER_SHAPES[shape_idx]
     rng = np.random.default_rng(1000 + 17 * shape_idx + seed)
     x = np.empty((n, p))
     half = p // 2
     x[:, :half] = rng.random((n, half))
     x[:, half:] = rng.integers(0, 10, (n, p - half))
-    cols = rng.choice(p, 6, replace=False)
+    lin = rng.choice(p, 4, replace=False)
+    a, b = rng.choice(half, 2, replace=False)
     beta = rng.normal(0, 1, 4)
-    xs = x / np.maximum(x.max(axis=0), 1e-12)
-    y = xs[:, cols[:4]] @ beta + np.sin(np.pi * xs[:, cols[4]] * xs[:, cols[5]]) + rng.normal(0, 0.5, n)
+    y = x[:, lin] @ beta + np.sin(np.pi * x[:, a] * x[:, b]) + rng.normal(0, 0.5, n)
     w = rng.gamma(4.0, 1.0 / 4.0, n)
     return x, y, w
 

@@ -515,29 +515,43 @@ static int fit_ref(const orc_chain* C, orc_out* o) {
 }
 
 /* ================================================================ DEV mode: the B200 kernels' arithmetic */
-static inline int64_t fx_f(float x, float scale) { return (int64_t)llrintf(x * scale); }
+
+/* Apply-deltas of a tree update: every row moves r -= delta, delta = thn[dest] - tho[src] in FP32.  Non-moving rows of
+   leaf s use D[s] = thn[s] - tho[s]; a death moves the rows of l and r to nx, so D[l], D[r] hold thn[nx] - tho[l|r];
+   a birth moves the rows of nx to L (code <= c) or R, with deltas *DL / *DR. */
+static void apply_deltas(const orc_upd* pu, const float* tho, const float* thn, float* D, float* DL, float* DR) {
+  for (int s = 0; s < ORC_NODES; s++) D[s] = thn[s] - tho[s];
+  *DL = *DR = 0.0f;
+  if (pu->mode == 1) { *DL = thn[pu->L] - tho[pu->nx]; *DR = thn[pu->R] - tho[pu->nx]; }
+  else if (pu->mode == 2) { D[pu->l] = thn[pu->nx] - tho[pu->l]; D[pu->r] = thn[pu->nx] - tho[pu->r]; }
+}
 
 void orc_pass_dev(int n, uint8_t* leaf_prev, const uint8_t* leaf_cur, float* r, const float* w,
                   const uint8_t* qprev, const uint8_t* qcur, const orc_upd* pu, const float* tho, const float* thn,
                   int apply, const orc_prop* cp, const float* thc, int fx_shift, orc_stats* st) {
   const float scale = ldexpf(1.0f, fx_shift);
+  float D[ORC_NODES], DL = 0.0f, DR = 0.0f;
+  if (apply) apply_deltas(pu, tho, thn, D, &DL, &DR);
   memset(st, 0, sizeof *st);
   for (int i = 0; i < n; i++) {
     float ri = r[i];
     if (apply) {
       int lf = leaf_prev[i], lf2 = lf;
-      if (pu->mode == 1 && lf == pu->nx) lf2 = (qprev[i] <= pu->c) ? pu->L : pu->R;
-      else if (pu->mode == 2 && (lf == pu->l || lf == pu->r)) lf2 = pu->nx;
-      float t1 = ri + tho[lf];
-      ri = t1 - thn[lf2];
+      float delta = D[lf];
+      if (pu->mode == 1 && lf == pu->nx) {
+        int left = qprev[i] <= pu->c;
+        lf2 = left ? pu->L : pu->R;
+        delta = left ? DL : DR;
+      } else if (pu->mode == 2 && (lf == pu->l || lf == pu->r)) lf2 = pu->nx;
+      ri = ri - delta;
       r[i] = ri;
       leaf_prev[i] = (uint8_t)lf2;
     }
     if (leaf_cur) {
       int lc = leaf_cur[i];
+      float ws = w[i] * scale;              /* exact: scaling by a power of two */
       float R = ri + thc[lc];
-      float wr_f = w[i] * R;
-      int64_t wfx = fx_f(w[i], scale), wrfx = fx_f(wr_f, scale);
+      int64_t wfx = (int64_t)llrintf(ws), wrfx = (int64_t)llrintf(ws * R);
       st->S0[lc] += wfx; st->S1[lc] += wrfx;
       if (cp && cp->mode == 1 && lc == cp->nx) {
         if (qcur[i] <= cp->c) { st->nL++; st->sL0 += wfx; st->sL1 += wrfx; }

@@ -89,16 +89,20 @@ def test_pass_dev_sums_are_exact(orc):
     slots, lc, lp, r, w, qp, qc, th, upd, prop = _random_pass_state(rng, n, 5, 1)
     lp0, r0 = lp.copy(), r.copy()
     st = orc.pass_dev(n, lp, lc, r, w, qp, qc, upd, th[0], th[1], 1, prop, th[2], S)
-    # recompute in numpy
+    # recompute in numpy: r -= delta, delta = thn[dest] - tho[src] (FP32); fx terms of (w 2^S) * R
     lf = lp0.astype(int)
     lf2 = lf.copy()
     sel = lf == upd["nx"]
-    lf2[sel] = np.where(qp[sel] <= upd["c"], upd["L"], upd["R"])
-    rr = ((r0 + th[0][lf]).astype(np.float32) - th[1][lf2]).astype(np.float32)
+    left = qp[sel] <= upd["c"]
+    lf2[sel] = np.where(left, upd["L"], upd["R"])
+    D = (th[1] - th[0]).astype(np.float32)
+    delta = D[lf]
+    delta[sel] = np.where(left, np.float32(th[1][upd["L"]] - th[0][upd["nx"]]), np.float32(th[1][upd["R"]] - th[0][upd["nx"]]))
+    rr = (r0 - delta).astype(np.float32)
     assert np.array_equal(lp, lf2.astype(np.uint8)) and np.array_equal(r, rr)
     R = (rr + th[2][lc]).astype(np.float32)
-    wr = (w * R).astype(np.float32)
-    fx = np.rint((wr * np.float32(2.0**S)).astype(np.float32).astype(np.float64)).astype(np.int64)
+    ws = (w * np.float32(2.0**S)).astype(np.float32)
+    fx = np.rint((ws * R).astype(np.float32).astype(np.float64)).astype(np.int64)
     for s in slots:
         assert st["S1"][s] == fx[lc == s].sum()
     inx = lc == prop["nx"]
