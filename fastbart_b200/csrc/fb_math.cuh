@@ -1,5 +1,8 @@
 // fb_math.cuh -- deterministic device arithmetic of the sampler.
 //
+// The heavy functions are out of line (__noinline__): one copy of each in the kernel keeps the control warp's code
+// path short.
+//
 // Every function here is defined only through IEEE-754 operations that round the same way on any conforming
 // machine: + - * / sqrt in double, explicit fma(), conversions with round-to-nearest.  Files including it are compiled
 // with -fmad=false so that no a*b+c is contracted behind our back.  A CPU restatement of the same definitions
@@ -43,7 +46,7 @@ __device__ __forceinline__ double u52d(uint32_t hi, uint32_t lo) {
   return ((double)k + 0.5) * 0x1p-52;
 }
 
-__device__ __forceinline__ double fb_log(double x) {
+__device__ __noinline__ double fb_log(double x) {
   if (x != x) return x;
   if (x <= 0.0) return x == 0.0 ? -__longlong_as_double(0x7FF0000000000000LL) : __longlong_as_double(0x7FF8000000000000LL);
   if (__double_as_longlong(x) == 0x7FF0000000000000LL) return x;
@@ -72,7 +75,7 @@ __device__ __forceinline__ double fb_log(double x) {
   return fma(kd, 0x1.62e42fee00000p-1, fma(kd, 0x1.a39ef35793c76p-33, lf));
 }
 
-__device__ __forceinline__ double fb_exp(double x) {
+__device__ __noinline__ double fb_exp(double x) {
   if (x != x) return x;
   if (x > 709.78) return __longlong_as_double(0x7FF0000000000000LL);
   if (x < -745.2) return 0.0;
@@ -100,7 +103,7 @@ __device__ __forceinline__ double fb_exp(double x) {
   return p * __longlong_as_double((long long)((unsigned long long)(k + 1023) << 52));
 }
 
-__device__ __forceinline__ double fb_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag) {
+__device__ __noinline__ double fb_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag) {
   for (uint32_t t = 0; t < 64; t++) {
     const U4 x = philox(c0base + t, c1, c2, tag, seed);
     const double a = 2.0 * u52d(x.x, x.y) - 1.0, b = 2.0 * u52d(x.z, x.w) - 1.0;
@@ -110,7 +113,7 @@ __device__ __forceinline__ double fb_normal(uint64_t seed, uint32_t c0base, uint
   return 0.0;
 }
 
-__device__ __forceinline__ double fb_gamma(uint64_t seed, uint32_t it, double a) {
+__device__ __noinline__ double fb_gamma(uint64_t seed, uint32_t it, double a) {
   const double d = a - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
   for (uint32_t tt = 0; tt < 32; tt++) {
     const double x = fb_normal(seed, tt << 8, 0u, it, TAG_SIG_N);
@@ -125,7 +128,7 @@ __device__ __forceinline__ double fb_gamma(uint64_t seed, uint32_t it, double a)
 }
 
 // N(mean, 1) truncated to > tau; *capped is incremented when a loop gives up (then tau is returned).
-__device__ __forceinline__ double fb_rtnorm(uint64_t seed, uint32_t row, uint32_t it, double mean, double tau, int* capped) {
+__device__ __noinline__ double fb_rtnorm(uint64_t seed, uint32_t row, uint32_t it, double mean, double tau, int* capped) {
   tau = tau - mean;
   if (tau <= 0.0) {
     for (uint32_t tt = 0; tt < 64; tt++) {

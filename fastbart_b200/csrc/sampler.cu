@@ -81,9 +81,8 @@ struct PassU {
   const float2* tc;     // [64] {theta of tree j, compact leaf index as int bits}
   long long* bins;      // [NBS][RT]
   unsigned long long* ovb;
-  long long* wpart;     // [NWR][NBS]
-  long long* wsplit;    // [NWR][4]
-  int* wcnt;            // [NWR][2]
+  long long* s1c;       // [NBS] CTA totals of sum fx(w*R) per compact leaf
+  long long* split;     // [6] CTA totals sL0 sL1 sR0 sR1 nL nR
   float DL, DR;
   int n, ngroups, rt, RT, rwarp, nleaf;
   int apply, pmode, pnx, pc, pL, pR, pl, pr;
@@ -156,21 +155,23 @@ __device__ __forceinline__ void pass_rows(const PassU& P) {
       }
     }
   }
-  // per-warp reductions of the private bins (and reset them for the next pass)
+  // per-warp reductions of the private bins (reset for the next pass), then one shared atomic per warp and leaf into
+  // the CTA totals (integer adds: the order of the atomics does not matter)
   const int nb = P.nleaf < NBS ? P.nleaf : NBS;
   for (int b = 0; b < nb; b++) {
     const long long v = mybins[b * P.RT];
     mybins[b * P.RT] = 0;
     const long long s = warp_sum64(v);
-    if (lane == 0) P.wpart[P.rwarp * NBS + b] = s;
+    if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&P.s1c[b]), (unsigned long long)s);
   }
   if (P.cmode == 1) {
     const long long a0 = warp_sum64(sl0), a1 = warp_sum64(sl1), a2 = warp_sum64(sr0), a3 = warp_sum64(sr1);
     const int c0 = __reduce_add_sync(0xffffffffu, nl), c1 = __reduce_add_sync(0xffffffffu, nr);
     if (lane == 0) {
-      P.wsplit[P.rwarp * 4 + 0] = a0; P.wsplit[P.rwarp * 4 + 1] = a1;
-      P.wsplit[P.rwarp * 4 + 2] = a2; P.wsplit[P.rwarp * 4 + 3] = a3;
-      P.wcnt[P.rwarp * 2 + 0] = c0; P.wcnt[P.rwarp * 2 + 1] = c1;
+      unsigned long long* sp = reinterpret_cast<unsigned long long*>(P.split);
+      atomicAdd(sp + 0, (unsigned long long)a0); atomicAdd(sp + 1, (unsigned long long)a1);
+      atomicAdd(sp + 2, (unsigned long long)a2); atomicAdd(sp + 3, (unsigned long long)a3);
+      atomicAdd(sp + 4, (unsigned long long)c0); atomicAdd(sp + 5, (unsigned long long)c1);
     }
   }
 }
@@ -207,7 +208,7 @@ __device__ int count_goodvars(const DTree* t, int x, const int* nc, int p) {   /
   }
   return g;
 }
-__device__ __forceinline__ double lh(double b, double M, double t2) {   // src/bart_kernel.cpp:278
+__device__ __noinline__ double lh(double b, double M, double t2) {   // src/bart_kernel.cpp:278
   const double k = b * t2 + 1.0;
   return -0.5 * fbm::fb_log(k) + 0.5 * M * M * t2 / k;
 }
@@ -292,9 +293,8 @@ struct Smem {
   float2* tc;                   // [64] theta and compact leaf index of tree j
   double* z;                    // [64] mu normals of tree j
   long long* bins;              // [NBS][RT]
-  long long* wpart;             // [NWR][NBS]
-  long long* wsplit;            // [NWR][4]
-  int* wcnt;                    // [NWR][2]
+  long long* s1c;               // [NBS]
+  long long* split;             // [8]
   unsigned long long* ovb;      // [64]
   long long* red;               // [NW]
   Ctl* ctl;
@@ -303,7 +303,7 @@ struct Smem {
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_max, int rows_in_smem, size_t* off) {
-  const int NW = threads / 32, RT = threads - 32, NWR = NW - 1;
+  const int NW = threads / 32, RT = threads - 32;
   size_t o = 0;
   off[0] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // r
   off[1] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // ws
@@ -318,9 +318,9 @@ __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_
   off[10] = o; o += NODES * 8;                                               // tc
   off[11] = o; o += NODES * 8;                                               // z
   off[12] = o; o += (size_t)NBS * RT * 8;                                    // bins
-  off[13] = o; o += (size_t)NWR * NBS * 8;                                   // wpart
-  off[14] = o; o += (size_t)NWR * 4 * 8;                                     // wsplit
-  off[15] = o; o += align_up((size_t)NWR * 2 * 4, 16);                       // wcnt
+  off[13] = o; o += (size_t)NBS * 8;                                         // s1c
+  off[14] = o; o += 8 * 8;                                                   // split
+  off[15] = o; o += 0;                                                       // (unused)
   off[16] = o; o += NODES * 8;                                               // ovb
   off[17] = o; o += align_up((size_t)NW * 8, 16);                            // red
   off[18] = o; o += align_up(sizeof(Ctl), 16);                               // ctl
@@ -345,9 +345,8 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.tc = reinterpret_cast<float2*>(base + off[10]);
   S.z = reinterpret_cast<double*>(base + off[11]);
   S.bins = reinterpret_cast<long long*>(base + off[12]);
-  S.wpart = reinterpret_cast<long long*>(base + off[13]);
-  S.wsplit = reinterpret_cast<long long*>(base + off[14]);
-  S.wcnt = reinterpret_cast<int*>(base + off[15]);
+  S.s1c = reinterpret_cast<long long*>(base + off[13]);
+  S.split = reinterpret_cast<long long*>(base + off[14]);
   S.ovb = reinterpret_cast<unsigned long long*>(base + off[16]);
   S.red = reinterpret_cast<long long*>(base + off[17]);
   S.ctl = reinterpret_cast<Ctl*>(base + off[18]);
@@ -381,8 +380,8 @@ __device__ __forceinline__ void build_tc(const Smem& S, int j, int lane) {
 // ------------------------------------------------------------------------------------------------ one chain
 __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& S) {
   const DChain& C = B.chains[ci];
-  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, NW = T >> 5;
-  const int RT = T - 32, NWR = NW - 1;
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int RT = T - 32;
   const int n = C.n, m = C.m, n_pad = C.n_pad, ngroups = n_pad / 4;
   const unsigned long long seed = C.seed;
   const double t2 = C.tau * C.tau, a_prior = 1.0 / t2;
@@ -411,6 +410,8 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   }
   for (int k = tid; k < NBS * RT; k += T) S.bins[k] = 0;
   for (int s = tid; s < NODES; s += T) S.ovb[s] = 0ull;
+  if (tid < NBS) S.s1c[tid] = 0;
+  if (tid < 8) S.split[tid] = 0;
   __syncthreads();
   for (int i = tid; i < n_pad; i += T) ws[i] = __fmul_rn(wg[i], scale);   // exact: power-of-two scaling
   if (it0 == 0) {
@@ -475,7 +476,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         U.qprev = q + (long long)ctl.pv * n_pad;
         U.qcur = q + (long long)P.v * n_pad;
         U.r = r; U.ws = ws; U.D = S.D; U.tc = S.tc; U.bins = S.bins; U.ovb = S.ovb;
-        U.wpart = S.wpart; U.wsplit = S.wsplit; U.wcnt = S.wcnt;
+        U.s1c = S.s1c; U.split = S.split;
         U.DL = ctl.DL; U.DR = ctl.DR;
         U.n = n; U.ngroups = ngroups; U.rt = tid - 32; U.RT = RT; U.rwarp = warp - 1; U.nleaf = ctl.nleaf;
         U.apply = j > 0; U.pmode = ctl.pmode; U.pnx = ctl.pnx; U.pc = ctl.pc; U.pL = ctl.pL; U.pR = ctl.pR;
@@ -512,21 +513,15 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         for (int s = lane; s < NODES; s += 32) {
           if ((lm0 >> s) & 1ull) {
             const int ci2 = __float_as_int(S.tc[s].y);
-            long long v = 0;
-            if (ci2 < NBS) { for (int w2 = 0; w2 < NWR; w2++) v += S.wpart[w2 * NBS + ci2]; }
-            else v = (long long)S.ovb[s];
-            S.s1[s] = v;
+            S.s1[s] = ci2 < NBS ? S.s1c[ci2] : (long long)S.ovb[s];
           }
           if (nleaf > NBS) S.ovb[s] = 0ull;
         }
-        long long sv = 0;
-        if (P.mode == 1 && lane < 6) {
-          if (lane < 4) { for (int w2 = 0; w2 < NWR; w2++) sv += S.wsplit[w2 * 4 + lane]; }
-          else { for (int w2 = 0; w2 < NWR; w2++) sv += S.wcnt[w2 * 2 + lane - 4]; }
-        }
-        const long long sL0 = __shfl_sync(0xffffffffu, sv, 0), sL1 = __shfl_sync(0xffffffffu, sv, 1);
-        const long long sR0 = __shfl_sync(0xffffffffu, sv, 2), sR1 = __shfl_sync(0xffffffffu, sv, 3);
-        const int nL = (int)__shfl_sync(0xffffffffu, sv, 4), nR = (int)__shfl_sync(0xffffffffu, sv, 5);
+        const long long sL0 = S.split[0], sL1 = S.split[1], sR0 = S.split[2], sR1 = S.split[3];
+        const int nL = (int)S.split[4], nR = (int)S.split[5];
+        __syncwarp();
+        if (lane < NBS) S.s1c[lane] = 0;
+        if (lane < 8) S.split[lane] = 0;
         __syncwarp();
         bool eval = false;
         double bl = 0, Ml = 0, br = 0, Mr = 0;
@@ -541,16 +536,13 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         }
         bool accept = false;
         if (eval) {
+          // lanes 0..2 evaluate the three log marginal likelihoods at one call site: birth (l, r, l+r), death
+          // (l+r, l, r), in the order the ratio adds them
+          const int which = P.mode == 1 ? lane : (lane == 0 ? 2 : lane - 1);
+          const double hb = which == 0 ? bl : (which == 1 ? br : bl + br);
+          const double hM = which == 0 ? Ml : (which == 1 ? Mr : Ml + Mr);
           double hv = 0.0;
-          if (P.mode == 1) {
-            if (lane == 0) hv = lh(bl, Ml, t2);
-            else if (lane == 1) hv = lh(br, Mr, t2);
-            else if (lane == 2) hv = lh(bl + br, Ml + Mr, t2);
-          } else {
-            if (lane == 0) hv = lh(bl + br, Ml + Mr, t2);
-            else if (lane == 1) hv = lh(bl, Ml, t2);
-            else if (lane == 2) hv = lh(br, Mr, t2);
-          }
+          if (lane < 3) hv = lh(hb, hM, t2);
           const double h0 = __shfl_sync(0xffffffffu, hv, 0), h1 = __shfl_sync(0xffffffffu, hv, 1),
                        h2 = __shfl_sync(0xffffffffu, hv, 2);
           double lalpha = (P.mode == 1) ? P.logpr + h0 + h1 - h2 : P.logpr + h0 - h1 - h2;
@@ -773,7 +765,7 @@ int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size
 // One pass on explicit state, run by the same pass_rows() as the sampler: warp 0 builds the tables, warps 1.. stream.
 __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int tid = threadIdx.x, T = blockDim.x, NW = T >> 5, RT = T - 32, NWR = NW - 1, lane = tid & 31;
+  const int tid = threadIdx.x, T = blockDim.x, RT = T - 32, lane = tid & 31;
   const int rows_smem = a.rows_in_smem;
   unsigned char* p = smem;
   float* r = rows_smem ? reinterpret_cast<float*>(p) : a.r;
@@ -782,9 +774,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
   float* D = reinterpret_cast<float*>(p); p += NODES * 4;
   float2* tc = reinterpret_cast<float2*>(p); p += NODES * 8;
   long long* bins = reinterpret_cast<long long*>(p); p += (size_t)NBS * RT * 8;
-  long long* wpart = reinterpret_cast<long long*>(p); p += (size_t)NWR * NBS * 8;
-  long long* wsplit = reinterpret_cast<long long*>(p); p += (size_t)NWR * 4 * 8;
-  int* wcnt = reinterpret_cast<int*>(p); p += align_up((size_t)NWR * 2 * 4, 16);
+  long long* s1c = reinterpret_cast<long long*>(p); p += NBS * 8;
+  long long* split = reinterpret_cast<long long*>(p); p += 8 * 8;
   unsigned long long* ovb = reinterpret_cast<unsigned long long*>(p); p += NODES * 8;
   float* dlr = reinterpret_cast<float*>(p);
   const float scale = (float)pow2(a.fx_shift);
@@ -794,6 +785,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
   }
   for (int k = tid; k < NBS * RT; k += T) bins[k] = 0;
   for (int s = tid; s < NODES; s += T) ovb[s] = 0;
+  if (tid < NBS) s1c[tid] = 0;
+  if (tid < 8) split[tid] = 0;
   if (tid < 32) {
     const unsigned long long lm = a.leafmask;
     for (int s = lane; s < NODES; s += 32) {
@@ -813,7 +806,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
   if (tid >= 32) {
     PassU U;
     U.leaf_prev = a.leaf_prev; U.leaf_cur = a.leaf_cur; U.qprev = a.qprev; U.qcur = a.qcur;
-    U.r = r; U.ws = ws; U.D = D; U.tc = tc; U.bins = bins; U.ovb = ovb; U.wpart = wpart; U.wsplit = wsplit; U.wcnt = wcnt;
+    U.r = r; U.ws = ws; U.D = D; U.tc = tc; U.bins = bins; U.ovb = ovb; U.s1c = s1c; U.split = split;
     U.DL = dlr[0]; U.DR = dlr[1];
     U.n = a.n; U.ngroups = a.n_pad / 4; U.rt = tid - 32; U.RT = RT; U.rwarp = (tid >> 5) - 1; U.nleaf = nleaf;
     U.apply = a.apply; U.pmode = a.pmode; U.pnx = a.pnx; U.pc = a.pc; U.pL = a.pL; U.pR = a.pR; U.pl = a.pl; U.pr = a.pr;
@@ -825,30 +818,21 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
     long long v = 0;
     if ((a.leafmask >> s) & 1ull) {
       const int ci = __float_as_int(tc[s].y);
-      if (ci < NBS) { for (int w2 = 0; w2 < NWR; w2++) v += wpart[w2 * NBS + ci]; }
-      else v = (long long)ovb[s];
+      v = ci < NBS ? s1c[ci] : (long long)ovb[s];
     }
     a.out[s] = v;
   }
   if (tid == 0) {
-    long long x[4] = {0, 0, 0, 0};
-    long long c[2] = {0, 0};
-    if (a.stats && a.cmode == 1)
-      for (int w2 = 0; w2 < NWR; w2++) {
-        for (int k = 0; k < 4; k++) x[k] += wsplit[w2 * 4 + k];
-        c[0] += wcnt[w2 * 2]; c[1] += wcnt[w2 * 2 + 1];
-      }
-    for (int k = 0; k < 4; k++) a.out[NODES + k] = x[k];
-    a.out[NODES + 4] = c[0]; a.out[NODES + 5] = c[1];
+    const bool sp = a.stats && a.cmode == 1;
+    for (int k = 0; k < 6; k++) a.out[NODES + k] = sp ? split[k] : 0;
   }
   if (rows_smem)
     for (int i = tid; i < a.n_pad; i += T) a.r[i] = r[i];
 }
 
 int launch_debug_pass(DPassArgs a, int threads, void* stream) {
-  const int NW = threads / 32, RT = threads - 32, NWR = NW - 1;
-  const size_t rest = NODES * 4 + NODES * 8 + (size_t)NBS * RT * 8 + (size_t)NWR * NBS * 8 + (size_t)NWR * 32 +
-                      align_up((size_t)NWR * 8, 16) + NODES * 8 + 16;
+  const int RT = threads - 32;
+  const size_t rest = NODES * 4 + NODES * 8 + (size_t)NBS * RT * 8 + NBS * 8 + 64 + NODES * 8 + 16;
   a.rows_in_smem = (size_t)a.n_pad * 8 + rest <= 200 * 1024;
   const size_t smem = (a.rows_in_smem ? (size_t)a.n_pad * 8 : 0) + rest;
   if (cudaFuncSetAttribute(debug_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
