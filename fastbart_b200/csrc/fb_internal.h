@@ -11,6 +11,7 @@ constexpr int NMAX = 65536;    // rows per chain (src/bart_kernel.h:16)
 constexpr int MAXDEPTH = 24;   // src/bart_kernel.h:33
 constexpr int NB_MAX = 8;      // per-thread register bins of the fused pass; leaves beyond use shared atomics
 constexpr int MAX_THREADS = 512;
+constexpr int LEAF_STAT_WORDS = 96;   // per tree, 8-byte words: leaf sums of fx(w) [64], then row counts (int) [64]
 constexpr int MIN_THREADS = 64;   // warp 0 is the control warp; at least one row warp
 
 // Topology of one tree: 64 node slots (leaf values are kept apart, in th[]).  464 bytes, 16-byte multiple.
@@ -32,7 +33,7 @@ struct DChain {
   long long off_row;    // y, w, ybin, tm, rsave: [n_pad]
   long long off_q;      // codes [p][n_pad]
   long long off_leaf;   // leaf ids [m][n_pad]
-  long long off_tree;   // trees, th [m][64], s0 [m][64]
+  long long off_tree;   // trees, th [m][64], s0 [m][LEAF_STAT_WORDS]
   long long off_sigma;  // [nskip + ndpost]
   long long off_yhat;   // [ndpost][n]
   long long off_tout;   // [ndpost][m][64]
@@ -58,7 +59,7 @@ struct DBufs {
   float* wsave;
   uint8_t* leaf;
   DTree* trees;
-  long long* s0;
+  long long* s0;                   // per tree: leaf sums of fx(w) [64] (int64), then leaf row counts [64] (int32)
   float* th;
   double* tm;
   double* sigma_out;
@@ -73,8 +74,10 @@ struct DBufs {
 };
 
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem);
-int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, void* stream);
-int sampler_max_grid(int threads, size_t smem, int device);
+// groups of 4 rows per row thread held in registers (1, 2, 4, 8), or 0 when the rows stream from L2 in the pass
+int sampler_gmax(int threads, int n_pad_max);
+int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, void* stream);
+int sampler_max_grid(int threads, size_t smem, int device, int gmax);
 
 // Per-tree pass on explicit state (diagnostics / parity tests): one CTA.
 struct DPassArgs {

@@ -89,7 +89,7 @@ fb_status dalloc(T** p, size_t count) {
 
 struct fb_batch {
   int device = 0, nchains = 0, nskip = 0, ndpost = 0;
-  int threads = 256, grid = 0, spl = 0, launches = 0;
+  int threads = 256, grid = 0, spl = 0, launches = 0, gmax = 0;
   size_t smem = 0;
   std::vector<DChain> hch;
   std::vector<int> order;
@@ -177,9 +177,10 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   size_t smem = sampler_smem_bytes(T, m_max, n_pad_max, 1);
   if (smem > (size_t)optin) { rows_in_smem = 0; smem = sampler_smem_bytes(T, m_max, n_pad_max, 0); }
   if (smem > (size_t)optin) { delete b; return fail(FB_ERR_LIMIT, "shared memory %zu exceeds %d", smem, optin); }
-  const int maxgrid = sampler_max_grid(T, smem, opt->device);
+  const int gmax = sampler_gmax(T, n_pad_max);
+  const int maxgrid = sampler_max_grid(T, smem, opt->device, gmax);
   if (maxgrid <= 0) { delete b; return fail(FB_ERR_CUDA, "sampler kernel cannot be resident with %zu bytes of shared memory", smem); }
-  b->threads = T; b->smem = smem; b->grid = std::min(nchains, maxgrid);
+  b->threads = T; b->smem = smem; b->grid = std::min(nchains, maxgrid); b->gmax = gmax;
   b->spl = opt->sweeps_per_launch > 0 ? opt->sweeps_per_launch : S;
   b->launches = (S + b->spl - 1) / b->spl;
 
@@ -197,7 +198,7 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   fb_status s = FB_OK;
   if ((s = A(&dch, nchains)) || (s = A(&dst, nchains)) || (s = A(&dq, b->qbytes)) || (s = A(&dyin, b->rows)) ||
       (s = A(&dyw, b->rows)) || (s = A(&dw, b->rows)) || (s = A(&dyb, b->rows)) || (s = A(&drs, b->rows)) || (s = A(&dws, b->rows)) ||
-      (s = A(&dleaf, b->leafbytes)) || (s = A(&dtr, b->ntrees)) || (s = A(&ds0, b->ntrees * NODES)) ||
+      (s = A(&dleaf, b->leafbytes)) || (s = A(&dtr, b->ntrees)) || (s = A(&ds0, b->ntrees * LEAF_STAT_WORDS)) ||
       (s = A(&dth, b->ntrees * NODES)) || (s = A(&dtm, b->rows)) || (s = A(&dsig, b->nsig)) ||
       (s = A(&dyh, b->nyhat)) || (s = A(&dto, b->ntout)) || (s = A(&dord, nchains)) || (s = A(&dqueue, 1))) {
     delete b;
@@ -242,7 +243,7 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
   const int S = b->nskip + b->ndpost;
   for (int it0 = 0; it0 < S; it0 += b->spl) {
     const int it1 = std::min(S, it0 + b->spl);
-    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, stream) != 0)
+    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, b->gmax, stream) != 0)
       return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   return FB_OK;

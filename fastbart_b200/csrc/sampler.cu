@@ -8,15 +8,23 @@
 //     order, largest n*ntree first), so chains of uneven n, p and ntree share one launch.
 //   * Warp 0 is the control warp; warps 1.. stream the rows.  Rows live in shared memory (FP32 residual r and the
 //     weight pre-scaled to fixed point, ws = w * 2^S, one float4 per group of 4 rows); leaf ids [ntree][n] and
-//     cutpoint codes [p][n] stream from L2 as one 32-bit word per group.
-//   * Per sweep: (1) all proposals are drawn in parallel, one thread per tree (a proposal depends only on its own
-//     tree and on counter-based random numbers); (2) for each tree j the row warps make ONE fused pass that applies
-//     tree j-1's accepted move (leaf ids updated four at a time with byte-SIMD compares, r -= delta from a 64-entry
-//     table) and accumulates tree j's per-leaf sum of fx(w*R) into per-thread shared-memory bins plus the birth split
-//     sums, all exact int64 (order independent, hence bit-exact); warp sums use redux.sync on three 21-bit limbs.
-//     Meanwhile the control warp prefetches tree j's topology (cp.async) and draws the leaf-mu normals of every slot
-//     that can be a leaf after the move.  Then the control warp runs Metropolis-Hastings, the tree update and the mu
-//     draws in FP64, lanes in parallel; (3) an end-of-sweep pass refreshes every row's fit as an FP64 tree-order sum
+//     cutpoint codes [p][n] stream from L2 as one 32-bit word per group.  Each row thread owns fixed groups and keeps
+//     their leaf ids and codes in registers: the words it needs for the next tree are loaded at the end of the
+//     current pass, so the loads overlap the control phase instead of delaying the next pass.
+//   * Per tree step j, two phases separated by barriers:
+//     A. the row warps make ONE fused pass that applies tree j-1's accepted move (leaf ids updated four at a time
+//        with byte-SIMD compares, r -= delta from a 64-entry table) and accumulates tree j's per-leaf sum of
+//        fx(w*R) in per-thread register bins (1, 2, 4 or 8, by the tree's leaf count) plus the birth split sums,
+//        all exact int64 (order independent, hence bit-exact).  After a barrier every warp forms one CTA total from the per-thread partials (coalesced
+//        shared loads, then a warp sum by redux.sync on three 21-bit limbs).
+//        Meanwhile the control warp writes tree j-1's topology update back to global memory and fetches tree j+1
+//        (cp.async).
+//     B. 64 threads, one per node slot, decide Metropolis-Hastings (warps 0 and 1 each evaluate the three log
+//        marginal likelihoods on lanes 0..2) and draw the new leaf values in FP64; they publish the apply deltas of
+//        the move and tree j+1's leaf table for the next pass.
+//   * Per sweep: all proposals are drawn at the start, one thread per tree (a proposal depends only on its own tree
+//     and on counter-based random numbers), together with the leaf-mu normals of every slot that can be a leaf of
+//     that tree after its move, and the goodvar counts of new leaves; at the end one pass refreshes every row's fit as an FP64 tree-order sum
 //     of leaf values (which is also the draw's yhat.train), redraws the probit latent z, and sums rss for sigma.
 //   * sum(w) per leaf is maintained exactly per tree (root: all rows; birth: the split sums; death: the two
 //     children), so the pass reduces only sum(fx(w * R)).
@@ -33,16 +41,24 @@
 namespace fb {
 
 constexpr int NBS = NB_MAX;   // per-thread shared-memory bins (compact leaf index < NBS); beyond: shared atomics
+constexpr int TOT = 16;       // CTA totals per tree: [0, NBS) leaf sums, NBS.. sL0 sL1 nL
+constexpr int NSPLIT = 3;     // split partials per row thread: sum fx(w), sum fx(w*R), count of the left child
+constexpr int LST = LEAF_STAT_WORDS;
+constexpr int ZMAX = 16;      // leaf-mu normals drawn ahead per tree (candidate slots beyond are drawn in the step)
 
 struct Prop {                 // proposal of one tree for the current sweep
   double logpr, lu;
+  unsigned long long cand;    // slots that can be leaves after the move (normals drawn ahead, in slot order)
   uint8_t mode, nx, v, c, l, r, pad0, pad1;
 };
 struct Masks { unsigned long long used, leaf; };
 struct Ctl {                  // CTA-shared control state
-  int pmode, pnx, pv, pc, pL, pR, pl, pr;   // tree j-1's applied move
+  int pmode, pnx, pv, pc, pL, pR, pl, pr;   // the last decided move (tree j during pass j+1)
   float DL, DR;                             // apply deltas of a birth's left / right rows
-  int nleaf;                                // leaves of tree j
+  long long sL0, sR0;                       // leaf weight sums of a birth's children
+  int nL, nR;                               // and their row counts
+  unsigned long long used, leaf;            // node masks of the tree after the move
+  int nleaf[2];                             // leaves of the tree whose table is in buffer 0 / 1
   int births, deaths, caps, rtcaps;
   int chain;
   double sigma;
@@ -68,112 +84,170 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 __device__ __forceinline__ uint32_t bcast4(int v) { return (uint32_t)v * 0x01010101u; }
 __device__ __forceinline__ int byte_of(uint32_t w, int e) { return (int)((w >> (8 * e)) & 255u); }
+__device__ __forceinline__ uint32_t ld_u32(const uint8_t* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
 // ------------------------------------------------------------------------------------------------ fused row pass
 struct PassU {
-  uint8_t* leaf_prev;
-  const uint8_t* leaf_cur;
-  const uint8_t* qprev;
-  const uint8_t* qcur;
+  uint8_t* leaf_prev;         // tree j-1 leaf ids (written back after the move)
+  const uint8_t* leaf_cur;    // tree j leaf ids
+  const uint8_t* qprev;       // codes of tree j-1's split variable
+  const uint8_t* qcur;        // codes of tree j's proposed split variable
+  const uint8_t* leaf_next;   // tree j+1 leaf ids (prefetch), or null
+  const uint8_t* qnext;       // codes of tree j+1's proposed split variable (prefetch), or null
   float* r;
   const float* ws;
-  const float* D;       // [64] apply deltas
-  const float2* tc;     // [64] {theta of tree j, compact leaf index as int bits}
-  long long* bins;      // [NBS][RT]
-  unsigned long long* ovb;
-  long long* s1c;       // [NBS] CTA totals of sum fx(w*R) per compact leaf
-  long long* split;     // [6] CTA totals sL0 sL1 sR0 sR1 nL nR
+  const float* D;             // [64] apply deltas
+  const float2* tc;           // [64] {theta of tree j, compact leaf index as int bits}
+  long long* bins;            // [NBS + NSPLIT][RT]: per-thread leaf sums, then split partials
+  unsigned long long* ovb;    // [64] leaves with compact index >= NBS
+  long long* tot;             // [TOT] CTA totals
   float DL, DR;
-  int n, ngroups, rt, RT, rwarp, nleaf;
+  int n, ngroups, rt, RT, nleaf;
   int apply, pmode, pnx, pc, pL, pR, pl, pr;
   int cmode, cnx, cc;
 };
 
-// Applies tree j-1's move to its leaf ids and to r, accumulates tree j's statistics (src/bart_kernel.cpp:164-201
-// semantics; gpu/bart_batch.cu:184-227 fixed-point semantics).  Called by the row warps only; every lane of a row
-// warp must call it (warp-wide reductions at the end).
-__device__ __forceinline__ void pass_rows(const PassU& P) {
-  const int lane = threadIdx.x & 31;
-  long long* mybins = P.bins + P.rt;
-  long long sl0 = 0, sl1 = 0, sr0 = 0, sr1 = 0;
-  int nl = 0, nr = 0;
-  const uint32_t pnx4 = bcast4(P.pnx), pc4 = bcast4(P.pc), pl4 = bcast4(P.pl), pr4 = bcast4(P.pr);
-  const uint32_t pL4 = bcast4(P.pL), pR4 = bcast4(P.pR), cnx4 = bcast4(P.cnx), cc4 = bcast4(P.cc);
-  for (int g = P.rt; g < P.ngroups; g += P.RT) {
-    const uint32_t lc4 = *reinterpret_cast<const uint32_t*>(P.leaf_cur + 4 * g);
-    const uint32_t lp4 = P.apply ? *reinterpret_cast<const uint32_t*>(P.leaf_prev + 4 * g) : 0u;
-    const uint32_t qp4 = (P.apply && P.pmode == 1) ? __ldg(reinterpret_cast<const uint32_t*>(P.qprev + 4 * g)) : 0u;
-    const uint32_t qc4 = P.cmode == 1 ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
-    const float4 r4 = reinterpret_cast<const float4*>(P.r)[g];
-    const float4 w4 = reinterpret_cast<const float4*>(P.ws)[g];
-    float rr[4] = {r4.x, r4.y, r4.z, r4.w};
-    const float ww[4] = {w4.x, w4.y, w4.z, w4.w};
-    if (P.apply) {
-      uint32_t lpn = lp4, mv = 0u, side = 0u;
-      if (P.pmode == 1) {
-        mv = __vcmpeq4(lp4, pnx4);
-        side = __vcmpleu4(qp4, pc4);                       // 0xFF where the row goes left
-        lpn = (lp4 & ~mv) | (mv & ((side & pL4) | (~side & pR4)));
-      } else if (P.pmode == 2) {
-        const uint32_t md = __vcmpeq4(lp4, pl4) | __vcmpeq4(lp4, pr4);
-        lpn = (lp4 & ~md) | (md & pnx4);                   // death deltas come from the table
-      }
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        float delta = P.D[byte_of(lp4, e)];
-        if (byte_of(mv, e)) delta = byte_of(side, e) ? P.DL : P.DR;
-        rr[e] = __fsub_rn(rr[e], delta);
-      }
-      reinterpret_cast<float4*>(P.r)[g] = make_float4(rr[0], rr[1], rr[2], rr[3]);
-      if (lpn != lp4) *reinterpret_cast<uint32_t*>(P.leaf_prev + 4 * g) = lpn;
+// The words of one group that the pass of tree j consumes: leaf ids of trees j-1 (lp) and j (lc), codes of the
+// previous (qp) and current (qc) split variables.
+struct GroupWords { uint32_t lp, lc, qp, qc; };
+
+// One group of 4 rows: apply tree j-1's move, accumulate tree j's statistics (src/bart_kernel.cpp:164-201
+// semantics; gpu/bart_batch.cu:184-227 fixed-point semantics).  Leaf sums go to this thread's column of the bin
+// matrix (compact leaf index < NBS; conflict-free, RT * 8 bytes is a multiple of the 32 banks), leaves beyond to
+// shared atomics.  For a birth proposal only the left child's sums and count are accumulated: the right child's
+// follow from the node's totals.
+__device__ __forceinline__ void pass_group(const PassU& P, int g, const GroupWords& W, long long& sl0, long long& sl1,
+                                           int& nl) {
+  float* __restrict__ rp = P.r;
+  const float* __restrict__ wp = P.ws;
+  const float* __restrict__ Dp = P.D;
+  const float2* __restrict__ tcp = P.tc;
+  const float4 r4 = reinterpret_cast<const float4*>(rp)[g];
+  const float4 w4 = reinterpret_cast<const float4*>(wp)[g];
+  float rr[4] = {r4.x, r4.y, r4.z, r4.w};
+  const float ww[4] = {w4.x, w4.y, w4.z, w4.w};
+  if (P.apply) {
+    uint32_t lpn = W.lp, mv = 0u, side = 0u;
+    if (P.pmode == 1) {
+      mv = __vcmpeq4(W.lp, bcast4(P.pnx));
+      side = __vcmpleu4(W.qp, bcast4(P.pc));                // 0xFF where the row goes left
+      lpn = (W.lp & ~mv) | (mv & ((side & bcast4(P.pL)) | (~side & bcast4(P.pR))));
+    } else if (P.pmode == 2) {
+      const uint32_t md = __vcmpeq4(W.lp, bcast4(P.pl)) | __vcmpeq4(W.lp, bcast4(P.pr));
+      lpn = (W.lp & ~md) | (md & bcast4(P.pnx));          // death deltas come from the table
     }
-    long long wr[4];
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      const int lc = byte_of(lc4, e);
-      const float2 t = P.tc[lc];
-      const float R = __fadd_rn(rr[e], t.x);
-      wr[e] = __float2ll_rn(__fmul_rn(ww[e], R));
-      const int ci = __float_as_int(t.y);
-      if (ci < NBS) mybins[ci * P.RT] += wr[e];
-      else atomicAdd(&P.ovb[lc], (unsigned long long)wr[e]);
+      float delta = Dp[byte_of(W.lp, e)];
+      if (byte_of(mv, e)) delta = byte_of(side, e) ? P.DL : P.DR;
+      rr[e] = __fsub_rn(rr[e], delta);
     }
-    if (P.cmode == 1) {
-      uint32_t inx = __vcmpeq4(lc4, cnx4);
-      const int left = P.n - 4 * g;
-      if (left < 4) inx &= (1u << (8 * (left > 0 ? left : 0))) - 1u;   // rows beyond n are padding
-      if (inx) {
-        const uint32_t lq = __vcmpleu4(qc4, cc4);
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          if (byte_of(inx, e)) {
-            const long long wfx = __float2ll_rn(ww[e]);
-            if (byte_of(lq, e)) { nl++; sl0 += wfx; sl1 += wr[e]; }
-            else { nr++; sr0 += wfx; sr1 += wr[e]; }
-          }
-        }
-      }
-    }
+    reinterpret_cast<float4*>(rp)[g] = make_float4(rr[0], rr[1], rr[2], rr[3]);
+    if (lpn != W.lp) *reinterpret_cast<uint32_t*>(P.leaf_prev + 4 * g) = lpn;
   }
-  // per-warp reductions of the private bins (reset for the next pass), then one shared atomic per warp and leaf into
-  // the CTA totals (integer adds: the order of the atomics does not matter)
-  const int nb = P.nleaf < NBS ? P.nleaf : NBS;
-  for (int b = 0; b < nb; b++) {
-    const long long v = mybins[b * P.RT];
-    mybins[b * P.RT] = 0;
-    const long long s = warp_sum64(v);
-    if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&P.s1c[b]), (unsigned long long)s);
-  }
+  // rows of a birth proposal's node that go left (padding rows beyond n excluded)
+  uint32_t inl = 0u;
   if (P.cmode == 1) {
-    const long long a0 = warp_sum64(sl0), a1 = warp_sum64(sl1), a2 = warp_sum64(sr0), a3 = warp_sum64(sr1);
-    const int c0 = __reduce_add_sync(0xffffffffu, nl), c1 = __reduce_add_sync(0xffffffffu, nr);
-    if (lane == 0) {
-      unsigned long long* sp = reinterpret_cast<unsigned long long*>(P.split);
-      atomicAdd(sp + 0, (unsigned long long)a0); atomicAdd(sp + 1, (unsigned long long)a1);
-      atomicAdd(sp + 2, (unsigned long long)a2); atomicAdd(sp + 3, (unsigned long long)a3);
-      atomicAdd(sp + 4, (unsigned long long)c0); atomicAdd(sp + 5, (unsigned long long)c1);
+    inl = __vcmpeq4(W.lc, bcast4(P.cnx)) & __vcmpleu4(W.qc, bcast4(P.cc));
+    const int left = P.n - 4 * g;
+    if (left < 4) inl &= (1u << (8 * (left > 0 ? left : 0))) - 1u;
+    nl += __popc(inl) >> 3;
+  }
+  long long* mybins = P.bins + P.rt;
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int lc = byte_of(W.lc, e);
+    const float2 t = tcp[lc];
+    const float R = __fadd_rn(rr[e], t.x);
+    const long long wr = __float2ll_rn(__fmul_rn(ww[e], R));
+    const int ci = __float_as_int(t.y);
+    if (ci < NBS) mybins[ci * P.RT] += wr;
+    else atomicAdd(&P.ovb[lc], (unsigned long long)wr);
+    if (byte_of(inl, e)) { sl0 += __float2ll_rn(ww[e]); sl1 += wr; }
+  }
+}
+
+// End of the pass: the split partials join this thread's column of the bin matrix (rows NBS..); the CTA totals are
+// formed afterwards by reduce_totals(), one warp per total.
+__device__ __forceinline__ void pass_store(const PassU& P, long long sl0, long long sl1, int nl) {
+  if (P.cmode == 1) {
+    long long* mybins = P.bins + P.rt;
+    mybins[(NBS + 0) * P.RT] = sl0; mybins[(NBS + 1) * P.RT] = sl1; mybins[(NBS + 2) * P.RT] = nl;
+  }
+}
+
+// CTA totals of one pass: warp w sums row w of the bin matrix over the RT row threads (lanes read consecutive
+// threads' partials, and clears the leaf rows for the next pass), then reduces across the warp.  Exact int64.  Called
+// by every warp of the CTA after the pass and a barrier.
+__device__ __forceinline__ void reduce_totals(long long* bins, int RT, int nleaf, int cmode, long long* tot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
+  const int nb = nleaf < NBS ? nleaf : NBS;
+  for (int row = warp; row < NBS + NSPLIT; row += NW) {
+    const bool leafrow = row < NBS;
+    if (leafrow ? row >= nb : cmode != 1) continue;
+    long long* br = bins + (long long)row * RT;
+    long long v = 0;
+    for (int k = lane; k < RT; k += 32) {
+      v += br[k];
+      if (leafrow) br[k] = 0;
+    }
+    const long long t = warp_sum64(v);
+    if (lane == 0) tot[row] = t;
+  }
+}
+
+// Pass with words streamed from L2 in the pass itself (any n).
+__device__ void pass_rows_stream(const PassU& P) {
+  long long sl0 = 0, sl1 = 0;
+  int nl = 0;
+  for (int g = P.rt; g < P.ngroups; g += P.RT) {
+    GroupWords W;
+    W.lc = ld_u32(P.leaf_cur + 4 * g);
+    W.lp = P.apply ? ld_u32(P.leaf_prev + 4 * g) : 0u;
+    W.qp = (P.apply && P.pmode == 1) ? __ldg(reinterpret_cast<const uint32_t*>(P.qprev + 4 * g)) : 0u;
+    W.qc = P.cmode == 1 ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
+    pass_group(P, g, W, sl0, sl1, nl);
+  }
+  pass_store(P, sl0, sl1, nl);
+}
+
+// Pass with register-held words (each row thread owns at most G groups).  lcr/qcr hold tree j-1's words on entry
+// (tree j's on exit); nlc/nqc hold tree j's prefetched words on entry (tree j+1's on exit).  first: tree 0 of a
+// sweep (no prefetch available, nothing to apply).
+template <int G>
+__device__ __forceinline__ void pass_rows_regs(const PassU& P, bool first, uint32_t (&lcr)[G], uint32_t (&qcr)[G],
+                                               uint32_t (&nlc)[G], uint32_t (&nqc)[G]) {
+  long long sl0 = 0, sl1 = 0;
+  int nl = 0;
+#pragma unroll
+  for (int k = 0; k < G; k++) {
+    const int g = P.rt + k * P.RT;
+    if (g < P.ngroups) {
+      GroupWords W;
+      if (first) {
+        W.lc = ld_u32(P.leaf_cur + 4 * g);
+        W.qc = P.cmode == 1 ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
+      } else {
+        W.lc = nlc[k];
+        W.qc = nqc[k];
+      }
+      W.lp = lcr[k];
+      W.qp = qcr[k];
+      pass_group(P, g, W, sl0, sl1, nl);
+      lcr[k] = W.lc;
+      qcr[k] = W.qc;
     }
   }
+  // the next tree's words: in flight while the control phase runs
+#pragma unroll
+  for (int k = 0; k < G; k++) {
+    const int g = P.rt + k * P.RT;
+    if (g < P.ngroups && P.leaf_next) {
+      nlc[k] = ld_u32(P.leaf_next + 4 * g);
+      nqc[k] = P.qnext ? __ldg(reinterpret_cast<const uint32_t*>(P.qnext + 4 * g)) : 0u;
+    }
+  }
+  pass_store(P, sl0, sl1, nl);
 }
 
 // ------------------------------------------------------------------------------------------------ tree helpers
@@ -207,6 +281,16 @@ __device__ int count_goodvars(const DTree* t, int x, const int* nc, int p) {   /
     g += (U >= L);
   }
   return g;
+}
+// goodvar count of node x, lanes of one warp over the predictors (p <= 32)
+__device__ __forceinline__ int count_goodvars_warp(const DTree* t, int x, const int* nc, int p, int lane) {
+  bool good = false;
+  if (lane < p) {
+    int L, U;
+    node_range(t, x, lane, nc[lane], L, U);
+    good = U >= L;
+  }
+  return __popc(__ballot_sync(0xffffffffu, good));
 }
 __device__ __noinline__ double lh(double b, double M, double t2) {   // src/bart_kernel.cpp:278
   const double k = b * t2 + 1.0;
@@ -276,6 +360,16 @@ __device__ Prop propose(DTree* t, const DChain& C, int j, int it, Masks& mk) {
     const fbm::U4 y = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_MH, C.seed);
     P.lu = fbm::fb_log(fbm::u32d(y.x));
   }
+  // every slot that can be a leaf after the move: the current leaves, the two slots a birth would take, the node a
+  // death would restore
+  unsigned long long cand = used & leafm;
+  if (P.mode == 1) {
+    const int L = first_free(used, -1), R = L >= 0 ? first_free(used, L) : -1;
+    if (L >= 0 && R >= 0) cand |= (1ull << L) | (1ull << R);
+  } else if (P.mode == 2) {
+    cand |= 1ull << P.nx;
+  }
+  P.cand = cand;
   return P;
 }
 
@@ -285,17 +379,15 @@ struct Smem {
   float* th;                    // [m][64]
   Prop* prop;                   // [m]
   Masks* masks;                 // [m]
-  DTree* tcur;                  // tree j (copy)
-  long long* s0cur;             // [64]
-  long long* s1;                // [64]
-  float* tho;                   // [64] leaf values of tree j before its mu draw
-  float* D;                     // [64] apply deltas of tree j-1's update
-  float2* tc;                   // [64] theta and compact leaf index of tree j
-  double* z;                    // [64] mu normals of tree j
-  long long* bins;              // [NBS][RT]
-  long long* s1c;               // [NBS]
-  long long* split;             // [8]
-  unsigned long long* ovb;      // [64]
+  DTree* tree;                  // [2] topology of trees j and j+1 (buffer j & 1)
+  long long* s0t;               // [2][LST] leaf statistics of the same trees (S0 [64], then row counts int [64])
+  float* D;                     // [64] apply deltas of the last decided move
+  float2* tc;                   // [2][64] theta and compact leaf index
+  double* z;                    // [64] mu normals of tree j beyond the first ZMAX candidates
+  double* zall;                 // [m][ZMAX] mu normals drawn ahead
+  long long* bins;              // [NBS + NSPLIT][RT]
+  long long* tot;               // [2][TOT]
+  unsigned long long* ovb;      // [2][64]
   long long* red;               // [NW]
   Ctl* ctl;
 };
@@ -310,23 +402,20 @@ __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_
   off[2] = o; o += align_up((size_t)m_max * NODES * 4, 16);                  // th
   off[3] = o; o += align_up((size_t)m_max * sizeof(Prop), 16);               // prop
   off[4] = o; o += align_up((size_t)m_max * sizeof(Masks), 16);              // masks
-  off[5] = o; o += align_up(sizeof(DTree), 16);                              // tcur
-  off[6] = o; o += NODES * 8;                                                // s0cur
-  off[7] = o; o += NODES * 8;                                                // s1
-  off[8] = o; o += NODES * 4;                                                // tho
-  off[9] = o; o += NODES * 4;                                                // D
-  off[10] = o; o += NODES * 8;                                               // tc
-  off[11] = o; o += NODES * 8;                                               // z
-  off[12] = o; o += (size_t)NBS * RT * 8;                                    // bins
-  off[13] = o; o += (size_t)NBS * 8;                                         // s1c
-  off[14] = o; o += 8 * 8;                                                   // split
-  off[15] = o; o += 0;                                                       // (unused)
-  off[16] = o; o += NODES * 8;                                               // ovb
-  off[17] = o; o += align_up((size_t)NW * 8, 16);                            // red
-  off[18] = o; o += align_up(sizeof(Ctl), 16);                               // ctl
+  off[5] = o; o += 2 * align_up(sizeof(DTree), 16);                          // tree[2]
+  off[6] = o; o += 2 * LST * 8;                                              // s0t[2]
+  off[7] = o; o += NODES * 4;                                                // D
+  off[8] = o; o += 2 * NODES * 8;                                            // tc[2]
+  off[9] = o; o += NODES * 8;                                                // z
+  off[10] = o; o += (size_t)(NBS + NSPLIT) * RT * 8;                         // bins (leaf rows, split rows)
+  off[11] = o; o += 2 * TOT * 8;                                             // tot[2]
+  off[12] = o; o += 2 * NODES * 8;                                           // ovb[2]
+  off[13] = o; o += align_up((size_t)NW * 8, 16);                            // red
+  off[14] = o; o += align_up(sizeof(Ctl), 16);                               // ctl
+  off[15] = o; o += (size_t)m_max * ZMAX * 8;                                // zall
   return o;
 }
-constexpr int NOFF = 19;
+constexpr int NOFF = 16;
 
 __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max, int rows_in_smem) {
   size_t off[NOFF];
@@ -337,19 +426,17 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.th = reinterpret_cast<float*>(base + off[2]);
   S.prop = reinterpret_cast<Prop*>(base + off[3]);
   S.masks = reinterpret_cast<Masks*>(base + off[4]);
-  S.tcur = reinterpret_cast<DTree*>(base + off[5]);
-  S.s0cur = reinterpret_cast<long long*>(base + off[6]);
-  S.s1 = reinterpret_cast<long long*>(base + off[7]);
-  S.tho = reinterpret_cast<float*>(base + off[8]);
-  S.D = reinterpret_cast<float*>(base + off[9]);
-  S.tc = reinterpret_cast<float2*>(base + off[10]);
-  S.z = reinterpret_cast<double*>(base + off[11]);
-  S.bins = reinterpret_cast<long long*>(base + off[12]);
-  S.s1c = reinterpret_cast<long long*>(base + off[13]);
-  S.split = reinterpret_cast<long long*>(base + off[14]);
-  S.ovb = reinterpret_cast<unsigned long long*>(base + off[16]);
-  S.red = reinterpret_cast<long long*>(base + off[17]);
-  S.ctl = reinterpret_cast<Ctl*>(base + off[18]);
+  S.tree = reinterpret_cast<DTree*>(base + off[5]);
+  S.s0t = reinterpret_cast<long long*>(base + off[6]);
+  S.D = reinterpret_cast<float*>(base + off[7]);
+  S.tc = reinterpret_cast<float2*>(base + off[8]);
+  S.z = reinterpret_cast<double*>(base + off[9]);
+  S.bins = reinterpret_cast<long long*>(base + off[10]);
+  S.tot = reinterpret_cast<long long*>(base + off[11]);
+  S.ovb = reinterpret_cast<unsigned long long*>(base + off[12]);
+  S.red = reinterpret_cast<long long*>(base + off[13]);
+  S.ctl = reinterpret_cast<Ctl*>(base + off[14]);
+  S.zall = reinterpret_cast<double*>(base + off[15]);
   return S;
 }
 
@@ -366,18 +453,58 @@ __device__ long long block_sum64(long long x, long long* red) {
   return t;
 }
 
-// theta / compact-index table of tree j (control warp)
-__device__ __forceinline__ void build_tc(const Smem& S, int j, int lane) {
+// theta / compact-index table of tree j into buffer j & 1 (one slot per thread: s = 0..63)
+__device__ __forceinline__ void build_tc_slot(const Smem& S, int j, int s) {
   const unsigned long long lm = S.masks[j].leaf & S.masks[j].used;
-  const float* thj = S.th + j * NODES;
-  for (int s = lane; s < NODES; s += 32) {
-    const int ci = ((lm >> s) & 1ull) ? __popcll(lm & ((1ull << s) - 1ull)) : 255;
-    S.tc[s] = make_float2(thj[s], __int_as_float(ci));
+  const int ci = ((lm >> s) & 1ull) ? __popcll(lm & ((1ull << s) - 1ull)) : 255;
+  S.tc[(j & 1) * NODES + s] = make_float2(S.th[j * NODES + s], __int_as_float(ci));
+  if (s == 0) S.ctl->nleaf[j & 1] = __popcll(lm);
+}
+
+// copy tree j (topology and leaf weight sums) from global memory into buffer j & 1 (control warp)
+__device__ __forceinline__ void fetch_tree(const Smem& S, const DTree* trees, const long long* s0g, int j, int lane) {
+  constexpr int TW = (int)(sizeof(DTree) / 16), SW = LST * 8 / 16;
+  unsigned char* td = reinterpret_cast<unsigned char*>(S.tree + (j & 1));
+  unsigned char* sd = reinterpret_cast<unsigned char*>(S.s0t + (j & 1) * LST);
+  for (int k = lane; k < TW + SW; k += 32) {
+    if (k < TW) cp_async16(td + 16 * k, reinterpret_cast<const unsigned char*>(trees + j) + 16 * k);
+    else cp_async16(sd + 16 * (k - TW), reinterpret_cast<const unsigned char*>(s0g + (long long)j * LST) + 16 * (k - TW));
   }
-  if (lane == 0) S.ctl->nleaf = __popcll(lm);
+}
+
+// apply the decided move of tree j (ctl) to its topology and leaf statistics in buffer j & 1 and write the tree back
+// (control warp)
+__device__ void commit_tree(const Smem& S, const DChain& C, DTree* trees, long long* s0g, int j, int lane) {
+  const Ctl& ctl = *S.ctl;
+  DTree* t = S.tree + (j & 1);
+  long long* s0 = S.s0t + (j & 1) * LST;
+  int* cnt = reinterpret_cast<int*>(s0 + NODES);
+  const int mode = ctl.pmode, nx = ctl.pnx;
+  if (lane == 0) {
+    if (mode == 1) {
+      const int L = ctl.pL, R = ctl.pR;
+      t->v[nx] = (uint8_t)ctl.pv; t->c[nx] = (uint8_t)ctl.pc; t->l[nx] = (uint8_t)L; t->r[nx] = (uint8_t)R;
+      t->par[L] = (uint8_t)nx; t->par[R] = (uint8_t)nx; t->l[L] = t->r[L] = t->l[R] = t->r[R] = 0;
+      t->d[L] = t->d[R] = (uint8_t)(t->d[nx] + 1);
+      t->ngv[L] = t->ngv[R] = 255;   // counted by the next sweep's proposal step
+      s0[L] = ctl.sL0; s0[R] = ctl.sR0; cnt[L] = ctl.nL; cnt[R] = ctl.nR;
+    } else if (mode == 2) {
+      const int l = ctl.pl, r = ctl.pr;
+      s0[nx] = s0[l] + s0[r]; cnt[nx] = cnt[l] + cnt[r];
+      t->l[nx] = 0; t->r[nx] = 0; t->v[nx] = 0; t->c[nx] = 0;
+    }
+    if (mode) { t->used = ctl.used; t->leaf = ctl.leaf; }
+  }
+  __syncwarp();
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(t);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(trees + j);
+  for (int k = lane; k < (int)(sizeof(DTree) / 4); k += 32) dst[k] = src[k];
+  for (int k = lane; k < LST; k += 32) s0g[(long long)j * LST + k] = s0[k];
+  __syncwarp();
 }
 
 // ------------------------------------------------------------------------------------------------ one chain
+template <int G>
 __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& S) {
   const DChain& C = B.chains[ci];
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -390,7 +517,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   const uint8_t* q = B.q + C.off_q;
   uint8_t* leaf = B.leaf + C.off_leaf;
   DTree* trees = B.trees + C.off_tree;
-  long long* s0g = B.s0 + C.off_tree * NODES;
+  long long* s0g = B.s0 + C.off_tree * LST;
   float* thg = B.th + C.off_tree * NODES;
   double* ywork = B.ywork + C.off_row;
   const float* wg = B.win + C.off_row;
@@ -401,6 +528,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   float* ws = B.rows_in_smem ? S.ws : wsg;
   Ctl& ctl = *S.ctl;
   DState& st = B.states[ci];
+  const bool regs = G > 0 && ngroups <= G * RT;   // register-held words for this chain
 
   // ---------------------------------------------------------------- chain start or resume
   if (tid == 0) {
@@ -408,10 +536,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     else { ctl.sigma = st.sigma; ctl.births = st.births; ctl.deaths = st.deaths; ctl.caps = st.caps; ctl.rtcaps = st.rtcaps; }
     ctl.pmode = 0;
   }
-  for (int k = tid; k < NBS * RT; k += T) S.bins[k] = 0;
-  for (int s = tid; s < NODES; s += T) S.ovb[s] = 0ull;
-  if (tid < NBS) S.s1c[tid] = 0;
-  if (tid < 8) S.split[tid] = 0;
+  for (int k = tid; k < (NBS + NSPLIT) * RT; k += T) S.bins[k] = 0;
   __syncthreads();
   for (int i = tid; i < n_pad; i += T) ws[i] = __fmul_rn(wg[i], scale);   // exact: power-of-two scaling
   if (it0 == 0) {
@@ -444,7 +569,13 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       else if (byte0 == 7 * NODES || byte0 == 7 * NODES + 8) val = 1u;
       reinterpret_cast<uint32_t*>(trees + j)[k % TWORDS] = val;
     }
-    for (int k = tid; k < m * NODES; k += T) s0g[k] = (k % NODES == 0) ? swt : 0ll;
+    for (int k = tid; k < m * LST; k += T) {   // root: all rows; counts are ints in words 64..95
+      const int w = k % LST;
+      long long v = 0;
+      if (w == 0) v = swt;
+      else if (w == NODES) v = (long long)(unsigned)n;   // cnt[0] = n (little endian: low half of word 64)
+      s0g[k] = v;
+    }
   } else {
     if (B.rows_in_smem)
       for (int i = tid; i < n_pad; i += T) S.r[i] = rg[i];
@@ -452,77 +583,104 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   }
   __syncthreads();
 
+  // words of the row thread's groups (register path)
+  uint32_t lcr[G > 0 ? G : 1], qcr[G > 0 ? G : 1], nlc[G > 0 ? G : 1], nqc[G > 0 ? G : 1];
+
   for (int it = it0; it < it1; it++) {
     const double inv_s2 = 1.0 / (ctl.sigma * ctl.sigma);
-    // ---------------------------------------------------------------- (1) proposals, one thread per tree
+    // ---------------------------------------------------------------- proposals, one thread per tree
     for (int j = tid; j < m; j += T) {
       Masks mk;
-      S.prop[j] = propose(trees + j, C, j, it, mk);
+      const Prop P = propose(trees + j, C, j, it, mk);
+      S.prop[j] = P;
       S.masks[j] = mk;
+      int k = 0;
+      for (unsigned long long cm = P.cand; cm && k < ZMAX; cm &= cm - 1ull, k++) {
+        const int sl = __ffsll((long long)cm) - 1;
+        S.zall[j * ZMAX + k] = fbm::fb_normal(seed, (uint32_t)sl << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
+      }
     }
+    for (int k = tid; k < 2 * TOT; k += T) S.tot[k] = 0;
+    for (int k = tid; k < 2 * NODES; k += T) S.ovb[k] = 0ull;
     __syncthreads();
     if (warp == 0) {
-      build_tc(S, 0, lane);
+      fetch_tree(S, trees, s0g, 0, lane);
+      if (m > 1) fetch_tree(S, trees, s0g, 1, lane);
+      build_tc_slot(S, 0, lane);
+      build_tc_slot(S, 0, lane + 32);
       if (lane == 0) ctl.pmode = 0;
+      cp_async_wait_all();
     }
     __syncthreads();
-    // ---------------------------------------------------------------- (2) trees
+    // ---------------------------------------------------------------- trees
     for (int j = 0; j < m; j++) {
       const Prop P = S.prop[j];
+      const int cur = j & 1;
+      // ------------------------------------------------------------ phase A: row pass | control prefetch
       if (warp > 0) {
         PassU U;
         U.leaf_prev = j > 0 ? leaf + (long long)(j - 1) * n_pad : nullptr;
         U.leaf_cur = leaf + (long long)j * n_pad;
         U.qprev = q + (long long)ctl.pv * n_pad;
         U.qcur = q + (long long)P.v * n_pad;
-        U.r = r; U.ws = ws; U.D = S.D; U.tc = S.tc; U.bins = S.bins; U.ovb = S.ovb;
-        U.s1c = S.s1c; U.split = S.split;
+        if (j + 1 < m) {
+          const Prop Pn = S.prop[j + 1];
+          U.leaf_next = leaf + (long long)(j + 1) * n_pad;
+          U.qnext = Pn.mode == 1 ? q + (long long)Pn.v * n_pad : nullptr;
+        } else {
+          U.leaf_next = nullptr;
+          U.qnext = nullptr;
+        }
+        U.r = r; U.ws = ws; U.D = S.D; U.tc = S.tc + cur * NODES; U.bins = S.bins; U.ovb = S.ovb + cur * NODES;
+        U.tot = S.tot + cur * TOT;
         U.DL = ctl.DL; U.DR = ctl.DR;
-        U.n = n; U.ngroups = ngroups; U.rt = tid - 32; U.RT = RT; U.rwarp = warp - 1; U.nleaf = ctl.nleaf;
+        U.n = n; U.ngroups = ngroups; U.rt = tid - 32; U.RT = RT; U.nleaf = ctl.nleaf[cur];
         U.apply = j > 0; U.pmode = ctl.pmode; U.pnx = ctl.pnx; U.pc = ctl.pc; U.pL = ctl.pL; U.pR = ctl.pR;
         U.pl = ctl.pl; U.pr = ctl.pr;
         U.cmode = P.mode; U.cnx = P.nx; U.cc = P.c;
-        pass_rows(U);
+        if constexpr (G > 0) {
+          if (regs) pass_rows_regs<G>(U, j == 0, lcr, qcr, nlc, nqc);
+          else pass_rows_stream(U);
+        } else {
+          pass_rows_stream(U);
+        }
       } else {
-        // control warp during the pass: prefetch tree j, draw the normals of every slot that can be a leaf after
-        // this step's move (current leaves, the two slots a birth would take, the node a death would restore)
-        constexpr int TW = (int)(sizeof(DTree) / 16), SW = NODES * 8 / 16;
-        for (int k = lane; k < TW + SW; k += 32) {
-          if (k < TW) cp_async16(reinterpret_cast<unsigned char*>(S.tcur) + 16 * k, reinterpret_cast<const unsigned char*>(trees + j) + 16 * k);
-          else cp_async16(reinterpret_cast<unsigned char*>(S.s0cur) + 16 * (k - TW), reinterpret_cast<const unsigned char*>(s0g + (long long)j * NODES) + 16 * (k - TW));
-        }
-        const Masks mk = S.masks[j];
-        unsigned long long cand = mk.leaf & mk.used;
-        if (P.mode == 1) {
-          const int L = first_free(mk.used, -1), R = L >= 0 ? first_free(mk.used, L) : -1;
-          if (L >= 0 && R >= 0) cand |= (1ull << L) | (1ull << R);
-        } else if (P.mode == 2) {
-          cand |= 1ull << P.nx;
-        }
-        for (int s = lane; s < NODES; s += 32)
-          if ((cand >> s) & 1ull) S.z[s] = fbm::fb_normal(seed, (uint32_t)s << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
+        // control warp: commit tree j-1, fetch tree j+1 into the freed buffer, draw the normals of every slot that
+        // can be a leaf of tree j after its move (current leaves, the two slots a birth would take, the node a death
+        // would restore)
+        if (j > 0) commit_tree(S, C, trees, s0g, j - 1, lane);
+        if (j + 1 < m && j > 0) fetch_tree(S, trees, s0g, j + 1, lane);
+        const unsigned long long cand = P.cand;
+        if (__popcll(cand) > ZMAX)
+          for (int s = lane; s < NODES; s += 32)
+            if (((cand >> s) & 1ull) && __popcll(cand & ((1ull << s) - 1ull)) >= ZMAX)
+              S.z[s] = fbm::fb_normal(seed, (uint32_t)s << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
         cp_async_wait_all();
       }
       __syncthreads();
-      // ---------------------------------------------------------------- control: MH, tree update, mu draws
-      if (warp == 0) {
-        const int nleaf = ctl.nleaf;
+      reduce_totals(S.bins, RT, ctl.nleaf[cur], P.mode, S.tot + cur * TOT);
+      __syncthreads();
+      // ------------------------------------------------------------ phase B: MH and leaf draws, one thread per slot
+      if (tid < NODES) {
+        const int s = tid;
         const Masks mk = S.masks[j];
-        unsigned long long used = mk.used, leafm = mk.leaf;
-        const unsigned long long lm0 = used & leafm;
-        for (int s = lane; s < NODES; s += 32) {
-          if ((lm0 >> s) & 1ull) {
-            const int ci2 = __float_as_int(S.tc[s].y);
-            S.s1[s] = ci2 < NBS ? S.s1c[ci2] : (long long)S.ovb[s];
-          }
-          if (nleaf > NBS) S.ovb[s] = 0ull;
+        const long long* tot = S.tot + cur * TOT;
+        const unsigned long long* ovb = S.ovb + cur * NODES;
+        const float2* tcj = S.tc + cur * NODES;
+        const long long* s0 = S.s0t + cur * LST;
+        const int* cnt = reinterpret_cast<const int*>(s0 + NODES);
+        float* thj = S.th + j * NODES;
+        auto s1of = [&](int slot) -> long long {
+          const int c = __float_as_int(tcj[slot].y);
+          return c < NBS ? tot[c] : (long long)ovb[slot];
+        };
+        // birth split: the left child's sums come from the pass, the right child's from the node's totals
+        long long sL0 = 0, sL1 = 0, sR0 = 0, sR1 = 0;
+        int nL = 0, nR = 0;
+        if (P.mode == 1) {
+          sL0 = tot[NBS + 0]; sL1 = tot[NBS + 1]; nL = (int)tot[NBS + 2];
+          sR0 = s0[P.nx] - sL0; sR1 = s1of(P.nx) - sL1; nR = cnt[P.nx] - nL;
         }
-        const long long sL0 = S.split[0], sL1 = S.split[1], sR0 = S.split[2], sR1 = S.split[3];
-        const int nL = (int)S.split[4], nR = (int)S.split[5];
-        __syncwarp();
-        if (lane < NBS) S.s1c[lane] = 0;
-        if (lane < 8) S.split[lane] = 0;
-        __syncwarp();
         bool eval = false;
         double bl = 0, Ml = 0, br = 0, Mr = 0;
         if (P.mode == 1 && nL >= 5 && nR >= 5) {
@@ -531,13 +689,13 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           br = (double)sR0 * sci * inv_s2; Mr = (double)sR1 * sci * inv_s2;
         } else if (P.mode == 2) {
           eval = true;
-          bl = (double)S.s0cur[P.l] * sci * inv_s2; Ml = (double)S.s1[P.l] * sci * inv_s2;
-          br = (double)S.s0cur[P.r] * sci * inv_s2; Mr = (double)S.s1[P.r] * sci * inv_s2;
+          bl = (double)s0[P.l] * sci * inv_s2; Ml = (double)s1of(P.l) * sci * inv_s2;
+          br = (double)s0[P.r] * sci * inv_s2; Mr = (double)s1of(P.r) * sci * inv_s2;
         }
         bool accept = false;
         if (eval) {
-          // lanes 0..2 evaluate the three log marginal likelihoods at one call site: birth (l, r, l+r), death
-          // (l+r, l, r), in the order the ratio adds them
+          // lanes 0..2 of each of the two warps evaluate the three log marginal likelihoods at one call site:
+          // birth (l, r, l+r), death (l+r, l, r), in the order the ratio adds them
           const int which = P.mode == 1 ? lane : (lane == 0 ? 2 : lane - 1);
           const double hb = which == 0 ? bl : (which == 1 ? br : bl + br);
           const double hM = which == 0 ? Ml : (which == 1 ? Mr : Ml + Mr);
@@ -549,76 +707,61 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           if (lalpha > 0) lalpha = 0;
           accept = P.lu < lalpha;
         }
-        int nmode = 0, L = 0, R = 0, l = 0, rr = 0;
-        DTree* t = S.tcur;
+        int nmode = 0, L = 0, R = 0;
+        bool cap = false;
+        unsigned long long used = mk.used, leafm = mk.leaf;
         if (accept && P.mode == 1) {
           L = first_free(used, -1);
           R = L >= 0 ? first_free(used, L) : -1;
-          if (L < 0 || R < 0) {
-            if (lane == 0) ctl.caps++;
-            L = R = 0;
-          } else {
-            const int nx = P.nx;
-            if (lane == 0) {
-              t->v[nx] = P.v; t->c[nx] = P.c; t->l[nx] = (uint8_t)L; t->r[nx] = (uint8_t)R;
-              t->par[L] = (uint8_t)nx; t->par[R] = (uint8_t)nx; t->l[L] = t->r[L] = t->l[R] = t->r[R] = 0;
-              t->d[L] = t->d[R] = (uint8_t)(t->d[nx] + 1);
-              t->ngv[L] = t->ngv[R] = 255;   // resolved by the next sweep's proposal step
-              S.s0cur[L] = sL0; S.s0cur[R] = sR0; S.s1[L] = sL1; S.s1[R] = sR1;
-              ctl.births++;
-            }
-            used |= (1ull << L) | (1ull << R);
-            leafm = (leafm & ~(1ull << nx)) | (1ull << L) | (1ull << R);
+          if (L < 0 || R < 0) { cap = true; L = R = 0; }
+          else {
             nmode = 1;
+            used |= (1ull << L) | (1ull << R);
+            leafm = (leafm & ~(1ull << P.nx)) | (1ull << L) | (1ull << R);
           }
         } else if (accept && P.mode == 2) {
-          const int nx = P.nx;
-          l = P.l; rr = P.r;
-          if (lane == 0) {
-            S.s0cur[nx] = S.s0cur[l] + S.s0cur[rr]; S.s1[nx] = S.s1[l] + S.s1[rr];
-            t->l[nx] = 0; t->r[nx] = 0; t->v[nx] = 0; t->c[nx] = 0;
-            ctl.deaths++;
-          }
-          used &= ~((1ull << l) | (1ull << rr));
-          leafm = (leafm & ~((1ull << l) | (1ull << rr))) | (1ull << nx);
           nmode = 2;
+          used &= ~((1ull << P.l) | (1ull << P.r));
+          leafm = (leafm & ~((1ull << P.l) | (1ull << P.r))) | (1ull << P.nx);
         }
-        if (lane == 0) { t->used = used; t->leaf = leafm; S.masks[j].used = used; S.masks[j].leaf = leafm; }
-        __syncwarp();
-        // leaf mu draws (DRMU), lanes in parallel over slots; apply deltas D[s] = new - old
-        const unsigned long long lm = used & leafm;
-        float* thj = S.th + j * NODES;
-        for (int s = lane; s < NODES; s += 32) {
-          const float old = thj[s];
-          S.tho[s] = old;
-          float nw = old;
-          if ((lm >> s) & 1ull) {
-            const double b = (double)S.s0cur[s] * sci * inv_s2, M = (double)S.s1[s] * sci * inv_s2;
-            nw = (float)(M / (a_prior + b) + S.z[s] / sqrt(a_prior + b));
-          }
+        // this thread's slot: new leaf value (DRMU) and apply delta
+        const unsigned long long lm0 = mk.used & mk.leaf, lm1 = used & leafm;
+        const float old = thj[s];
+        float nw = old;
+        if ((lm1 >> s) & 1ull) {
+          long long S0s, S1s;
+          if (nmode == 1 && s == L) { S0s = sL0; S1s = sL1; }
+          else if (nmode == 1 && s == R) { S0s = sR0; S1s = sR1; }
+          else if (nmode == 2 && s == P.nx) { S0s = s0[P.l] + s0[P.r]; S1s = s1of(P.l) + s1of(P.r); }
+          else { S0s = s0[s]; S1s = ((lm0 >> s) & 1ull) ? s1of(s) : 0ll; }
+          const double b = (double)S0s * sci * inv_s2, M = (double)S1s * sci * inv_s2;
+          const int zi = __popcll(P.cand & ((1ull << s) - 1ull));
+          const double z = zi < ZMAX ? S.zall[j * ZMAX + zi] : S.z[s];
+          nw = (float)(M / (a_prior + b) + z / sqrt(a_prior + b));
           thj[s] = nw;
-          S.D[s] = __fsub_rn(nw, old);
         }
-        __syncwarp();
-        if (lane == 0) {
-          float DL = 0.0f, DR = 0.0f;
-          if (nmode == 1) { DL = __fsub_rn(thj[L], S.tho[P.nx]); DR = __fsub_rn(thj[R], S.tho[P.nx]); }
-          else if (nmode == 2) { S.D[l] = __fsub_rn(thj[P.nx], S.tho[l]); S.D[rr] = __fsub_rn(thj[P.nx], S.tho[rr]); }
-          ctl.DL = DL; ctl.DR = DR;
-          ctl.pmode = nmode; ctl.pnx = P.nx; ctl.pv = P.v; ctl.pc = P.c; ctl.pL = L; ctl.pR = R; ctl.pl = l; ctl.pr = rr;
+        // leaf values of slots that stop being leaves do not change, so the reads below see old values
+        if (!(nmode == 2 && (s == P.l || s == P.r))) S.D[s] = __fsub_rn(nw, old);
+        if (nmode == 2 && s == P.nx) { S.D[P.l] = __fsub_rn(nw, thj[P.l]); S.D[P.r] = __fsub_rn(nw, thj[P.r]); }
+        if (nmode == 1 && s == L) ctl.DL = __fsub_rn(nw, thj[P.nx]);
+        if (nmode == 1 && s == R) ctl.DR = __fsub_rn(nw, thj[P.nx]);
+        if (s == 0) {
+          if (cap) ctl.caps++;
+          if (nmode == 1) ctl.births++;
+          if (nmode == 2) ctl.deaths++;
+          ctl.pmode = nmode; ctl.pnx = P.nx; ctl.pv = P.v; ctl.pc = P.c; ctl.pL = L; ctl.pR = R;
+          ctl.pl = P.l; ctl.pr = P.r; ctl.sL0 = sL0; ctl.sR0 = sR0; ctl.nL = nL; ctl.nR = nR;
+          ctl.used = used; ctl.leaf = leafm;
         }
-        // write tree j back
-        {
-          const uint32_t* src = reinterpret_cast<const uint32_t*>(t);
-          uint32_t* dst = reinterpret_cast<uint32_t*>(trees + j);
-          for (int k = lane; k < (int)(sizeof(DTree) / 4); k += 32) dst[k] = src[k];
-          for (int k = lane; k < NODES; k += 32) s0g[(long long)j * NODES + k] = S.s0cur[k];
-        }
-        if (j + 1 < m) build_tc(S, j + 1, lane);
+        // the next tree's table; its accumulators start at zero
+        if (j + 1 < m) build_tc_slot(S, j + 1, s);
+        S.ovb[(cur ^ 1) * NODES + s] = 0ull;
       }
       __syncthreads();
     }
-    // ---------------------------------------------------------------- (3) end of sweep
+    // ---------------------------------------------------------------- end of sweep
+    if (warp == 0) commit_tree(S, C, trees, s0g, m - 1, lane);
+    __syncthreads();
     const bool keep = it >= C.nskip;
     const int dr = it - C.nskip;
     int caps = 0;
@@ -630,7 +773,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       uint8_t* lp = leaf + (long long)(m - 1) * n_pad;
       const uint8_t* qp = q + (long long)ctl.pv * n_pad;
       for (int g = tid; g < ngroups; g += T) {
-        const uint32_t lp4 = *reinterpret_cast<const uint32_t*>(lp + 4 * g);
+        const uint32_t lp4 = ld_u32(lp + 4 * g);
         uint32_t lpn = lp4;
         if (pmode == 1) {
           const uint32_t mv = __vcmpeq4(lp4, pnx4), side = __vcmpleu4(__ldg(reinterpret_cast<const uint32_t*>(qp + 4 * g)), pc4);
@@ -646,7 +789,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         for (; jj + 16 <= m - 1; jj += 16) {
           uint32_t l4[16];
 #pragma unroll
-          for (int u = 0; u < 16; u++) l4[u] = *reinterpret_cast<const uint32_t*>(leaf + (long long)(jj + u) * n_pad + 4 * g);
+          for (int u = 0; u < 16; u++) l4[u] = ld_u32(leaf + (long long)(jj + u) * n_pad + 4 * g);
 #pragma unroll
           for (int u = 0; u < 16; u++) {
             const float* thj = S.th + (jj + u) * NODES;
@@ -655,7 +798,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           }
         }
         for (; jj < m; jj++) {
-          const uint32_t l4 = jj == m - 1 ? lpn : *reinterpret_cast<const uint32_t*>(leaf + (long long)jj * n_pad + 4 * g);
+          const uint32_t l4 = jj == m - 1 ? lpn : ld_u32(leaf + (long long)jj * n_pad + 4 * g);
           const float* thj = S.th + jj * NODES;
           f0 += (double)thj[l4 & 255u]; f1 += (double)thj[(l4 >> 8) & 255u];
           f2 += (double)thj[(l4 >> 16) & 255u]; f3 += (double)thj[l4 >> 24];
@@ -726,6 +869,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   __syncthreads();
 }
 
+template <int G>
 __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it0, int it1) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem);
@@ -735,8 +879,25 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it
     const int qi = S.ctl->chain;
     __syncthreads();
     if (qi >= B.nchains) break;
-    run_chain(B, B.order[qi], it0, it1, S);
+    run_chain<G>(B, B.order[qi], it0, it1, S);
   }
+}
+
+using KernelFn = void (*)(DBufs, int, int);
+static KernelFn kernel_for(int gmax) {
+  switch (gmax) {
+    case 1: return sampler_kernel<1>;
+    case 2: return sampler_kernel<2>;
+    case 4: return sampler_kernel<4>;
+    case 8: return sampler_kernel<8>;
+    default: return sampler_kernel<0>;
+  }
+}
+
+int sampler_gmax(int threads, int n_pad_max) {
+  const int RT = threads - 32;
+  const int g = (n_pad_max / 4 + RT - 1) / RT;
+  return g <= 1 ? 1 : g <= 2 ? 2 : g <= 4 ? 4 : g <= 8 ? 8 : 0;
 }
 
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem) {
@@ -744,25 +905,27 @@ size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_sme
   return smem_layout(threads, m_max, n_pad_max, rows_in_smem, off);
 }
 
-int sampler_max_grid(int threads, size_t smem, int device) {
+int sampler_max_grid(int threads, size_t smem, int device, int gmax) {
   int per_sm = 0, nsm = 0;
-  cudaFuncSetAttribute(sampler_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sampler_kernel, threads, smem) != cudaSuccess) return -1;
+  const KernelFn k = kernel_for(gmax);
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess) return -1;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
   return per_sm * nsm;
 }
 
-int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, void* stream) {
+int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (cudaFuncSetAttribute(sampler_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return -1;
+  const KernelFn k = kernel_for(gmax);
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
   if (cudaMemsetAsync(b.queue, 0, sizeof(int), s) != cudaSuccess) return -1;
-  sampler_kernel<<<grid, threads, smem, s>>>(b, it0, it1);
+  k<<<grid, threads, smem, s>>>(b, it0, it1);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 // ------------------------------------------------------------------------------------------------ diagnostics
-// One pass on explicit state, run by the same pass_rows() as the sampler: warp 0 builds the tables, warps 1.. stream.
+// One pass on explicit state, run by the same pass code as the sampler (streaming form): warp 0 builds the tables,
+// warps 1.. stream the rows.
 __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x, T = blockDim.x, RT = T - 32, lane = tid & 31;
@@ -773,20 +936,20 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
   p += rows_smem ? (size_t)a.n_pad * 8 : 0;
   float* D = reinterpret_cast<float*>(p); p += NODES * 4;
   float2* tc = reinterpret_cast<float2*>(p); p += NODES * 8;
-  long long* bins = reinterpret_cast<long long*>(p); p += (size_t)NBS * RT * 8;
-  long long* s1c = reinterpret_cast<long long*>(p); p += NBS * 8;
-  long long* split = reinterpret_cast<long long*>(p); p += 8 * 8;
+  long long* bins = reinterpret_cast<long long*>(p); p += (size_t)(NBS + NSPLIT) * RT * 8;
+  long long* tot = reinterpret_cast<long long*>(p); p += TOT * 8;
   unsigned long long* ovb = reinterpret_cast<unsigned long long*>(p); p += NODES * 8;
-  float* dlr = reinterpret_cast<float*>(p);
+  float* dlr = reinterpret_cast<float*>(p); p += 16;
+  unsigned long long* nodesum = reinterpret_cast<unsigned long long*>(p);   // sum fx(w), row count of the birth node
   const float scale = (float)pow2(a.fx_shift);
   for (int i = tid; i < a.n_pad; i += T) {
     if (rows_smem) r[i] = a.r[i];
     ws[i] = __fmul_rn(a.w[i], scale);
   }
-  for (int k = tid; k < NBS * RT; k += T) bins[k] = 0;
+  for (int k = tid; k < (NBS + NSPLIT) * RT; k += T) bins[k] = 0;
   for (int s = tid; s < NODES; s += T) ovb[s] = 0;
-  if (tid < NBS) s1c[tid] = 0;
-  if (tid < 8) split[tid] = 0;
+  if (tid < TOT) tot[tid] = 0;
+  if (tid < 2) nodesum[tid] = 0;
   if (tid < 32) {
     const unsigned long long lm = a.leafmask;
     for (int s = lane; s < NODES; s += 32) {
@@ -806,25 +969,44 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
   if (tid >= 32) {
     PassU U;
     U.leaf_prev = a.leaf_prev; U.leaf_cur = a.leaf_cur; U.qprev = a.qprev; U.qcur = a.qcur;
-    U.r = r; U.ws = ws; U.D = D; U.tc = tc; U.bins = bins; U.ovb = ovb; U.s1c = s1c; U.split = split;
+    U.leaf_next = nullptr; U.qnext = nullptr;
+    U.r = r; U.ws = ws; U.D = D; U.tc = tc; U.bins = bins; U.ovb = ovb; U.tot = tot;
     U.DL = dlr[0]; U.DR = dlr[1];
-    U.n = a.n; U.ngroups = a.n_pad / 4; U.rt = tid - 32; U.RT = RT; U.rwarp = (tid >> 5) - 1; U.nleaf = nleaf;
+    U.n = a.n; U.ngroups = a.n_pad / 4; U.rt = tid - 32; U.RT = RT; U.nleaf = nleaf;
     U.apply = a.apply; U.pmode = a.pmode; U.pnx = a.pnx; U.pc = a.pc; U.pL = a.pL; U.pR = a.pR; U.pl = a.pl; U.pr = a.pr;
     U.cmode = a.stats ? a.cmode : 0; U.cnx = a.cnx; U.cc = a.cc;
-    pass_rows(U);
+    pass_rows_stream(U);
   }
+  __syncthreads();
+  reduce_totals(bins, RT, nleaf, a.stats ? a.cmode : 0, tot);
   __syncthreads();
   for (int s = tid; s < NODES; s += T) {
     long long v = 0;
     if ((a.leafmask >> s) & 1ull) {
       const int ci = __float_as_int(tc[s].y);
-      v = ci < NBS ? s1c[ci] : (long long)ovb[s];
+      v = ci < NBS ? tot[ci] : (long long)ovb[s];
     }
     a.out[s] = v;
   }
+  // The sampler keeps each leaf's sum fx(w) and row count with its tree; here they are counted directly, and the
+  // right child's statistics follow from them as in the sampler.
+  const bool sp = a.stats && a.cmode == 1;
+  if (sp) {
+    long long s0 = 0, c = 0;
+    for (int i = tid; i < a.n; i += T)
+      if (a.leaf_cur[i] == a.cnx) { s0 += __float2ll_rn(ws[i]); c++; }
+    atomicAdd(&nodesum[0], (unsigned long long)s0);
+    atomicAdd(&nodesum[1], (unsigned long long)c);
+  }
+  __syncthreads();
   if (tid == 0) {
-    const bool sp = a.stats && a.cmode == 1;
-    for (int k = 0; k < 6; k++) a.out[NODES + k] = sp ? split[k] : 0;
+    for (int k = 0; k < 6; k++) a.out[NODES + k] = 0;
+    if (sp) {
+      const long long sL0 = tot[NBS + 0], sL1 = tot[NBS + 1], nL = tot[NBS + 2];
+      a.out[NODES + 0] = sL0; a.out[NODES + 1] = sL1;
+      a.out[NODES + 2] = (long long)nodesum[0] - sL0; a.out[NODES + 3] = a.out[a.cnx] - sL1;
+      a.out[NODES + 4] = nL; a.out[NODES + 5] = (long long)nodesum[1] - nL;
+    }
   }
   if (rows_smem)
     for (int i = tid; i < a.n_pad; i += T) a.r[i] = r[i];
@@ -832,7 +1014,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
 
 int launch_debug_pass(DPassArgs a, int threads, void* stream) {
   const int RT = threads - 32;
-  const size_t rest = NODES * 4 + NODES * 8 + (size_t)NBS * RT * 8 + NBS * 8 + 64 + NODES * 8 + 16;
+  const size_t rest = NODES * 4 + NODES * 8 + (size_t)(NBS + NSPLIT) * RT * 8 + TOT * 8 + NODES * 8 + 32;
   a.rows_in_smem = (size_t)a.n_pad * 8 + rest <= 200 * 1024;
   const size_t smem = (a.rows_in_smem ? (size_t)a.n_pad * 8 : 0) + rest;
   if (cudaFuncSetAttribute(debug_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
