@@ -18,7 +18,7 @@ FB_OK, FB_ERR_ARG, FB_ERR_LIMIT, FB_ERR_CUDA, FB_ERR_PARSE, FB_ERR_SHAPE, FB_ERR
 EXPORTS = ["fb_last_error", "fb_version", "fb_fit_batch", "fb_batch_create", "fb_batch_run", "fb_batch_sync",
            "fb_batch_download", "fb_batch_launch_info", "fb_batch_destroy", "fb_fbart", "fb_trees_text",
            "fb_varcount", "fb_compile_trees", "fb_compiled_info", "fb_compiled_arrays", "fb_compiled_free",
-           "fb_predict_draw", "fb_predict_draws_device", "fb_debug_tree_pass"]
+           "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass"]
 
 
 class FastbartError(RuntimeError):
@@ -94,6 +94,7 @@ def lib() -> C.CDLL:
         L.fb_compiled_free.restype = None
         L.fb_predict_draw.argtypes = [vp, vp, i, i, i, d, vp]
         L.fb_predict_draws_device.argtypes = [vp, vp, i, i, i, i, i, d, vp, i, vp]
+        L.fb_predict_draw_static.argtypes = [vp, vp, i, i, i, d, vp]
         L.fb_debug_tree_pass.argtypes = [C.POINTER(PassState), vp]
         for f in EXPORTS:
             if f not in ("fb_last_error", "fb_version", "fb_trees_text", "fb_batch_destroy", "fb_compiled_free"):

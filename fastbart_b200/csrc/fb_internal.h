@@ -105,6 +105,10 @@ struct DForest {
   const int* var; const int* child; const double* cut; const double* theta; const int* root;
   int ntree, ndpost, p, nnodes;
 };
+// fixed device scratch of the allocation-free predict call: n * (ncol + 1) doubles at most (8 MiB per device)
+constexpr size_t PREDICT_SCRATCH_DOUBLES = size_t(1) << 20;
+// 0: *ptr = the scratch's address on `device` (the current device); -1: CUDA error; -2: device ordinal not tracked
+int predict_scratch_address(int device, double** ptr);
 int launch_predict(const DForest& f, const double* x, int n, int ld, int draw0, int ndraws, double mu, double* out,
                    int ldo, void* stream);
 

@@ -608,6 +608,38 @@ fb_status fb_predict_draw(const fb_compiled* ct, const double* const* cols, int 
   return s;
 }
 
+fb_status fb_predict_draw_static(const fb_compiled* ct, const double* const* cols, int ncol, int n, int draw,
+                                 double mu, double* out) {
+  if (!ct) return fail(FB_ERR_ARG, "compiled trees are NULL");
+  if (ncol != ct->p) return fail(FB_ERR_SHAPE, "newdata has %d columns, the trees use %d", ncol, ct->p);
+  if (draw < 1 || draw > ct->ndpost) return fail(FB_ERR_RANGE, "draw %d out of range 1..%d", draw, ct->ndpost);
+  if (n <= 0) return FB_OK;
+  if (!cols || !out) return fail(FB_ERR_ARG, "cols and out are required");
+  const size_t need = (size_t)n * ((size_t)ncol + 1);
+  if (need > PREDICT_SCRATCH_DOUBLES)
+    return fail(FB_ERR_LIMIT,
+                "n * (ncol + 1) = %zu doubles exceeds the fixed device scratch of %zu doubles; split the rows over "
+                "several calls or use fb_predict_draw",
+                need, (size_t)PREDICT_SCRATCH_DOUBLES);
+  CK(cudaSetDevice(ct->device));
+  double* scr = nullptr;
+  const int rc = predict_scratch_address(ct->device, &scr);
+  if (rc == -2) return fail(FB_ERR_LIMIT, "device %d: the fixed scratch is tracked for devices 0..63", ct->device);
+  if (rc != 0)
+    return fail(FB_ERR_CUDA, "cannot resolve the fixed predict scratch on device %d: %s", ct->device,
+                cudaGetErrorString(cudaGetLastError()));
+  double* dx = scr;                        // [ncol][n]
+  double* dout = scr + (size_t)n * ncol;   // [n]
+  for (int v = 0; v < ncol; v++)
+    if (cudaMemcpy(dx + (size_t)v * n, cols[v], sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(FB_ERR_CUDA, "copy of column %d failed", v);
+  if (launch_predict(ct->forest(), dx, n, n, draw - 1, 1, mu, dout, n, nullptr) != 0)
+    return fail(FB_ERR_CUDA, "predict launch failed");
+  if (cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(FB_ERR_CUDA, "copy of the result failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return FB_OK;
+}
+
 // ------------------------------------------------------------------------------------------------ diagnostics
 fb_status fb_debug_tree_pass(const fb_pass_state* s, int64_t* out) {
   if (!s || !out || !s->r || !s->w || !s->tho || !s->thn || !s->thc) return fail(FB_ERR_ARG, "missing argument");

@@ -8,6 +8,9 @@
 // draw share them.  The grid's y dimension enumerates draws, so a bulk call (many draws) runs in one launch.
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "fb_internal.h"
 
 namespace fb {
@@ -44,6 +47,37 @@ int launch_predict(const DForest& f, const double* x, int n, int ld, int draw0, 
                                                                             out + (long long)d0 * ldo, ldo);
     if (cudaGetLastError() != cudaSuccess) return -1;
   }
+  return 0;
+}
+
+// Fixed device scratch of fb_predict_draw_static: the newdata columns and the result are staged here instead of in
+// device memory allocated per call.  It belongs to the library's module, so every device that loads the library
+// holds it until the process exits.  Nothing in it needs to start at zero: each call copies in all the columns it
+// reads, and the kernel writes every result it returns.
+static __device__ __align__(256) double g_predict_scratch[PREDICT_SCRATCH_DOUBLES];
+
+namespace {
+constexpr int kScratchDevices = 64;
+std::atomic<double*> g_scratch_addr[kScratchDevices];
+std::mutex g_scratch_mu;
+}  // namespace
+
+// Device address of the scratch on `device`, which must be the current device.  The first call on a device resolves
+// it (host code only knows the array's host-side stand-in); later calls return the cached address.
+int predict_scratch_address(int device, double** ptr) {
+  if (device < 0 || device >= kScratchDevices) return -2;
+  double* a = g_scratch_addr[device].load(std::memory_order_acquire);
+  if (!a) {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    a = g_scratch_addr[device].load(std::memory_order_relaxed);
+    if (!a) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_predict_scratch) != cudaSuccess || !p) return -1;
+      a = static_cast<double*>(p);
+      g_scratch_addr[device].store(a, std::memory_order_release);
+    }
+  }
+  *ptr = a;
   return 0;
 }
 

@@ -132,6 +132,20 @@ fb_status fb_predict_draw(const fb_compiled* ct, const double* const* cols, int 
  * values at out_dev + d*ldo, for draws draw0 .. draw0+ndraws-1 (1-based).  Enqueued on cuda_stream. */
 fb_status fb_predict_draws_device(const fb_compiled* ct, const double* x_dev, int ncol, int n, int ld, int draw0,
                                   int ndraws, double mu, double* out_dev, int ldo, void* cuda_stream);
+/* fb_predict_draw without any device allocation.  No counterpart in the reference (its predict_draw_cpp runs on the
+ * host).  Same arguments, results and errors as fb_predict_draw, which allocates and frees device buffers for the
+ * columns and the result on every call.  This form stages them in a fixed 8 MiB device array instead; every device
+ * that loads the library holds that array until the process exits.  It is meant for callers that cannot call
+ * cudaMalloc: a process whose device memory is already held by another framework's caching allocator or by a fixed
+ * budget, where a new allocation can fail, and latency-sensitive loops, where cudaFree synchronizes the whole device
+ * and stalls every other stream.
+ * Limit: n * (ncol + 1) <= 1048576 doubles; larger inputs fail with FB_ERR_LIMIT (split the rows over several calls).
+ * The first call on a device does the set-up: it looks up the array's device address with that device current.
+ * Make that first call before any stream capture.  Nothing in the array needs to start at zero, because each call
+ * copies in all its columns and the kernel writes every result.  All calls on a device share the one array, so calls
+ * that overlap on the GPU (from several host threads) race; serialize them. */
+fb_status fb_predict_draw_static(const fb_compiled* ct, const double* const* cols, int ncol, int n, int draw,
+                                 double mu, double* out);
 
 /* ------------------------------------------------------------------------------------------------ diagnostics */
 
