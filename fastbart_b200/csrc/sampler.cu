@@ -81,6 +81,8 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t bcast4(int v) { return (uint32_t)v * 0x01010101u; }
 __device__ __forceinline__ int byte_of(uint32_t w, int e) { return (int)((w >> (8 * e)) & 255u); }
@@ -461,7 +463,7 @@ __device__ __forceinline__ void build_tc_slot(const Smem& S, int j, int s) {
   if (s == 0) S.ctl->nleaf[j & 1] = __popcll(lm);
 }
 
-// copy tree j (topology and leaf weight sums) from global memory into buffer j & 1 (control warp)
+// copy tree j (topology and leaf statistics) from global memory into buffer j & 1 (control warp); one cp.async group
 __device__ __forceinline__ void fetch_tree(const Smem& S, const DTree* trees, const long long* s0g, int j, int lane) {
   constexpr int TW = (int)(sizeof(DTree) / 16), SW = LST * 8 / 16;
   unsigned char* td = reinterpret_cast<unsigned char*>(S.tree + (j & 1));
@@ -470,6 +472,7 @@ __device__ __forceinline__ void fetch_tree(const Smem& S, const DTree* trees, co
     if (k < TW) cp_async16(td + 16 * k, reinterpret_cast<const unsigned char*>(trees + j) + 16 * k);
     else cp_async16(sd + 16 * (k - TW), reinterpret_cast<const unsigned char*>(s0g + (long long)j * LST) + 16 * (k - TW));
   }
+  cp_async_commit();
 }
 
 // apply the decided move of tree j (ctl) to its topology and leaf statistics in buffer j & 1 and write the tree back
@@ -655,7 +658,9 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           for (int s = lane; s < NODES; s += 32)
             if (((cand >> s) & 1ull) && __popcll(cand & ((1ull << s) - 1ull)) >= ZMAX)
               S.z[s] = fbm::fb_normal(seed, (uint32_t)s << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
-        cp_async_wait_all();
+        // tree j's copy (issued one step earlier) must have landed before phase B; tree j+1's may stay in flight
+        if (j + 1 < m && j > 0) cp_async_wait_prev();
+        else cp_async_wait_all();
       }
       __syncthreads();
       reduce_totals(S.bins, RT, ctl.nleaf[cur], P.mode, S.tot + cur * TOT);
