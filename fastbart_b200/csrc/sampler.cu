@@ -14,9 +14,10 @@
 //   * Per tree step j, two phases separated by barriers:
 //     A. the row warps make ONE fused pass that applies tree j-1's accepted move (leaf ids updated four at a time
 //        with byte-SIMD compares, r -= delta from a 64-entry table) and accumulates tree j's per-leaf sum of
-//        fx(w*R) in per-thread register bins (1, 2, 4 or 8, by the tree's leaf count) plus the birth split sums,
-//        all exact int64 (order independent, hence bit-exact).  After a barrier every warp forms one CTA total from the per-thread partials (coalesced
-//        shared loads, then a warp sum by redux.sync on three 21-bit limbs).
+//        fx(w*R) in per-thread shared-memory bins (one column of the bin matrix per row thread; leaves beyond the
+//        8th by shared atomics) plus the left child's sums and count of a birth proposal, all exact int64 (order
+//        independent, hence bit-exact).  After a barrier every warp forms one CTA total from the per-thread
+//        partials (coalesced shared loads, then a warp sum by redux.sync on three 21-bit limbs).
 //        Meanwhile the control warp writes tree j-1's topology update back to global memory and fetches tree j+1
 //        (cp.async).
 //     B. 64 threads, one per node slot, decide Metropolis-Hastings (warps 0 and 1 each evaluate the three log
@@ -26,8 +27,9 @@
 //     and on counter-based random numbers), together with the leaf-mu normals of every slot that can be a leaf of
 //     that tree after its move, and the goodvar counts of new leaves; at the end one pass refreshes every row's fit as an FP64 tree-order sum
 //     of leaf values (which is also the draw's yhat.train), redraws the probit latent z, and sums rss for sigma.
-//   * sum(w) per leaf is maintained exactly per tree (root: all rows; birth: the split sums; death: the two
-//     children), so the pass reduces only sum(fx(w * R)).
+//   * sum(fx(w)) and the row count of every leaf are kept exactly with each tree (root: all rows; birth: the split
+//     sums; death: the two children), so the pass reduces only sum(fx(w * R)) per leaf, and a birth's right child
+//     follows from its node's totals minus the left child's.
 //   * Random numbers: Philox4x32-10 keyed by the chain seed, counter = (draw index, tree or row, sweep, purpose).
 //   * All control arithmetic is IEEE FP64 through fb_math.cuh; the file is compiled with -fmad=false.  The oracle's
 //     DEV mode (oracle/fb_oracle.c) restates exactly this arithmetic on the CPU.
