@@ -260,6 +260,14 @@ def compile_trees(fit: BartFit, device: int = 0) -> CompiledTrees:
                          device)
 
 
+def predict_draws_device(ct: CompiledTrees, x_ptr: int, ncol: int, n: int, ld: int, draw0: int, ndraws: int,
+                         out_ptr: int, ldo: int, stream: int = 0) -> None:
+    """Bulk predict_draw on device memory (fb_predict_draws_device): column v of x at x_ptr + 8*v*ld, draw
+    draw0 + d (1-based) written to out_ptr + 8*d*ldo; enqueued on `stream` (a CUDA stream handle, 0 = default)."""
+    check(_lib.lib().fb_predict_draws_device(ct.handle(), x_ptr, int(ncol), int(n), int(ld), int(draw0), int(ndraws),
+                                             ct.mu, out_ptr, int(ldo), stream or None))
+
+
 def predict_draw(ct: CompiledTrees, newdata, m: int) -> np.ndarray:
     """predict_draw() of R/predict_draw.R:13-18: f (+ mu) of posterior draw m (1-based) on the rows of newdata."""
     X = np.asarray(newdata, dtype=np.float64)

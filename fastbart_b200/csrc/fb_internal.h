@@ -101,8 +101,20 @@ struct DPassArgs {
 int launch_debug_pass(DPassArgs a, int threads, void* stream);
 
 // Evaluator (predict_draw) on device.
+// One node of the tiled evaluator's packed layout (16 bytes, one load per step).  Internal node: v = cut, children at
+// child and child + 1, split variable var.  Leaf: v = leaf value, child = its own index, var = p (a column that is
+// -inf in the evaluator's tile, so the step x >= v never leaves the leaf).
+struct PNode { double v; int child; int var; };
+static_assert(sizeof(PNode) == 16, "PNode layout");
 struct DForest {
   const int* var; const int* child; const double* cut; const double* theta; const int* root;
+  const PNode* nodes;
+  const uint8_t* gdepth;   // [ndpost][ceil(ntree / 4)] deepest leaf of each group of 4 consecutive trees
+  // code-compare layout (null when not applicable): nodes packed in 32 bits, relative to their draw's first node
+  // (child | var << 16 | c << 24; leaves point to themselves with c = 255), and the cutpoints of every predictor
+  // (cuts[cutoff[v] .. cutoff[v + 1]), strictly increasing)
+  const uint32_t* n32; const double* cuts; const int* cutoff;
+  int maxnd;               // most nodes of one draw
   int ntree, ndpost, p, nnodes;
 };
 // fixed device scratch of the allocation-free predict call: n * (ncol + 1) doubles at most (8 MiB per device)

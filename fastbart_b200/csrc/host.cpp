@@ -414,20 +414,28 @@ fb_status fb_fbart(const int* q, int n, int p, const double* y, const double* wt
 // ------------------------------------------------------------------------------------------------ evaluator
 struct fb_compiled {
   int device = 0, ndpost = 0, ntree = 0, p = 0;
-  std::vector<int> var, child, root;
+  std::vector<int> var, child, root, cidx;
   std::vector<double> cut, theta;
   int* dvar = nullptr; int* dchild = nullptr; int* droot = nullptr;
   double* dcut = nullptr; double* dtheta = nullptr;
+  PNode* dnodes = nullptr;
+  uint8_t* dgdep = nullptr;
+  uint32_t* dn32 = nullptr;     // code-compare layout (null when the cutpoints do not allow it)
+  double* dcutflat = nullptr;
+  int* dcutoff = nullptr;
+  int maxnd = 0;
   ~fb_compiled() {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(device);
-    cudaFree(dvar); cudaFree(dchild); cudaFree(droot); cudaFree(dcut); cudaFree(dtheta);
+    cudaFree(dvar); cudaFree(dchild); cudaFree(droot); cudaFree(dcut); cudaFree(dtheta); cudaFree(dnodes); cudaFree(dgdep);
+    cudaFree(dn32); cudaFree(dcutflat); cudaFree(dcutoff);
     cudaSetDevice(cur);
   }
   DForest forest() const {
     DForest f;
-    f.var = dvar; f.child = dchild; f.cut = dcut; f.theta = dtheta; f.root = droot;
+    f.var = dvar; f.child = dchild; f.cut = dcut; f.theta = dtheta; f.root = droot; f.nodes = dnodes; f.gdepth = dgdep;
+    f.n32 = dn32; f.cuts = dcutflat; f.cutoff = dcutoff; f.maxnd = maxnd;
     f.ntree = ntree; f.ndpost = ndpost; f.p = p; f.nnodes = (int)var.size();
     return f;
   }
@@ -508,6 +516,7 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
     slot.assign(1, (int)ct->var.size());
     ct->root[(size_t)t] = slot[0];
     ct->var.push_back(0); ct->child.push_back(-1); ct->cut.push_back(0.0); ct->theta.push_back(0.0);
+    ct->cidx.push_back(0);
     for (size_t h = 0; h < qk.size(); h++) {
       const int k = qk[h], me = slot[h];
       ct->theta[me] = th[k];
@@ -515,13 +524,16 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
       if (L != pos.end()) {
         auto R = pos.find(2 * nid[k] + 1);
         if (R == pos.end()) { delete ct; return fail(FB_ERR_PARSE, "tree %lld: node %llu has one child", t, nid[k]); }
-        if (v[k] < 0 || v[k] >= ncol || c[k] < 0 || c[k] >= ncut[v[k]]) {
+        if (v[k] < 0 || v[k] >= ncol || v[k] >= p || c[k] < 0 || c[k] >= ncut[v[k]]) {
           delete ct;
           return fail(FB_ERR_PARSE, "tree %lld: split (v %d, c %d) is not a cutpoint", t, v[k], c[k]);
         }
         const int ch = (int)ct->var.size();
-        ct->var[me] = v[k]; ct->cut[me] = cutpoints[v[k]][c[k]]; ct->child[me] = ch;
-        for (int z = 0; z < 2; z++) { ct->var.push_back(0); ct->child.push_back(-1); ct->cut.push_back(0.0); ct->theta.push_back(0.0); }
+        ct->var[me] = v[k]; ct->cut[me] = cutpoints[v[k]][c[k]]; ct->child[me] = ch; ct->cidx[me] = c[k];
+        for (int z = 0; z < 2; z++) {
+          ct->var.push_back(0); ct->child.push_back(-1); ct->cut.push_back(0.0); ct->theta.push_back(0.0);
+          ct->cidx.push_back(0);
+        }
         qk.push_back(L->second); slot.push_back(ch);
         qk.push_back(R->second); slot.push_back(ch + 1);
       }
@@ -531,6 +543,80 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete ct; return fail(FB_ERR_CUDA, "no CUDA device is available"); }
   if (cudaSetDevice(device) != cudaSuccess) { delete ct; return fail(FB_ERR_CUDA, "cannot use device %d", device); }
   const size_t N = ct->var.size();
+  // packed nodes of the tiled evaluator: a leaf points to itself and tests the sentinel column p (all -inf), so a
+  // walk may take more steps than its depth; per draw and group of 4 trees, the deepest leaf's depth
+  std::vector<PNode> pn(N);
+  std::vector<int> dep(N, 0);
+  for (size_t k = 0; k < N; k++) {
+    const int ch = ct->child[k];
+    if (ch >= 0) { dep[ch] = dep[ch + 1] = dep[k] + 1; pn[k] = PNode{ct->cut[k], ch, ct->var[k]}; }
+    else pn[k] = PNode{ct->theta[k], (int)k, ct->p};
+  }
+  const int G = (ct->ntree + 3) / 4;
+  std::vector<uint8_t> gd((size_t)nd * G, 0);
+  int deepest = 0;
+  for (long long t = 0; t < nd * m; t++) {
+    const size_t b = (size_t)ct->root[(size_t)t], e = t + 1 < nd * m ? (size_t)ct->root[(size_t)t + 1] : N;
+    int mx = 0;
+    for (size_t k = b; k < e; k++) mx = std::max(mx, dep[k]);
+    deepest = std::max(deepest, mx);
+    uint8_t& g = gd[(size_t)(t / m) * G + (size_t)(t % m) / 4];
+    g = (uint8_t)std::min(255, std::max<int>(g, mx));
+  }
+  const bool tiled = deepest <= 255;   // deeper trees use only the streaming evaluator
+  // code-compare layout: x >= cutpoints[v][c]  <=>  code_v(x) > c, with code_v(x) the number of cutpoints of v that
+  // are <= x, exact when every cutpoint list is finite and strictly increasing; nodes then pack into 32 bits
+  // (child relative to the draw's first node | var << 16 | c << 24; a leaf points to itself with c = 255)
+  bool codes = tiled && p <= 255;
+  for (int u = 0; codes && u < ncol; u++) {
+    if (ncut[u] < 0 || ncut[u] > 255) codes = false;
+    for (int k = 0; codes && k < ncut[u]; k++)
+      if (!std::isfinite(cutpoints[u][k]) || (k > 0 && !(cutpoints[u][k - 1] < cutpoints[u][k]))) codes = false;
+  }
+  int maxnd = 0;
+  for (long long d = 0; d < nd; d++) {
+    const size_t b = (size_t)ct->root[(size_t)(d * m)], e = d + 1 < nd ? (size_t)ct->root[(size_t)((d + 1) * m)] : N;
+    maxnd = std::max(maxnd, (int)(e - b));
+  }
+  if (maxnd > 65535) codes = false;
+  std::vector<uint32_t> n32;
+  std::vector<double> cutflat;
+  std::vector<int> cutoff;
+  if (codes) {
+    n32.resize(N);
+    for (long long d = 0; d < nd; d++) {
+      const size_t b = (size_t)ct->root[(size_t)(d * m)], e = d + 1 < nd ? (size_t)ct->root[(size_t)((d + 1) * m)] : N;
+      for (size_t k = b; k < e; k++) {
+        const int ch = ct->child[k];
+        n32[k] = ch >= 0 ? (uint32_t)(ch - b) | (uint32_t)ct->var[k] << 16 | (uint32_t)ct->cidx[k] << 24
+                         : (uint32_t)(k - b) | 255u << 24;
+      }
+    }
+    cutoff.assign(1, 0);
+    for (int u = 0; u < (int)p; u++) {
+      const int nc = u < ncol ? ncut[u] : 0;
+      for (int k = 0; k < nc; k++) cutflat.push_back(cutpoints[u][k]);
+      cutoff.push_back((int)cutflat.size());
+    }
+    if (cutflat.empty()) cutflat.push_back(0.0);
+    ct->maxnd = maxnd;
+  }
+  if (tiled && (cudaMalloc(&ct->dnodes, N * sizeof(PNode)) != cudaSuccess ||
+                cudaMemcpy(ct->dnodes, pn.data(), N * sizeof(PNode), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMalloc(&ct->dgdep, gd.size()) != cudaSuccess ||
+                cudaMemcpy(ct->dgdep, gd.data(), gd.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
+    delete ct;
+    return fail(FB_ERR_CUDA, "cannot upload the compiled trees");
+  }
+  if (codes && (cudaMalloc(&ct->dn32, N * 4) != cudaSuccess ||
+                cudaMemcpy(ct->dn32, n32.data(), N * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMalloc(&ct->dcutflat, cutflat.size() * 8) != cudaSuccess ||
+                cudaMemcpy(ct->dcutflat, cutflat.data(), cutflat.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMalloc(&ct->dcutoff, cutoff.size() * 4) != cudaSuccess ||
+                cudaMemcpy(ct->dcutoff, cutoff.data(), cutoff.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)) {
+    delete ct;
+    return fail(FB_ERR_CUDA, "cannot upload the compiled trees");
+  }
   if (cudaMalloc(&ct->dvar, N * 4) != cudaSuccess || cudaMalloc(&ct->dchild, N * 4) != cudaSuccess ||
       cudaMalloc(&ct->dcut, N * 8) != cudaSuccess || cudaMalloc(&ct->dtheta, N * 8) != cudaSuccess ||
       cudaMalloc(&ct->droot, ct->root.size() * 4) != cudaSuccess ||

@@ -1,6 +1,8 @@
 // predict.cu -- predict_draw on the device (src/predict.cpp:49-73).
 //
-// Streaming evaluator: each thread owns one row of one draw and walks the draw's trees in order 1..ntree with the
+// Two evaluators with the same arithmetic.  The tiled one (predict_tiled_kernel, used when the columns of a row tile
+// fit in shared memory) is described at its definition.  The streaming one (predict_kernel, any p):
+// each thread owns one row of one draw and walks the draw's trees in order 1..ntree with the
 // branch-free step k = child[k] + (x[var[k]] >= cut[k]) over the breadth-first node arrays (children adjacent), adding
 // leaf values to an FP64 accumulator that starts at 0; mu is added last.  That is the reference's summation order, so
 // results are bit-identical to predict_draw_cpp / pwbart.  Rows of a warp are consecutive, so the x reads of each
@@ -8,6 +10,7 @@
 // draw share them.  The grid's y dimension enumerates draws, so a bulk call (many draws) runs in one launch.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -36,15 +39,195 @@ __global__ void __launch_bounds__(256) predict_kernel(DForest f, const double* _
   out[(long long)blockIdx.y * ldo + i] = __dadd_rn(acc, mu);
 }
 
+// Tiled evaluator for inputs whose columns fit in shared memory (p < PT_MAXP).  A CTA stages the x of PT_ROWS
+// consecutive rows in shared memory once ([p + 1][PT_ROWS], coalesced; column p is -inf), then evaluates a range of
+// draws for them, so x crosses HBM once however many draws are evaluated.  A thread walks four trees at a time with a
+// fixed number of steps, the deepest leaf of the four (leaves loop on themselves, see PNode): no data-dependent
+// branches, and the four node chains overlap.  Leaf values are added in tree order, so the FP64 sum is the same
+// sequence of additions as the one-tree-at-a-time loop of src/predict.cpp:62-70.
+constexpr int PT_ROWS = 128;
+constexpr int PT_MAXP = 96;
+
+struct NodeReg { double v; int child, var; };
+
+__device__ __forceinline__ NodeReg load_node(const PNode* __restrict__ nodes, int k) {
+  const double2 q = __ldg(reinterpret_cast<const double2*>(nodes + k));
+  return NodeReg{q.x, __double2loint(q.y), __double2hiint(q.y)};
+}
+__device__ __forceinline__ void step(NodeReg& a, const PNode* __restrict__ nodes, const double* xr) {
+  a = load_node(nodes, a.child + (xr[a.var * PT_ROWS] >= a.v ? 1 : 0));
+}
+
+__global__ void __launch_bounds__(PT_ROWS) predict_tiled_kernel(DForest f, const double* __restrict__ x, int n, int ld,
+                                                                int draw0, int ndraws, int dpc, double mu,
+                                                                double* __restrict__ out, int ldo) {
+  extern __shared__ double xs[];   // [p + 1][PT_ROWS]
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x * PT_ROWS + tid;
+  for (int v = 0; v < f.p; v++) xs[v * PT_ROWS + tid] = i < n ? x[(long long)v * ld + i] : 0.0;
+  xs[f.p * PT_ROWS + tid] = -__longlong_as_double(0x7FF0000000000000LL);
+  __syncthreads();
+  if (i >= n) return;
+  const double* xr = xs + tid;
+  const PNode* __restrict__ nodes = f.nodes;
+  const int m = f.ntree, G = (m + 3) / 4, m4 = m & ~3;
+  const int d0 = blockIdx.y * dpc, d1 = min(ndraws, d0 + dpc);
+  for (int d = d0; d < d1; d++) {
+    const int* __restrict__ root = f.root + (long long)(draw0 + d) * m;
+    const uint8_t* __restrict__ gdep = f.gdepth + (long long)(draw0 + d) * G;
+    double acc = 0.0;
+    for (int t = 0; t < m4; t += 4) {
+      NodeReg a = load_node(nodes, __ldg(root + t)), b = load_node(nodes, __ldg(root + t + 1));
+      NodeReg c = load_node(nodes, __ldg(root + t + 2)), e = load_node(nodes, __ldg(root + t + 3));
+      const int depth = __ldg(gdep + (t >> 2));
+      for (int s = 0; s < depth; s++) {
+        step(a, nodes, xr);
+        step(b, nodes, xr);
+        step(c, nodes, xr);
+        step(e, nodes, xr);
+      }
+      acc = __dadd_rn(acc, a.v);
+      acc = __dadd_rn(acc, b.v);
+      acc = __dadd_rn(acc, c.v);
+      acc = __dadd_rn(acc, e.v);
+    }
+    if (m4 < m) {
+      const int depth = __ldg(gdep + (m4 >> 2));
+      for (int t = m4; t < m; t++) {
+        NodeReg a = load_node(nodes, __ldg(root + t));
+        for (int s = 0; s < depth; s++) step(a, nodes, xr);
+        acc = __dadd_rn(acc, a.v);
+      }
+    }
+    out[(long long)d * ldo + i] = __dadd_rn(acc, mu);
+  }
+}
+
+// Code-compare evaluator, the default when the cutpoints allow it (DForest::n32).  A CTA of PC_ROWS threads (one row
+// each) first turns its rows' x into cutpoint codes, code_v(x) = number of cutpoints of v that are <= x (binary
+// search; NaN gives 0), kept in shared memory as bytes [p][PC_ROWS]: then x >= cut[v][c] is code_v(x) > c exactly.
+// For each draw of its range it stages that draw's packed nodes (4 bytes each) and leaf values in shared memory, and
+// every thread walks four trees at a time for the group's fixed depth (leaves loop on themselves): per step one
+// broadcast node load and one byte load, both from shared memory.  Leaf values are added in tree order, the same
+// FP64 additions as src/predict.cpp:62-70.
+constexpr int PC_ROWS = 256;
+
+__device__ __forceinline__ int cstep(int k, const uint32_t* nd, const uint8_t* cr) {
+  const uint32_t w = nd[k];
+  return (int)(w & 0xFFFFu) + (cr[((w >> 16) & 0xFFu) * PC_ROWS] > (w >> 24) ? 1 : 0);
+}
+
+__global__ void __launch_bounds__(PC_ROWS) predict_codes_kernel(DForest f, const double* __restrict__ x, int n, int ld,
+                                                                int draw0, int ndraws, int dpc, double mu,
+                                                                double* __restrict__ out, int ldo, int ncodes) {
+  extern __shared__ __align__(16) unsigned char pc_smem[];
+  double* th_s = reinterpret_cast<double*>(pc_smem);                   // [maxnd]
+  uint32_t* nd_s = reinterpret_cast<uint32_t*>(th_s + f.maxnd);       // [maxnd]
+  uint8_t* code_s = reinterpret_cast<uint8_t*>(nd_s + f.maxnd);        // [ncodes][PC_ROWS]
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x * PC_ROWS + tid;
+  const bool live = i < n;
+  for (int v = 0; v < ncodes; v++) {
+    int lo = 0;
+    if (live) {
+      const double xv = x[(long long)v * ld + i];
+      const double* __restrict__ cv = f.cuts + f.cutoff[v];
+      int hi = f.cutoff[v + 1] - f.cutoff[v];
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(cv + mid) <= xv) lo = mid + 1;
+        else hi = mid;
+      }
+    }
+    code_s[v * PC_ROWS + tid] = (uint8_t)lo;
+  }
+  const uint8_t* cr = code_s + tid;
+  const int m = f.ntree, G = (m + 3) / 4, m4 = m & ~3;
+  const long long ntot = (long long)f.ndpost * m;
+  const int d0 = blockIdx.y * dpc, d1 = min(ndraws, d0 + dpc);
+  for (int d = d0; d < d1; d++) {
+    const long long t0 = (long long)(draw0 + d) * m;
+    const int base = __ldg(f.root + t0);
+    const int cnt = (t0 + m < ntot ? __ldg(f.root + t0 + m) : f.nnodes) - base;
+    __syncthreads();   // the previous draw's nodes are no longer read
+    for (int k = tid; k < cnt; k += PC_ROWS) {
+      nd_s[k] = __ldg(f.n32 + base + k);
+      th_s[k] = __ldg(f.theta + base + k);
+    }
+    __syncthreads();
+    if (!live) continue;
+    const int* __restrict__ root = f.root + t0;
+    const uint8_t* __restrict__ gdep = f.gdepth + (long long)(draw0 + d) * G;
+    double acc = 0.0;
+    for (int t = 0; t < m4; t += 4) {
+      int a = __ldg(root + t) - base, b = __ldg(root + t + 1) - base;
+      int c = __ldg(root + t + 2) - base, e = __ldg(root + t + 3) - base;
+      const int depth = __ldg(gdep + (t >> 2));
+      for (int s = 0; s < depth; s++) {
+        a = cstep(a, nd_s, cr);
+        b = cstep(b, nd_s, cr);
+        c = cstep(c, nd_s, cr);
+        e = cstep(e, nd_s, cr);
+      }
+      acc = __dadd_rn(acc, th_s[a]);
+      acc = __dadd_rn(acc, th_s[b]);
+      acc = __dadd_rn(acc, th_s[c]);
+      acc = __dadd_rn(acc, th_s[e]);
+    }
+    if (m4 < m) {
+      const int depth = __ldg(gdep + (m4 >> 2));
+      for (int t = m4; t < m; t++) {
+        int a = __ldg(root + t) - base;
+        for (int s = 0; s < depth; s++) a = cstep(a, nd_s, cr);
+        acc = __dadd_rn(acc, th_s[a]);
+      }
+    }
+    out[(long long)d * ldo + i] = __dadd_rn(acc, mu);
+  }
+}
+
 int launch_predict(const DForest& f, const double* x, int n, int ld, int draw0, int ndraws, double mu, double* out,
                    int ldo, void* stream) {
   if (n <= 0 || ndraws <= 0) return 0;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t csmem = (size_t)f.maxnd * 12 + (size_t)f.p * PC_ROWS;
+  if (f.n32 && f.gdepth && csmem <= 160 * 1024) {
+    const int tiles = (n + PC_ROWS - 1) / PC_ROWS;
+    // enough CTAs for every SM (8 per SM), each taking a contiguous range of draws
+    const long long target = 8ll * nsm;
+    const int chunks = (int)std::min<long long>(ndraws, std::max<long long>(1, (target + tiles - 1) / tiles));
+    const int dpc = (ndraws + chunks - 1) / chunks;
+    const int ny = (ndraws + dpc - 1) / dpc;
+    if (csmem > 48 * 1024 &&
+        cudaFuncSetAttribute(predict_codes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem) !=
+            cudaSuccess)
+      return -1;
+    predict_codes_kernel<<<dim3(tiles, ny), PC_ROWS, csmem, st>>>(f, x, n, ld, draw0, ndraws, dpc, mu, out, ldo,
+                                                                  f.p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  }
+  if (f.p < PT_MAXP && f.nodes && f.gdepth) {
+    const int tiles = (n + PT_ROWS - 1) / PT_ROWS;
+    // enough CTAs for every SM (16 per SM), each taking a contiguous range of draws
+    const long long target = 16ll * nsm;
+    const int chunks = (int)std::min<long long>(ndraws, std::max<long long>(1, (target + tiles - 1) / tiles));
+    const int dpc = (ndraws + chunks - 1) / chunks;
+    const int ny = (ndraws + dpc - 1) / dpc;
+    const size_t smem = (size_t)(f.p + 1) * PT_ROWS * sizeof(double);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(predict_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+      return -1;
+    predict_tiled_kernel<<<dim3(tiles, ny), PT_ROWS, smem, st>>>(f, x, n, ld, draw0, ndraws, dpc, mu, out, ldo);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  }
   const int T = 256;
   for (int d0 = 0; d0 < ndraws; d0 += 65535) {
     const int nd = ndraws - d0 < 65535 ? ndraws - d0 : 65535;
     dim3 grid((n + T - 1) / T, nd);
-    predict_kernel<<<grid, T, 0, reinterpret_cast<cudaStream_t>(stream)>>>(f, x, n, ld, draw0 + d0, mu,
-                                                                            out + (long long)d0 * ldo, ldo);
+    predict_kernel<<<grid, T, 0, st>>>(f, x, n, ld, draw0 + d0, mu, out + (long long)d0 * ldo, ldo);
     if (cudaGetLastError() != cudaSuccess) return -1;
   }
   return 0;

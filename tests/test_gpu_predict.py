@@ -53,3 +53,62 @@ def test_fpbart_object():
     ct = F.compile_trees(fit)
     f = F.predict_draw(ct, x, 3)
     assert np.max(np.abs(f - fit["yhat.train"][2])) < 1e-8
+
+
+def _random_forest(rng, ndpost, ntree, p, ncut, max_depth=4):
+    """Packed trees (src/bart_kernel.cpp:559-571 format) with random splits on p predictors."""
+    trees = np.zeros((ndpost, ntree, 64), dtype=np.uint64)
+    for d in range(ndpost):
+        for t in range(ntree):
+            slots = [255] * 64                       # v per slot; 255 = unused
+            words = [0] * 64
+            free = list(range(1, 64))
+
+            def grow(s, depth):
+                if depth < max_depth and rng.random() < 0.6 and len(free) >= 2:
+                    l, r = free.pop(0), free.pop(0)
+                    v, c = int(rng.integers(p)), int(rng.integers(ncut))
+                    words[s] = v | (c << 8) | (l << 16) | (r << 24)
+                    slots[s] = v
+                    grow(l, depth + 1)
+                    grow(r, depth + 1)
+                else:
+                    th = np.float32(rng.normal(0, 0.3)).view(np.uint32)
+                    words[s] = int(th) << 32
+                    slots[s] = 0
+            grow(0, 0)
+            for s in range(64):
+                trees[d, t, s] = np.uint64(words[s] if slots[s] != 255 else 255)
+    return trees
+
+
+@pytest.mark.parametrize("p, n, ndraws, dup", [(3, 1, 3, False), (5, 333, 7, False), (95, 300, 4, False),
+                                                (120, 129, 2, False), (5, 333, 7, True), (95, 300, 4, True),
+                                                (96, 300, 4, True)])
+def test_bulk_predict_bit_exact_all_evaluators(orc, p, n, ndraws, dup):
+    """Strictly increasing cutpoints run the code-compare evaluator; a repeated cutpoint (dup) forces the FP64
+    comparisons: the tiled evaluator for p < 96, the streaming one beyond.  Ragged row tiles, several draws, x values
+    that sit exactly on cutpoints."""
+    import torch
+    rng = np.random.default_rng(p * 1000 + n)
+    ncut = 20
+    cps = [np.sort(rng.random(ncut)) for _ in range(p)]
+    if dup:
+        cps[0][1] = cps[0][0]
+    trees = _random_forest(rng, ndraws, 37, p, ncut)
+    text = orc.trees_text(trees, p)
+    ct = F.CompiledTrees(text, cps, mu=0.25)
+    ref = orc.compile_trees(text, cps)
+    x = rng.random((n, p))
+    for v in range(p):   # some values exactly on a cutpoint (x >= cut goes right)
+        hit = rng.random(n) < 0.2
+        x[hit, v] = cps[v][rng.integers(0, ncut, hit.sum())]
+    xd = torch.tensor(np.ascontiguousarray(x.T), device="cuda")
+    out = torch.full((ndraws, n), float("nan"), dtype=torch.float64, device="cuda")
+    F.predict_draws_device(ct, xd.data_ptr(), p, n, n, 1, ndraws, out.data_ptr(), n)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    for d in range(ndraws):
+        o = orc.predict_draw(ref, [x[:, v] for v in range(p)], d + 1, 0.25)
+        assert np.array_equal(got[d], o), d
+        assert np.array_equal(F.predict_draw(ct, x, d + 1), o)
