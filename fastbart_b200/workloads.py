@@ -11,6 +11,7 @@ shipped, so these generators stand in for them with the same shapes, sizes and v
                     x 16 multinomial bootstrap resamples; half U(0,1) and half integer 0..9 columns;
                     y = linear term on 4 columns + sin(pi xa xb) + N(0, .5^2); w ~ Gamma(4, 4); ntree 200
   friedman_large    n 65,536, p 32, numcut 255, Friedman-5 on x1..x5 + N(0,1), 16 chains
+  random_forest     posterior draws of trees grown from BART's tree prior (packed node format), for bulk predict
 """
 from __future__ import annotations
 
@@ -134,4 +135,36 @@ def friedman_large(nchains=16, n=65536, p=32, seed=0, **kw) -> list:
         kw2.setdefault("seed", 777 + c)
         kw2.setdefault("numcut", 255)
         out.append(fwbart_chain(x, y, None, **kw2))
+    return out
+
+
+def random_forest(ndpost: int, ntree: int, p: int, ncut, seed=0, base=0.95, power=2.0, sd=0.3,
+                  max_depth=6) -> np.ndarray:
+    """Packed trees [ndpost][ntree][64] (src/bart_kernel.cpp:559-571 format: v | c<<8 | l<<16 | r<<24 |
+    float_bits(theta)<<32, v = 255 for unused slots) grown from BART's tree prior: a node at depth d splits with
+    probability base / (1 + d)^power, on a uniform predictor and cut index; leaf values N(0, sd^2) as float.
+    `ncut` is the cutpoint count of every predictor (an int, or one per predictor)."""
+    rng = np.random.default_rng(seed)
+    nc = np.broadcast_to(np.asarray(ncut, dtype=np.int64), (p,))
+    out = np.full((ndpost, ntree, 64), 255, dtype=np.uint64)
+    for d in range(ndpost):
+        for t in range(ntree):
+            words = {}
+            free = list(range(1, 64))
+
+            def grow(s, depth):
+                if (depth < max_depth and len(free) >= 2 and p > 0
+                        and rng.random() < base / (1.0 + depth) ** power):
+                    l, r = free.pop(0), free.pop(0)
+                    v = int(rng.integers(p))
+                    c = int(rng.integers(max(int(nc[v]), 1)))
+                    words[s] = v | (c << 8) | (l << 16) | (r << 24)
+                    grow(l, depth + 1)
+                    grow(r, depth + 1)
+                else:
+                    th = int(np.float32(rng.normal(0.0, sd)).view(np.uint32))
+                    words[s] = th << 32
+            grow(0, 0)
+            for sl, wd in words.items():
+                out[d, t, sl] = np.uint64(wd)
     return out

@@ -55,33 +55,6 @@ def test_fpbart_object():
     assert np.max(np.abs(f - fit["yhat.train"][2])) < 1e-8
 
 
-def _random_forest(rng, ndpost, ntree, p, ncut, max_depth=4):
-    """Packed trees (src/bart_kernel.cpp:559-571 format) with random splits on p predictors."""
-    trees = np.zeros((ndpost, ntree, 64), dtype=np.uint64)
-    for d in range(ndpost):
-        for t in range(ntree):
-            slots = [255] * 64                       # v per slot; 255 = unused
-            words = [0] * 64
-            free = list(range(1, 64))
-
-            def grow(s, depth):
-                if depth < max_depth and rng.random() < 0.6 and len(free) >= 2:
-                    l, r = free.pop(0), free.pop(0)
-                    v, c = int(rng.integers(p)), int(rng.integers(ncut))
-                    words[s] = v | (c << 8) | (l << 16) | (r << 24)
-                    slots[s] = v
-                    grow(l, depth + 1)
-                    grow(r, depth + 1)
-                else:
-                    th = np.float32(rng.normal(0, 0.3)).view(np.uint32)
-                    words[s] = int(th) << 32
-                    slots[s] = 0
-            grow(0, 0)
-            for s in range(64):
-                trees[d, t, s] = np.uint64(words[s] if slots[s] != 255 else 255)
-    return trees
-
-
 @pytest.mark.parametrize("p, n, ndraws, dup", [(3, 1, 3, False), (5, 333, 7, False), (95, 300, 4, False),
                                                 (120, 129, 2, False), (5, 333, 7, True), (95, 300, 4, True),
                                                 (96, 300, 4, True)])
@@ -95,7 +68,7 @@ def test_bulk_predict_bit_exact_all_evaluators(orc, p, n, ndraws, dup):
     cps = [np.sort(rng.random(ncut)) for _ in range(p)]
     if dup:
         cps[0][1] = cps[0][0]
-    trees = _random_forest(rng, ndraws, 37, p, ncut)
+    trees = W.random_forest(ndraws, 37, p, ncut, seed=p + n, base=0.9, power=0.8, max_depth=5)
     text = orc.trees_text(trees, p)
     ct = F.CompiledTrees(text, cps, mu=0.25)
     ref = orc.compile_trees(text, cps)
