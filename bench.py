@@ -260,10 +260,8 @@ def bench_ours(args):
     clk = clocks.stop()
     step_ms = [a.elapsed_time(c) for a, c in evs]
     tot_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    from fastbart_b200 import shard
+    tot_ms = shard.max_over_ranks(tot_ms, device="cuda")
     units = len(chains) * S * args.steps * world
     value = units / (tot_ms / 1000.0)
 
@@ -326,13 +324,8 @@ def bench_ours(args):
             torch.cuda.synchronize()
             if k > 0:
                 times.append(time.perf_counter() - t1)
-        e2e_s = max(times) if world == 1 else times[-1]
-        if world > 1:
-            t = torch.tensor([sum(times)], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item()) / len(times)
-        else:
-            e2e_s = sum(times) / len(times)
+        from fastbart_b200 import shard
+        e2e_s = shard.max_over_ranks(sum(times), device="cuda") / len(times)
         e2e = {"value": len(chains) * S * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": len(times), "ms_per_step": 1000 * e2e_s,
                "api": "fb_fit_batch (host buffers; allocation, H2D, MCMC, D2H of sigma/yhat/yhat_mean/trees)"}
@@ -475,10 +468,8 @@ def bench_predict(args):
         dist.barrier()
     clk = clocks.stop()
     tot_ms = sum(a.elapsed_time(b) for a, b in evs)
-    if world > 1:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    from fastbart_b200 import shard
+    tot_ms = shard.max_over_ranks(tot_ms, device="cuda")
     per_s = tot_ms / 1000.0 / args.steps
     value = PRED_DRAWS * PRED_ROWS * world / per_s
     alg = PRED_P * PRED_ROWS * 8 + PRED_DRAWS * PRED_ROWS * 8 + ct.nnodes * 12
@@ -495,7 +486,7 @@ def bench_predict(args):
         t1 = time.perf_counter()
         for d in range(ed):
             F.predict_draw(ct, xh, 2 + d)
-        e2e_s = (time.perf_counter() - t1) / ed
+        e2e_s = shard.max_over_ranks((time.perf_counter() - t1) / ed, device="cuda")
         e2e = {"value": PRED_ROWS * world / e2e_s, "unit": PRED_UNIT, "h2d_bytes_per_step": PRED_P * PRED_ROWS * 8,
                "d2h_bytes_per_step": PRED_ROWS * 8, "steps": ed, "ms_per_step": 1000 * e2e_s,
                "api": "fb_predict_draw (one draw per call: host columns copied in, result copied out)"}
