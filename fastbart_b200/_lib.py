@@ -18,7 +18,21 @@ FB_OK, FB_ERR_ARG, FB_ERR_LIMIT, FB_ERR_CUDA, FB_ERR_PARSE, FB_ERR_SHAPE, FB_ERR
 EXPORTS = ["fb_last_error", "fb_version", "fb_fit_batch", "fb_batch_create", "fb_batch_run", "fb_batch_sync",
            "fb_batch_download", "fb_batch_launch_info", "fb_batch_destroy", "fb_fbart", "fb_trees_text",
            "fb_varcount", "fb_compile_trees", "fb_compiled_info", "fb_compiled_arrays", "fb_compiled_free",
-           "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass"]
+           "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass",
+           "fb_batch_set_proposal", "fb_batch_collect", "fb_batch_training_data", "fb_train_proposal",
+           "fb_mlp_loss_grad"]
+
+MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
+
+
+class ProposalModel(C.Structure):
+    _fields_ = [("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_void_p), ("mix", C.c_double)]
+
+
+class TrainOptions(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double), ("seed", C.c_uint64),
+                ("device", C.c_int)]
 
 
 class FastbartError(RuntimeError):
@@ -96,6 +110,13 @@ def lib() -> C.CDLL:
         L.fb_predict_draws_device.argtypes = [vp, vp, i, i, i, i, i, d, vp, i, vp]
         L.fb_predict_draw_static.argtypes = [vp, vp, i, i, i, d, vp]
         L.fb_debug_tree_pass.argtypes = [C.POINTER(PassState), vp]
+        L.fb_batch_set_proposal.argtypes = [vp, C.POINTER(ProposalModel)]
+        L.fb_batch_collect.argtypes = [vp, i]
+        L.fb_batch_training_data.argtypes = [vp, vp, vp, vp, i, C.POINTER(i)]
+        L.fb_train_proposal.argtypes = [vp, vp, vp, i, C.POINTER(TrainOptions), C.POINTER(ProposalModel),
+                                        vp, vp, vp, vp, vp, vp, vp]
+        L.fb_mlp_loss_grad.argtypes = [C.POINTER(ProposalModel), vp, vp, vp, i, i, C.POINTER(d), vp, vp, vp, vp, vp,
+                                       vp]
         for f in EXPORTS:
             if f not in ("fb_last_error", "fb_version", "fb_trees_text", "fb_batch_destroy", "fb_compiled_free"):
                 getattr(L, f).restype = C.c_int

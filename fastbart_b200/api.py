@@ -109,6 +109,30 @@ class Batch:
         check(_lib.lib().fb_batch_download(self._h, oarr))
         return [_collect(o, oarr[k]) for k, (o, _) in enumerate(outs)]
 
+    def set_proposal(self, model: dict | None):
+        """Learned split-variable proposal for the next runs (see `train_proposal`); None restores BART's."""
+        if model is None:
+            check(_lib.lib().fb_batch_set_proposal(self._h, None))
+            return
+        ms = _model_struct(model, self._keep)
+        check(_lib.lib().fb_batch_set_proposal(self._h, C.byref(ms)))
+
+    def collect(self, capacity: int):
+        """Collect the accepted births of the next runs as training examples (at most `capacity` per run)."""
+        self._cap = int(capacity)
+        check(_lib.lib().fb_batch_collect(self._h, self._cap))
+
+    def training_data(self) -> tuple[np.ndarray, np.ndarray, np.ndarray, int]:
+        """(x [k][98] float32, y [k] int32, mask [k] uint32, accepted births of the run) of the last run."""
+        cap = getattr(self, "_cap", 0)
+        x = np.zeros((max(cap, 1), _lib.MLP_IN), np.float32)
+        y = np.zeros(max(cap, 1), np.int32)
+        m = np.zeros(max(cap, 1), np.uint32)
+        cnt = C.c_int()
+        check(_lib.lib().fb_batch_training_data(self._h, ptr(x), ptr(y), ptr(m), cap, C.byref(cnt)))
+        k = min(cnt.value, cap)
+        return x[:k], y[:k], m[:k], cnt.value
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.lib().fb_batch_destroy(self._h)
@@ -119,6 +143,58 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------------------------------------ learned proposal
+def _model_struct(model: dict, keep: list) -> _lib.ProposalModel:
+    arrs = []
+    for k, dt in (("w1", np.uint16), ("b1", np.float32), ("w2", np.uint16), ("b2", np.float32), ("w3", np.uint16),
+                  ("b3", np.float32)):
+        a = np.ascontiguousarray(model[k], dtype=dt)
+        keep.append(a)
+        arrs.append(a.ctypes.data)
+    ms = _lib.ProposalModel(*arrs, float(model.get("mix", 0.5)))
+    keep.append(ms)
+    return ms
+
+
+def _empty_model() -> dict:
+    H, I, O = _lib.MLP_H, _lib.MLP_IN, _lib.MLP_OUT
+    return dict(w1=np.zeros((H, I), np.uint16), b1=np.zeros(H, np.float32), w2=np.zeros((H, H), np.uint16),
+                b2=np.zeros(H, np.float32), w3=np.zeros((O, H), np.uint16), b3=np.zeros(O, np.float32))
+
+
+def train_proposal(x, y, mask, epochs: int = 10, batch: int = 512, lr: float = 2e-3, seed: int = 0,
+                   init: dict | None = None, mix: float = 0.5, device: int = 0) -> tuple[dict, np.ndarray]:
+    """Trains the proposal MLP on the device (masked softmax cross-entropy, Adam); returns (model, epoch losses)."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.int32)
+    mask = np.ascontiguousarray(mask, np.uint32)
+    out = _empty_model()
+    losses = np.zeros(int(epochs))
+    keep: list = []
+    opt = _lib.TrainOptions(int(epochs), int(batch), float(lr), int(seed) & 0xFFFFFFFFFFFFFFFF, int(device))
+    ini = C.byref(_model_struct(init, keep)) if init is not None else None
+    check(_lib.lib().fb_train_proposal(ptr(x), ptr(y), ptr(mask), len(y), C.byref(opt), ini,
+                                       *(ptr(out[k]) for k in ("w1", "b1", "w2", "b2", "w3", "b3")), ptr(losses)))
+    out["mix"] = float(mix)
+    return out, losses
+
+
+def mlp_loss_grad(model: dict, x, y, mask, device: int = 0) -> tuple[float, dict]:
+    """One forward/backward of the device training kernels: mean loss and gradients (FP32)."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.int32)
+    mask = np.ascontiguousarray(mask, np.uint32)
+    keep: list = []
+    ms = _model_struct(model, keep)
+    H, I, O = _lib.MLP_H, _lib.MLP_IN, _lib.MLP_OUT
+    g = dict(w1=np.zeros((H, I), np.float32), b1=np.zeros(H, np.float32), w2=np.zeros((H, H), np.float32),
+             b2=np.zeros(H, np.float32), w3=np.zeros((O, H), np.float32), b3=np.zeros(O, np.float32))
+    loss = C.c_double()
+    check(_lib.lib().fb_mlp_loss_grad(C.byref(ms), ptr(x), ptr(y), ptr(mask), len(y), int(device), C.byref(loss),
+                                      *(ptr(g[k]) for k in ("w1", "b1", "w2", "b2", "w3", "b3"))))
+    return loss.value, g
 
 
 # ------------------------------------------------------------------------------------------------ tree text

@@ -12,7 +12,11 @@ constexpr int MAXDEPTH = 24;   // src/bart_kernel.h:33
 constexpr int NB_MAX = 8;      // per-thread register bins of the fused pass; leaves beyond use shared atomics
 constexpr int MAX_THREADS = 512;
 constexpr int LEAF_STAT_WORDS = 96;   // per tree, 8-byte words: leaf sums of fx(w) [64], then row counts (int) [64]
-constexpr int MIN_THREADS = 64;   // warp 0 is the control warp; at least one row warp
+constexpr int MIN_THREADS = 64;
+// learned proposal MLP: node features -> hidden -> hidden -> one logit per predictor
+constexpr int MLP_IN = 98;
+constexpr int MLP_H = 64;
+constexpr int MLP_OUT = 32;   // warp 0 is the control warp; at least one row warp
 
 // Topology of one tree: 64 node slots (leaf values are kept apart, in th[]).  464 bytes, 16-byte multiple.
 struct DTree {
@@ -71,6 +75,19 @@ struct DBufs {
   int m_max;
   int n_pad_max;
   int rows_in_smem;
+  // learned split-variable proposal (null mw1: BART's uniform proposal)
+  const uint16_t* mw1; const float* mb1;   // [MLP_H][MLP_IN] bf16, [MLP_H]
+  const uint16_t* mw2; const float* mb2;   // [MLP_H][MLP_H], [MLP_H]
+  const uint16_t* mw3; const float* mb3;   // [MLP_OUT][MLP_H], [MLP_OUT]
+  double mix;                              // probability of the model component
+  // accepted births as training examples (train_cap 0: off)
+  float* feat;                             // [trees][MLP_IN] features of each tree's birth proposal
+  unsigned* feat_valid;                    // [trees] valid-variable mask of that proposal
+  float* train_x;                          // [train_cap][MLP_IN]
+  int* train_y;
+  unsigned* train_mask;
+  int* train_count;
+  int train_cap;
 };
 
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem);
@@ -117,6 +134,21 @@ struct DForest {
   int maxnd;               // most nodes of one draw
   int ntree, ndpost, p, nnodes;
 };
+// Learned-proposal training (mlp.cu).  Flat FP32 parameter vector: w1 [H][IN], b1 [H], w2 [H][H], b2 [H],
+// w3 [OUT][H], b3 [OUT]; the forward pass reads BF16 copies of the weights.
+constexpr int MLP_NPARAM = MLP_H * MLP_IN + MLP_H + MLP_H * MLP_H + MLP_H + MLP_OUT * MLP_H + MLP_OUT;
+struct MlpParams {
+  uint16_t* w1; uint16_t* w2; uint16_t* w3;   // BF16 weights (device)
+  const float* b1; const float* b2; const float* b3;
+};
+size_t mlp_grad_smem();
+// summed gradients (and summed loss) of examples idx[0..B) (or 0..B when idx is null), added into grad / *loss
+int mlp_grad_launch(const MlpParams& P, const float* X, const int* Y, const unsigned* M, const int* idx, int B,
+                    float* grad, float* loss, void* stream);
+// Adam step `step` (1-based) with gradient grad * inv_batch; refreshes the BF16 weights of P
+int mlp_adam_launch(float* p, float* m1, float* m2, const float* g, float inv_batch, float lr, int step,
+                    const MlpParams& P, void* stream);
+
 // fixed device scratch of the allocation-free predict call: n * (ncol + 1) doubles at most (8 MiB per device)
 constexpr size_t PREDICT_SCRATCH_DOUBLES = size_t(1) << 20;
 // 0: *ptr = the scratch's address on `device` (the current device); -1: CUDA error; -2: device ordinal not tracked

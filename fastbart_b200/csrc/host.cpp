@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <random>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -97,6 +98,8 @@ struct fb_batch {
   std::vector<void*> allocs;
   long long rows = 0, qbytes = 0, leafbytes = 0, ntrees = 0, nsig = 0, nyhat = 0, ntout = 0;
   cudaStream_t stream = nullptr;
+  void* model_mem = nullptr;   // learned proposal weights (owned; also listed in allocs)
+  int collect_cap = 0;         // allocated capacity of the training-example buffers
   ~fb_batch() {
     int cur = 0;
     cudaGetDevice(&cur);
@@ -241,10 +244,83 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
   CK(cudaSetDevice(b->device));
   b->stream = reinterpret_cast<cudaStream_t>(stream);
   const int S = b->nskip + b->ndpost;
+  if (b->d.train_cap > 0 && cudaMemsetAsync(b->d.train_count, 0, sizeof(int), b->stream) != cudaSuccess)
+    return fail(FB_ERR_CUDA, "cannot reset the training-example counter");
   for (int it0 = 0; it0 < S; it0 += b->spl) {
     const int it1 = std::min(S, it0 + b->spl);
     if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, b->gmax, stream) != 0)
       return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  return FB_OK;
+}
+
+fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
+  if (!b) return fail(FB_ERR_ARG, "batch is NULL");
+  CK(cudaSetDevice(b->device));
+  if (!model || model->mix <= 0.0) {
+    b->d.mw1 = nullptr; b->d.mix = 0.0;
+    return FB_OK;
+  }
+  if (!model->w1 || !model->b1 || !model->w2 || !model->b2 || !model->w3 || !model->b3)
+    return fail(FB_ERR_ARG, "every weight and bias array of the model is required");
+  if (!(model->mix <= 1.0)) return fail(FB_ERR_ARG, "mix must be in (0, 1]");
+  const size_t n1 = (size_t)MLP_H * MLP_IN, n2 = (size_t)MLP_H * MLP_H, n3 = (size_t)MLP_OUT * MLP_H;
+  if (!b->model_mem) {
+    if (cudaMalloc(&b->model_mem, 2 * (n1 + n2 + n3) + 4 * (2 * MLP_H + MLP_OUT)) != cudaSuccess)
+      return fail(FB_ERR_CUDA, "out of device memory");
+    b->allocs.push_back(b->model_mem);
+  }
+  unsigned char* m = static_cast<unsigned char*>(b->model_mem);
+  uint16_t* w1 = reinterpret_cast<uint16_t*>(m); uint16_t* w2 = w1 + n1; uint16_t* w3 = w2 + n2;
+  float* b1 = reinterpret_cast<float*>(w3 + n3); float* b2 = b1 + MLP_H; float* b3 = b2 + MLP_H;
+  CK(cudaMemcpy(w1, model->w1, 2 * n1, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(w2, model->w2, 2 * n2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(w3, model->w3, 2 * n3, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b1, model->b1, 4 * MLP_H, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b2, model->b2, 4 * MLP_H, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b3, model->b3, 4 * MLP_OUT, cudaMemcpyHostToDevice));
+  b->d.mw1 = w1; b->d.mw2 = w2; b->d.mw3 = w3; b->d.mb1 = b1; b->d.mb2 = b2; b->d.mb3 = b3; b->d.mix = model->mix;
+  return FB_OK;
+}
+
+fb_status fb_batch_collect(fb_batch* b, int capacity) {
+  if (!b) return fail(FB_ERR_ARG, "batch is NULL");
+  if (capacity < 0) return fail(FB_ERR_ARG, "capacity must be >= 0");
+  CK(cudaSetDevice(b->device));
+  if (capacity > b->collect_cap) {
+    void *feat = nullptr, *fv = nullptr, *tx = nullptr, *ty = nullptr, *tm = nullptr, *tc = nullptr;
+    if (cudaMalloc(&feat, sizeof(float) * MLP_IN * (size_t)b->ntrees) != cudaSuccess ||
+        cudaMalloc(&fv, sizeof(unsigned) * (size_t)b->ntrees) != cudaSuccess ||
+        cudaMalloc(&tx, sizeof(float) * MLP_IN * (size_t)capacity) != cudaSuccess ||
+        cudaMalloc(&ty, sizeof(int) * (size_t)capacity) != cudaSuccess ||
+        cudaMalloc(&tm, sizeof(unsigned) * (size_t)capacity) != cudaSuccess || cudaMalloc(&tc, sizeof(int)) != cudaSuccess) {
+      cudaFree(feat); cudaFree(fv); cudaFree(tx); cudaFree(ty); cudaFree(tm); cudaFree(tc);
+      return fail(FB_ERR_CUDA, "out of device memory");
+    }
+    for (void* q : {feat, fv, tx, ty, tm, tc}) b->allocs.push_back(q);
+    b->d.feat = static_cast<float*>(feat); b->d.feat_valid = static_cast<unsigned*>(fv);
+    b->d.train_x = static_cast<float*>(tx); b->d.train_y = static_cast<int*>(ty);
+    b->d.train_mask = static_cast<unsigned*>(tm); b->d.train_count = static_cast<int*>(tc);
+    b->collect_cap = capacity;
+  }
+  b->d.train_cap = capacity;
+  return FB_OK;
+}
+
+fb_status fb_batch_training_data(fb_batch* b, float* x, int* y, uint32_t* mask, int cap, int* count) {
+  if (!b || !count) return fail(FB_ERR_ARG, "batch and count are required");
+  CK(cudaSetDevice(b->device));
+  *count = 0;
+  if (b->d.train_cap <= 0) return FB_OK;
+  CK(cudaStreamSynchronize(b->stream));
+  int total = 0;
+  CK(cudaMemcpy(&total, b->d.train_count, sizeof(int), cudaMemcpyDeviceToHost));
+  *count = total;
+  const int k = std::min(std::min(total, b->d.train_cap), std::max(cap, 0));
+  if (k > 0) {
+    if (x) CK(cudaMemcpy(x, b->d.train_x, sizeof(float) * MLP_IN * (size_t)k, cudaMemcpyDeviceToHost));
+    if (y) CK(cudaMemcpy(y, b->d.train_y, sizeof(int) * (size_t)k, cudaMemcpyDeviceToHost));
+    if (mask) CK(cudaMemcpy(mask, b->d.train_mask, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost));
   }
   return FB_OK;
 }
@@ -723,6 +799,172 @@ fb_status fb_predict_draw_static(const fb_compiled* ct, const double* const* col
     return fail(FB_ERR_CUDA, "predict launch failed");
   if (cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
     return fail(FB_ERR_CUDA, "copy of the result failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return FB_OK;
+}
+
+// ------------------------------------------------------------------------------------------------ proposal MLP
+}  // extern "C"
+
+namespace {
+constexpr size_t kN1 = (size_t)MLP_H * MLP_IN, kN2 = (size_t)MLP_H * MLP_H, kN3 = (size_t)MLP_OUT * MLP_H;
+constexpr size_t kOffB1 = kN1, kOffW2 = kOffB1 + MLP_H, kOffB2 = kOffW2 + kN2, kOffW3 = kOffB2 + MLP_H,
+                 kOffB3 = kOffW3 + kN3;
+
+float bf16_host(uint16_t h) { uint32_t u = (uint32_t)h << 16; float f; std::memcpy(&f, &u, 4); return f; }
+uint16_t bf16_round_host(float f) {
+  uint32_t u; std::memcpy(&u, &f, 4);
+  return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
+
+// device state of one training or gradient job; frees everything on scope exit
+struct MlpJob {
+  std::vector<void*> mem;
+  ~MlpJob() { for (void* p : mem) cudaFree(p); }
+  template <class T> bool alloc(T** p, size_t n) {
+    if (cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (n ? n : 1)) != cudaSuccess) return false;
+    mem.push_back(*p);
+    return true;
+  }
+};
+
+fb_status check_examples(const float* x, const int* y, const uint32_t* mask, int count) {
+  if (!x || !y || !mask || count < 1) return fail(FB_ERR_ARG, "x, y, mask and count >= 1 are required");
+  for (int k = 0; k < count; k++)
+    if (y[k] < 0 || y[k] >= MLP_OUT || !((mask[k] >> y[k]) & 1u))
+      return fail(FB_ERR_ARG, "example %d: label %d is not one of its valid predictors", k, y[k]);
+  return FB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+fb_status fb_train_proposal(const float* x, const int* y, const uint32_t* mask, int count,
+                            const fb_train_options* opt, const fb_proposal_model* init, uint16_t* out_w1,
+                            float* out_b1, uint16_t* out_w2, float* out_b2, uint16_t* out_w3, float* out_b3,
+                            double* losses) {
+  if (!opt || !out_w1 || !out_b1 || !out_w2 || !out_b2 || !out_w3 || !out_b3)
+    return fail(FB_ERR_ARG, "options and every output array are required");
+  if (opt->epochs < 1 || opt->batch < 1 || !(opt->lr > 0.0)) return fail(FB_ERR_ARG, "epochs, batch and lr must be > 0");
+  fb_status st = check_examples(x, y, mask, count);
+  if (st != FB_OK) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  CK(cudaSetDevice(opt->device));
+  // initial parameters (host): the given model, or seeded uniform(-a, a) with a = sqrt(6 / fan_in), zero biases
+  std::vector<float> P(MLP_NPARAM, 0.0f);
+  if (init) {
+    if (!init->w1 || !init->b1 || !init->w2 || !init->b2 || !init->w3 || !init->b3)
+      return fail(FB_ERR_ARG, "every weight and bias array of the initial model is required");
+    for (size_t k = 0; k < kN1; k++) P[k] = bf16_host(init->w1[k]);
+    for (size_t k = 0; k < kN2; k++) P[kOffW2 + k] = bf16_host(init->w2[k]);
+    for (size_t k = 0; k < kN3; k++) P[kOffW3 + k] = bf16_host(init->w3[k]);
+    for (int k = 0; k < MLP_H; k++) { P[kOffB1 + k] = init->b1[k]; P[kOffB2 + k] = init->b2[k]; }
+    for (int k = 0; k < MLP_OUT; k++) P[kOffB3 + k] = init->b3[k];
+  } else {
+    std::mt19937_64 g(opt->seed);
+    std::uniform_real_distribution<float> u(-1.0f, 1.0f);
+    const float a1 = std::sqrt(6.0f / MLP_IN), a2 = std::sqrt(6.0f / MLP_H), a3 = 0.1f * std::sqrt(6.0f / MLP_H);
+    for (size_t k = 0; k < kN1; k++) P[k] = bf16_host(bf16_round_host(a1 * u(g)));
+    for (size_t k = 0; k < kN2; k++) P[kOffW2 + k] = bf16_host(bf16_round_host(a2 * u(g)));
+    for (size_t k = 0; k < kN3; k++) P[kOffW3 + k] = bf16_host(bf16_round_host(a3 * u(g)));
+  }
+  std::vector<uint16_t> W(kN1 + kN2 + kN3);
+  for (size_t k = 0; k < kN1; k++) W[k] = bf16_round_host(P[k]);
+  for (size_t k = 0; k < kN2; k++) W[kN1 + k] = bf16_round_host(P[kOffW2 + k]);
+  for (size_t k = 0; k < kN3; k++) W[kN1 + kN2 + k] = bf16_round_host(P[kOffW3 + k]);
+  MlpJob job;
+  float *dx = nullptr, *dp = nullptr, *dm1 = nullptr, *dm2 = nullptr, *dg = nullptr, *dl = nullptr;
+  int *dy = nullptr, *didx = nullptr;
+  unsigned* dmask = nullptr;
+  uint16_t* dw = nullptr;
+  if (!job.alloc(&dx, (size_t)count * MLP_IN) || !job.alloc(&dy, count) || !job.alloc(&dmask, count) ||
+      !job.alloc(&didx, count) || !job.alloc(&dp, MLP_NPARAM) || !job.alloc(&dm1, MLP_NPARAM) ||
+      !job.alloc(&dm2, MLP_NPARAM) || !job.alloc(&dg, MLP_NPARAM) || !job.alloc(&dl, 1) || !job.alloc(&dw, W.size()))
+    return fail(FB_ERR_CUDA, "out of device memory");
+  CK(cudaMemcpy(dx, x, sizeof(float) * MLP_IN * (size_t)count, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dy, y, sizeof(int) * (size_t)count, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dmask, mask, sizeof(unsigned) * (size_t)count, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dp, P.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw, W.data(), sizeof(uint16_t) * W.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemset(dm1, 0, sizeof(float) * MLP_NPARAM));
+  CK(cudaMemset(dm2, 0, sizeof(float) * MLP_NPARAM));
+  MlpParams MP{dw, dw + kN1, dw + kN1 + kN2, dp + kOffB1, dp + kOffB2, dp + kOffB3};
+  std::vector<int> perm(count);
+  for (int k = 0; k < count; k++) perm[k] = k;
+  std::mt19937_64 shuf(opt->seed ^ 0x5851F42D4C957F2Dull);
+  int step = 0;
+  for (int e = 0; e < opt->epochs; e++) {
+    std::shuffle(perm.begin(), perm.end(), shuf);
+    CK(cudaMemcpy(didx, perm.data(), sizeof(int) * (size_t)count, cudaMemcpyHostToDevice));
+    CK(cudaMemset(dl, 0, sizeof(float)));
+    for (int s0 = 0; s0 < count; s0 += opt->batch) {
+      const int B = std::min(opt->batch, count - s0);
+      CK(cudaMemsetAsync(dg, 0, sizeof(float) * MLP_NPARAM));
+      if (mlp_grad_launch(MP, dx, dy, dmask, didx + s0, B, dg, dl, nullptr) != 0)
+        return fail(FB_ERR_CUDA, "gradient kernel failed: %s", cudaGetErrorString(cudaGetLastError()));
+      if (mlp_adam_launch(dp, dm1, dm2, dg, 1.0f / (float)B, (float)opt->lr, ++step, MP, nullptr) != 0)
+        return fail(FB_ERR_CUDA, "update kernel failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    float l = 0.0f;
+    CK(cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost));
+    if (losses) losses[e] = (double)l / count;
+  }
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(P.data(), dp, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(W.data(), dw, sizeof(uint16_t) * W.size(), cudaMemcpyDeviceToHost));
+  std::memcpy(out_w1, W.data(), 2 * kN1);
+  std::memcpy(out_w2, W.data() + kN1, 2 * kN2);
+  std::memcpy(out_w3, W.data() + kN1 + kN2, 2 * kN3);
+  std::memcpy(out_b1, P.data() + kOffB1, 4 * MLP_H);
+  std::memcpy(out_b2, P.data() + kOffB2, 4 * MLP_H);
+  std::memcpy(out_b3, P.data() + kOffB3, 4 * MLP_OUT);
+  return FB_OK;
+}
+
+fb_status fb_mlp_loss_grad(const fb_proposal_model* model, const float* x, const int* y, const uint32_t* mask,
+                           int count, int device, double* loss, float* gw1, float* gb1, float* gw2, float* gb2,
+                           float* gw3, float* gb3) {
+  if (!model || !model->w1 || !model->b1 || !model->w2 || !model->b2 || !model->w3 || !model->b3 || !loss)
+    return fail(FB_ERR_ARG, "model and loss are required");
+  fb_status st = check_examples(x, y, mask, count);
+  if (st != FB_OK) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  CK(cudaSetDevice(device));
+  std::vector<float> P(MLP_NPARAM, 0.0f);
+  for (int k = 0; k < MLP_H; k++) { P[kOffB1 + k] = model->b1[k]; P[kOffB2 + k] = model->b2[k]; }
+  for (int k = 0; k < MLP_OUT; k++) P[kOffB3 + k] = model->b3[k];
+  MlpJob job;
+  float *dx = nullptr, *dp = nullptr, *dg = nullptr, *dl = nullptr;
+  int* dy = nullptr;
+  unsigned* dmask = nullptr;
+  uint16_t* dw = nullptr;
+  if (!job.alloc(&dx, (size_t)count * MLP_IN) || !job.alloc(&dy, count) || !job.alloc(&dmask, count) ||
+      !job.alloc(&dp, MLP_NPARAM) || !job.alloc(&dg, MLP_NPARAM) || !job.alloc(&dl, 1) ||
+      !job.alloc(&dw, kN1 + kN2 + kN3))
+    return fail(FB_ERR_CUDA, "out of device memory");
+  CK(cudaMemcpy(dx, x, sizeof(float) * MLP_IN * (size_t)count, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dy, y, sizeof(int) * (size_t)count, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dmask, mask, sizeof(unsigned) * (size_t)count, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dp, P.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw, model->w1, 2 * kN1, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw + kN1, model->w2, 2 * kN2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw + kN1 + kN2, model->w3, 2 * kN3, cudaMemcpyHostToDevice));
+  CK(cudaMemset(dg, 0, sizeof(float) * MLP_NPARAM));
+  CK(cudaMemset(dl, 0, sizeof(float)));
+  MlpParams MP{dw, dw + kN1, dw + kN1 + kN2, dp + kOffB1, dp + kOffB2, dp + kOffB3};
+  if (mlp_grad_launch(MP, dx, dy, dmask, nullptr, count, dg, dl, nullptr) != 0)
+    return fail(FB_ERR_CUDA, "gradient kernel failed: %s", cudaGetErrorString(cudaGetLastError()));
+  CK(cudaDeviceSynchronize());
+  std::vector<float> G(MLP_NPARAM);
+  float l = 0.0f;
+  CK(cudaMemcpy(G.data(), dg, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost));
+  const float inv = 1.0f / (float)count;
+  *loss = (double)l / count;
+  auto put = [&](float* dst, size_t off, size_t n) { if (dst) for (size_t k = 0; k < n; k++) dst[k] = G[off + k] * inv; };
+  put(gw1, 0, kN1); put(gb1, kOffB1, MLP_H); put(gw2, kOffW2, kN2); put(gb2, kOffB2, MLP_H);
+  put(gw3, kOffW3, kN3); put(gb3, kOffB3, MLP_OUT);
   return FB_OK;
 }
 

@@ -1,0 +1,200 @@
+// mlp.cu -- training kernels of the learned split-variable proposal (no counterpart in the reference).
+//
+// The model is the sampler's proposal MLP: MLP_IN node features -> MLP_H -> MLP_H -> MLP_OUT logits (ReLU between),
+// BF16 weights and FP32 biases, trained by masked softmax cross-entropy on accepted births (the split variable
+// given the node's features, over the predictors with a non-empty cut range at the node).
+//
+// Parameters live in one flat FP32 vector (the master copy) in the order w1 [H][IN], b1 [H], w2 [H][H], b2 [H],
+// w3 [OUT][H], b3 [OUT]; the forward pass reads the BF16-rounded weights, exactly as the sampler does.
+//   mlp_grad_kernel   one CTA per tile of MT_TILE examples: forward, softmax, backward for the tile in shared
+//                     memory, then one atomic add per parameter and tile into the FP32 gradient vector (and the
+//                     tile's summed loss).  Tiny GEMMs (at most 64 x 98 per layer): CUDA cores, no tensor cores.
+//   mlp_adam_kernel   Adam step on the master weights from the summed gradients / batch size, refreshing the BF16
+//                     copies of the weights.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fb_internal.h"
+
+namespace fb {
+
+constexpr int MT_TILE = 32;
+constexpr int MT_THREADS = 256;
+
+__device__ __forceinline__ float bf16_to_f(uint16_t h) { return __uint_as_float((unsigned)h << 16); }
+__device__ __forceinline__ uint16_t f_to_bf16(float f) {   // round to nearest even (finite inputs)
+  const unsigned u = __float_as_uint(f);
+  return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
+
+__global__ void __launch_bounds__(MT_THREADS) mlp_grad_kernel(MlpParams P, const float* __restrict__ X,
+                                                              const int* __restrict__ Y,
+                                                              const unsigned* __restrict__ M,
+                                                              const int* __restrict__ idx, int B,
+                                                              float* __restrict__ grad, float* __restrict__ loss) {
+  extern __shared__ float ms[];
+  float* w1 = ms;                           // [H][IN]
+  float* w2 = w1 + MLP_H * MLP_IN;          // [H][H]
+  float* w3 = w2 + MLP_H * MLP_H;           // [OUT][H]
+  float* xs = w3 + MLP_OUT * MLP_H;         // [TILE][IN]
+  float* h1 = xs + MT_TILE * MLP_IN;        // [TILE][H]
+  float* h2 = h1 + MT_TILE * MLP_H;         // [TILE][H]
+  float* g3 = h2 + MT_TILE * MLP_H;         // [TILE][OUT]
+  float* d2 = g3 + MT_TILE * MLP_OUT;       // [TILE][H]
+  float* d1 = d2 + MT_TILE * MLP_H;         // [TILE][H]
+  float* lsum = d1 + MT_TILE * MLP_H;       // [1]
+  const int tid = threadIdx.x;
+  const int b0 = blockIdx.x * MT_TILE;
+  const int nb = min(MT_TILE, B - b0);
+  for (int k = tid; k < MLP_H * MLP_IN; k += MT_THREADS) w1[k] = bf16_to_f(P.w1[k]);
+  for (int k = tid; k < MLP_H * MLP_H; k += MT_THREADS) w2[k] = bf16_to_f(P.w2[k]);
+  for (int k = tid; k < MLP_OUT * MLP_H; k += MT_THREADS) w3[k] = bf16_to_f(P.w3[k]);
+  for (int k = tid; k < MT_TILE * MLP_IN; k += MT_THREADS) {
+    const int b = k / MLP_IN, f = k % MLP_IN;
+    xs[k] = b < nb ? X[(long long)(idx ? idx[b0 + b] : b0 + b) * MLP_IN + f] : 0.0f;
+  }
+  if (tid == 0) *lsum = 0.0f;
+  __syncthreads();
+  // forward
+  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
+    const int b = k / MLP_H, h = k % MLP_H;
+    float a = P.b1[h];
+    for (int f = 0; f < MLP_IN; f++) a += w1[h * MLP_IN + f] * xs[b * MLP_IN + f];
+    h1[k] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
+    const int b = k / MLP_H, h = k % MLP_H;
+    float a = P.b2[h];
+    for (int f = 0; f < MLP_H; f++) a += w2[h * MLP_H + f] * h1[b * MLP_H + f];
+    h2[k] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * MLP_OUT; k += MT_THREADS) {
+    const int b = k / MLP_OUT, o = k % MLP_OUT;
+    float a = P.b3[o];
+    for (int f = 0; f < MLP_H; f++) a += w3[o * MLP_H + f] * h2[b * MLP_H + f];
+    g3[k] = a;
+  }
+  __syncthreads();
+  // masked softmax and cross-entropy, one thread per example: g3 becomes dLoss/dz (summed, not averaged)
+  if (tid < MT_TILE) {
+    const int b = tid;
+    float* z = g3 + b * MLP_OUT;
+    if (b < nb) {
+      const long long e = idx ? idx[b0 + b] : b0 + b;
+      const unsigned mk = M[e];
+      const int y = Y[e];
+      float zmax = -3.0e38f;
+      for (int o = 0; o < MLP_OUT; o++) if ((mk >> o) & 1u) zmax = fmaxf(zmax, z[o]);
+      float S = 0.0f;
+      for (int o = 0; o < MLP_OUT; o++) S += ((mk >> o) & 1u) ? __expf(z[o] - zmax) : 0.0f;
+      atomicAdd(lsum, -(z[y] - zmax - __logf(S)));
+      for (int o = 0; o < MLP_OUT; o++)
+        z[o] = (((mk >> o) & 1u) ? __expf(z[o] - zmax) / S : 0.0f) - (o == y ? 1.0f : 0.0f);
+    } else {
+      for (int o = 0; o < MLP_OUT; o++) z[o] = 0.0f;
+    }
+  }
+  __syncthreads();
+  // backward through layer 3 and the second ReLU
+  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
+    const int b = k / MLP_H, h = k % MLP_H;
+    float a = 0.0f;
+    for (int o = 0; o < MLP_OUT; o++) a += g3[b * MLP_OUT + o] * w3[o * MLP_H + h];
+    d2[k] = h2[k] > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
+    const int b = k / MLP_H, h = k % MLP_H;
+    float a = 0.0f;
+    for (int o = 0; o < MLP_H; o++) a += d2[b * MLP_H + o] * w2[o * MLP_H + h];
+    d1[k] = h1[k] > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  // parameter gradients of the tile, one atomic add each
+  float* gw1 = grad;
+  float* gb1 = gw1 + MLP_H * MLP_IN;
+  float* gw2 = gb1 + MLP_H;
+  float* gb2 = gw2 + MLP_H * MLP_H;
+  float* gw3 = gb2 + MLP_H;
+  float* gb3 = gw3 + MLP_OUT * MLP_H;
+  for (int k = tid; k < MLP_H * MLP_IN; k += MT_THREADS) {
+    const int h = k / MLP_IN, f = k % MLP_IN;
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += d1[b * MLP_H + h] * xs[b * MLP_IN + f];
+    atomicAdd(gw1 + k, a);
+  }
+  for (int k = tid; k < MLP_H * MLP_H; k += MT_THREADS) {
+    const int h = k / MLP_H, f = k % MLP_H;
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += d2[b * MLP_H + h] * h1[b * MLP_H + f];
+    atomicAdd(gw2 + k, a);
+  }
+  for (int k = tid; k < MLP_OUT * MLP_H; k += MT_THREADS) {
+    const int o = k / MLP_H, f = k % MLP_H;
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += g3[b * MLP_OUT + o] * h2[b * MLP_H + f];
+    atomicAdd(gw3 + k, a);
+  }
+  if (tid < MLP_H) {
+    float a = 0.0f, c = 0.0f;
+    for (int b = 0; b < nb; b++) { a += d1[b * MLP_H + tid]; c += d2[b * MLP_H + tid]; }
+    atomicAdd(gb1 + tid, a);
+    atomicAdd(gb2 + tid, c);
+  }
+  if (tid < MLP_OUT) {
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += g3[b * MLP_OUT + tid];
+    atomicAdd(gb3 + tid, a);
+  }
+  __syncthreads();
+  if (tid == 0) atomicAdd(loss, *lsum);
+}
+
+// Adam on the flat parameter vector; weights (not biases) also refresh their BF16 copies.
+__global__ void mlp_adam_kernel(float* __restrict__ p, float* __restrict__ m1, float* __restrict__ m2,
+                                const float* __restrict__ g, int n, float inv_batch, float lr, float c1, float c2,
+                                MlpParams P) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float gk = g[k] * inv_batch;
+  const float a = 0.9f * m1[k] + 0.1f * gk;
+  const float b = 0.999f * m2[k] + 0.001f * gk * gk;
+  m1[k] = a;
+  m2[k] = b;
+  const float w = p[k] - lr * (a * c1) / (sqrtf(b * c2) + 1e-8f);
+  p[k] = w;
+  const int o1 = MLP_H * MLP_IN, o2 = o1 + MLP_H, o3 = o2 + MLP_H * MLP_H, o4 = o3 + MLP_H, o5 = o4 + MLP_OUT * MLP_H;
+  if (k < o1) P.w1[k] = f_to_bf16(w);
+  else if (k >= o2 && k < o3) P.w2[k - o2] = f_to_bf16(w);
+  else if (k >= o4 && k < o5) P.w3[k - o4] = f_to_bf16(w);
+}
+
+size_t mlp_grad_smem() {
+  return sizeof(float) * ((size_t)MLP_H * MLP_IN + MLP_H * MLP_H + MLP_OUT * MLP_H +
+                          (size_t)MT_TILE * (MLP_IN + 4 * MLP_H + MLP_OUT) + 1);
+}
+
+int mlp_grad_launch(const MlpParams& P, const float* X, const int* Y, const unsigned* M, const int* idx, int B,
+                    float* grad, float* loss, void* stream) {
+  if (B <= 0) return 0;
+  const size_t smem = mlp_grad_smem();
+  if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return -1;
+  mlp_grad_kernel<<<(B + MT_TILE - 1) / MT_TILE, MT_THREADS, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+      P, X, Y, M, idx, B, grad, loss);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int mlp_adam_launch(float* p, float* m1, float* m2, const float* g, float inv_batch, float lr, int step,
+                    const MlpParams& P, void* stream) {
+  const int n = MLP_NPARAM;
+  const float c1 = 1.0f / (1.0f - powf(0.9f, (float)step)), c2 = 1.0f / (1.0f - powf(0.999f, (float)step));
+  mlp_adam_kernel<<<(n + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(p, m1, m2, g, n, inv_batch,
+                                                                                       lr, c1, c2, P);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace fb

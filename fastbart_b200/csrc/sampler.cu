@@ -301,8 +301,87 @@ __device__ __noinline__ double lh(double b, double M, double t2) {   // src/bart
   return -0.5 * fbm::fb_log(k) + 0.5 * M * M * t2 / k;
 }
 
+// ------------------------------------------------------------------------------------------------ learned proposal
+// Features of node nx of tree t for the learned split-variable proposal (functions of the tree and the node's row
+// count only, so the forward and the reverse move see the same inputs):
+//   x[0] depth / 8;  x[1] floor(log2(cnt + 1)) / 16;
+//   x[2 + v]  min(internal nodes other than `exclude` splitting on v, 8) / 8;
+//   x[34 + v] cut range of v at nx, (U - L + 1) / numcut[v];  x[66 + v] L / numcut[v]  (0 when empty).
+// Returns the mask of predictors whose range at nx is non-empty.
+__device__ __noinline__ unsigned node_features(const DTree* t, int nx, int cnt, int exclude, const DChain& C, float* x) {
+  for (int k = 0; k < MLP_IN; k++) x[k] = 0.0f;
+  x[0] = __fdiv_rn((float)t->d[nx], 8.0f);
+  x[1] = __fdiv_rn((float)(31 - __clz(cnt + 1)), 16.0f);
+  int use[PMAX];
+  for (int v = 0; v < PMAX; v++) use[v] = 0;
+  const unsigned long long inner = t->used & ~t->leaf;
+  for (unsigned long long im = inner; im; im &= im - 1ull) {
+    const int sl = __ffsll((long long)im) - 1;
+    if (sl != exclude) use[t->v[sl]]++;
+  }
+  unsigned valid = 0u;
+  for (int v = 0; v < PMAX; v++) {
+    x[2 + v] = __fdiv_rn((float)(use[v] < 8 ? use[v] : 8), 8.0f);
+    if (v < C.p && C.numcut[v] > 0) {
+      int L, U;
+      node_range(t, nx, v, C.numcut[v], L, U);
+      if (U >= L) {
+        x[34 + v] = __fdiv_rn((float)(U - L + 1), (float)C.numcut[v]);
+        x[66 + v] = __fdiv_rn((float)L, (float)C.numcut[v]);
+        valid |= 1u << v;
+      }
+    }
+  }
+  return valid;
+}
+
+__device__ __forceinline__ float bf16f(uint16_t h) { return __uint_as_float((unsigned)h << 16); }
+
+// MLP forward (FP32, no fused multiply-add, fixed order) and masked softmax in FP64: q[v] for valid v, else 0.
+__device__ __noinline__ void model_probs(const DBufs& B, const float* x, unsigned valid, double* q) {
+  float h1[MLP_H], h2[MLP_H], z[MLP_OUT];
+  for (int h = 0; h < MLP_H; h++) {
+    float a = __ldg(B.mb1 + h);
+    const uint16_t* w = B.mw1 + h * MLP_IN;
+    for (int k = 0; k < MLP_IN; k++) a = __fadd_rn(a, __fmul_rn(bf16f(__ldg(w + k)), x[k]));
+    h1[h] = a > 0.0f ? a : 0.0f;
+  }
+  for (int h = 0; h < MLP_H; h++) {
+    float a = __ldg(B.mb2 + h);
+    const uint16_t* w = B.mw2 + h * MLP_H;
+    for (int k = 0; k < MLP_H; k++) a = __fadd_rn(a, __fmul_rn(bf16f(__ldg(w + k)), h1[k]));
+    h2[h] = a > 0.0f ? a : 0.0f;
+  }
+  for (int o = 0; o < MLP_OUT; o++) {
+    float a = __ldg(B.mb3 + o);
+    const uint16_t* w = B.mw3 + o * MLP_H;
+    for (int k = 0; k < MLP_H; k++) a = __fadd_rn(a, __fmul_rn(bf16f(__ldg(w + k)), h2[k]));
+    z[o] = a;
+  }
+  double zmax = 0.0;
+  bool any = false;
+  for (int v = 0; v < MLP_OUT; v++)
+    if ((valid >> v) & 1u) { if (!any || (double)z[v] > zmax) zmax = (double)z[v]; any = true; }
+  double S = 0.0;
+  for (int v = 0; v < MLP_OUT; v++) {
+    q[v] = ((valid >> v) & 1u) ? fbm::fb_exp((double)z[v] - zmax) : 0.0;
+    S = S + q[v];
+  }
+  for (int v = 0; v < MLP_OUT; v++) q[v] = S > 0.0 ? q[v] / S : 0.0;
+}
+
+// probability that the mixture proposes valid predictor v: mix * q[v] + (1 - mix) / p
+__device__ __forceinline__ double mix_prob(double mix, const double* q, int v, int p) {
+  return mix * q[v] + (1.0 - mix) * (1.0 / (double)p);
+}
+
 // Proposal of tree j at sweep it (src/bart_kernel.cpp:413-464); also resolves unknown goodvar counts of leaves.
-__device__ Prop propose(DTree* t, const DChain& C, int j, int it, Masks& mk) {
+// With a learned model (B.mw1), the birth variable comes from the model's masked softmax with probability B.mix
+// (else uniformly, as BART), and pr carries the proposal-probability correction of the birth, or of the reverse birth
+// of a death, so the chain keeps BART's target.  cnt: the tree's per-slot row counts.  When training examples are
+// collected, the birth node's features go to feat / *fvalid.
+__device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cnt, int j, int it, Masks& mk,
+                        float* feat, unsigned* fvalid) {
   const double pb = 0.5;
   const unsigned long long used = t->used, leafm = t->leaf;
   mk.used = used; mk.leaf = leafm;
@@ -321,12 +400,37 @@ __device__ Prop propose(DTree* t, const DChain& C, int j, int it, Masks& mk) {
   const double PBx = ngood == 0 ? 0 : (single ? 1 : pb);
   const fbm::U4 x = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP, C.seed);
   const double ub = fbm::u32d(x.x), un = fbm::u32d(x.y), uv = fbm::u32d(x.z), uc = fbm::u32d(x.w);
+  const bool model = B.mw1 != nullptr && B.mix > 0.0;
   Prop P;
   P.mode = 0; P.nx = 0; P.v = 0; P.c = 0; P.l = 0; P.r = 0; P.pad0 = P.pad1 = 0; P.logpr = 0; P.lu = 0;
   double pr = 0;
   if (ub < PBx) {
     const int nx = select_kth(goodm, (int)(un * ngood));
-    int v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
+    int v;
+    double corr = 1.0;
+    if (model) {
+      float xf[MLP_IN];
+      double q[MLP_OUT];
+      const unsigned valid = node_features(t, nx, cnt[nx], -1, C, xf);
+      model_probs(B, xf, valid, q);
+      const fbm::U4 y2 = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP2, C.seed);
+      const double umix = fbm::u32d(y2.x), uvm = fbm::u32d(y2.y);
+      if (umix < B.mix && valid) {
+        double cum = 0.0;
+        int last = 0;
+        v = -1;
+        for (int k = 0; k < MLP_OUT; k++)
+          if ((valid >> k) & 1u) { cum = cum + q[k]; last = k; if (v < 0 && uvm < cum) v = k; }
+        if (v < 0) v = last;
+      } else {
+        v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
+      }
+      if ((valid >> v) & 1u) corr = (1.0 / (double)C.p) / mix_prob(B.mix, q, v, C.p);
+      if (feat) { for (int k = 0; k < MLP_IN; k++) feat[k] = xf[k]; *fvalid = valid; }
+    } else {
+      v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
+      if (feat) *fvalid = node_features(t, nx, cnt[nx], -1, C, feat);
+    }
     int bL, bU;
     node_range(t, nx, v, C.numcut[v], bL, bU);
     if (bU >= bL && (int)t->d[nx] + 1 < MAXDEPTH) {
@@ -346,6 +450,7 @@ __device__ Prop propose(DTree* t, const DChain& C, int j, int it, Masks& mk) {
       }
       const double Pbotx = (double)1 / ngood;
       pr = (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
+      if (model) pr = pr * corr;
       P.mode = 1; P.nx = (uint8_t)nx; P.v = (uint8_t)v; P.c = (uint8_t)c;
     }
   } else if (nnogs > 0) {
@@ -357,6 +462,13 @@ __device__ Prop propose(DTree* t, const DChain& C, int j, int it, Masks& mk) {
     const int ng2 = ngood - (t->ngv[l] > 0) - (t->ngv[r] > 0) + 1;
     const double Pboty = (double)1 / ng2, PDx = 1 - PBx, Pnogx = (double)1 / nnogs;
     pr = ((1 - PGny) * PBy * Pboty) / (PGny * (1 - PGlx) * (1 - PGrx) * PDx * Pnogx);
+    if (model) {   // the reverse move: birth of nx's split in the tree without it
+      float xf[MLP_IN];
+      double q[MLP_OUT];
+      const unsigned valid = node_features(t, nx, cnt[l] + cnt[r], nx, C, xf);
+      model_probs(B, xf, valid, q);
+      pr = pr * (mix_prob(B.mix, q, (int)t->v[nx], C.p) * (double)C.p);
+    }
     P.mode = 2; P.nx = (uint8_t)nx; P.l = (uint8_t)l; P.r = (uint8_t)r;
   }
   if (P.mode) {
@@ -479,8 +591,19 @@ __device__ __forceinline__ void fetch_tree(const Smem& S, const DTree* trees, co
 
 // apply the decided move of tree j (ctl) to its topology and leaf statistics in buffer j & 1 and write the tree back
 // (control warp)
-__device__ void commit_tree(const Smem& S, const DChain& C, DTree* trees, long long* s0g, int j, int lane) {
+__device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTree* trees, long long* s0g, int j,
+                            int lane) {
   const Ctl& ctl = *S.ctl;
+  if (B.train_cap > 0 && ctl.pmode == 1) {   // an accepted birth becomes a training example
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(B.train_count, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx < B.train_cap) {
+      const float* f = B.feat + (C.off_tree + j) * MLP_IN;
+      for (int k = lane; k < MLP_IN; k += 32) B.train_x[(long long)idx * MLP_IN + k] = f[k];
+      if (lane == 0) { B.train_y[idx] = ctl.pv; B.train_mask[idx] = B.feat_valid[C.off_tree + j]; }
+    }
+  }
   DTree* t = S.tree + (j & 1);
   long long* s0 = S.s0t + (j & 1) * LST;
   int* cnt = reinterpret_cast<int*>(s0 + NODES);
@@ -596,7 +719,9 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     // ---------------------------------------------------------------- proposals, one thread per tree
     for (int j = tid; j < m; j += T) {
       Masks mk;
-      const Prop P = propose(trees + j, C, j, it, mk);
+      float* featj = B.train_cap > 0 ? B.feat + (C.off_tree + j) * MLP_IN : nullptr;
+      const Prop P = propose(trees + j, C, B, reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES), j, it,
+                             mk, featj, B.feat_valid + (C.off_tree + j));
       S.prop[j] = P;
       S.masks[j] = mk;
       int k = 0;
@@ -653,7 +778,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         // control warp: commit tree j-1, fetch tree j+1 into the freed buffer, draw the normals of every slot that
         // can be a leaf of tree j after its move (current leaves, the two slots a birth would take, the node a death
         // would restore)
-        if (j > 0) commit_tree(S, C, trees, s0g, j - 1, lane);
+        if (j > 0) commit_tree(S, C, B, trees, s0g, j - 1, lane);
         if (j + 1 < m && j > 0) fetch_tree(S, trees, s0g, j + 1, lane);
         const unsigned long long cand = P.cand;
         if (__popcll(cand) > ZMAX)
@@ -767,7 +892,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       __syncthreads();
     }
     // ---------------------------------------------------------------- end of sweep
-    if (warp == 0) commit_tree(S, C, trees, s0g, m - 1, lane);
+    if (warp == 0) commit_tree(S, C, B, trees, s0g, m - 1, lane);
     __syncthreads();
     const bool keep = it >= C.nskip;
     const int dr = it - C.nskip;

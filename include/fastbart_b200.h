@@ -94,6 +94,52 @@ fb_status fb_batch_download(fb_batch* b, fb_chain_out* outs);
 fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes);
 void fb_batch_destroy(fb_batch* b);
 
+/* ---------------------------------------------------------------------------- learned split-variable proposal */
+
+/* Small MLP that proposes the split variable of a birth from node features (depth, row count, per-predictor use in
+ * the tree and cut range at the node): FB_MLP_IN -> FB_MLP_H -> FB_MLP_H -> FB_MLP_OUT logits, ReLU between, BF16
+ * weights (raw bits), FP32 biases.  A birth draws its variable from the masked softmax with probability mix, else
+ * uniformly as BART (src/bart_kernel.cpp:434); the Metropolis-Hastings ratio carries the exact proposal probabilities
+ * of the birth and of the reverse birth of a death, so the chain targets the same posterior as BART's proposal.
+ * No counterpart in the reference, which always proposes uniformly. */
+#define FB_MLP_IN 98
+#define FB_MLP_H 64
+#define FB_MLP_OUT 32
+typedef struct fb_proposal_model {
+  const uint16_t* w1; const float* b1;   /* [FB_MLP_H][FB_MLP_IN], [FB_MLP_H] */
+  const uint16_t* w2; const float* b2;   /* [FB_MLP_H][FB_MLP_H], [FB_MLP_H] */
+  const uint16_t* w3; const float* b3;   /* [FB_MLP_OUT][FB_MLP_H], [FB_MLP_OUT] */
+  double mix;                            /* probability of the model component, in (0, 1]; <= 0: BART's proposal */
+} fb_proposal_model;
+/* Uses `model` (copied to the device) for the batch's next runs; NULL or mix <= 0 restores BART's proposal. */
+fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model);
+/* Collects every accepted birth of the next runs as a training example (features of the node before the birth, the
+ * split variable, the mask of predictors with a non-empty cut range there), up to `capacity` per run; 0 stops. */
+fb_status fb_batch_collect(fb_batch* b, int capacity);
+/* Copies up to cap examples of the last run (x [cap][FB_MLP_IN], y, mask); *count receives the number of accepted
+ * births of the run (it can exceed the capacity). */
+fb_status fb_batch_training_data(fb_batch* b, float* x, int* y, uint32_t* mask, int cap, int* count);
+
+/* Training of the proposal MLP on the device (masked softmax cross-entropy, Adam, minibatches in a fixed seeded
+ * order).  Weights start from `init` when non-NULL (else a seeded scaled-uniform initialisation); the trained model
+ * is written to out_* (host arrays of the fb_proposal_model shapes, FP32 master weights rounded to BF16).
+ * losses[e] receives the mean loss of epoch e when non-NULL. */
+typedef struct fb_train_options {
+  int epochs, batch;        /* passes over the examples, examples per step */
+  double lr;                /* Adam step size */
+  uint64_t seed;            /* initialisation and shuffling */
+  int device;
+} fb_train_options;
+fb_status fb_train_proposal(const float* x, const int* y, const uint32_t* mask, int count,
+                            const fb_train_options* opt, const fb_proposal_model* init, uint16_t* out_w1,
+                            float* out_b1, uint16_t* out_w2, float* out_b2, uint16_t* out_w3, float* out_b3,
+                            double* losses);
+/* One forward and backward pass of the training kernels on `count` examples: mean loss and the gradients of the
+ * loss with respect to the (BF16-valued) weights and biases, in the shapes of fb_proposal_model (FP32). */
+fb_status fb_mlp_loss_grad(const fb_proposal_model* model, const float* x, const int* y, const uint32_t* mask,
+                           int count, int device, double* loss, float* gw1, float* gb1, float* gw2, float* gb2,
+                           float* gw3, float* gb3);
+
 /* fbart_cpp (src/glue.cpp:10-62) with R's memory layouts: q is the n x p integer code matrix (column-major), yhat is
  * ndpost x n and varcount ndpost x p (column-major, as Rcpp::NumericMatrix / IntegerMatrix).  trees_text receives
  * BART's tree text when non-NULL; *text_len always receives its length (call once with trees_text = NULL to size the

@@ -261,6 +261,216 @@ static oprop propose(const otree* t, const double* PG, const int* nc, int p, uni
   return o;
 }
 
+/* ================================================================ learned split-variable proposal (DEV mode) */
+static float bf16f(uint16_t h) { uint32_t u = (uint32_t)h << 16; float f; memcpy(&f, &u, 4); return f; }
+
+/* Features of leaf-to-be-split node nx of tree t (depends only on the tree and the node's row count):
+ *   x[0] depth / 8;  x[1] floor(log2(cnt + 1)) / 16;
+ *   x[2 + v]  min(number of internal nodes splitting on v, 8) / 8 (internal nodes other than `exclude`);
+ *   x[34 + v] cut range of v at nx, (U - L + 1) / numcut[v];  x[66 + v] L / numcut[v]  (0 when empty).
+ * Returns the mask of variables whose range at nx is non-empty. */
+static uint32_t orc_features(const otree* t, int nx, int cnt, int exclude, const int* nc, int p, float* x) {
+  for (int k = 0; k < ORC_MLP_IN; k++) x[k] = 0.0f;
+  x[0] = (float)t->d[nx] / 8.0f;
+  int bl = 0;
+  for (unsigned c = (unsigned)cnt + 1u; c > 1u; c >>= 1) bl++;
+  x[1] = (float)bl / 16.0f;
+  int use[ORC_PMAX];
+  for (int v = 0; v < ORC_PMAX; v++) use[v] = 0;
+  for (int s = 0; s < ORC_NODES; s++)
+    if (BIT(t->used, s) && !BIT(t->leaf, s) && s != exclude) use[t->v[s]]++;
+  uint32_t valid = 0;
+  for (int v = 0; v < ORC_PMAX; v++) {
+    x[2 + v] = (float)(use[v] < 8 ? use[v] : 8) / 8.0f;
+    if (v < p && nc[v] > 0) {
+      int L, U;
+      node_range(t, nx, v, nc[v], &L, &U);
+      if (U >= L) {
+        x[34 + v] = (float)(U - L + 1) / (float)nc[v];
+        x[66 + v] = (float)L / (float)nc[v];
+        valid |= 1u << v;
+      }
+    }
+  }
+  return valid;
+}
+
+void orc_mlp_logits(const orc_model* M, const float* x, float* z) {
+  float h1[ORC_MLP_H], h2[ORC_MLP_H];
+  for (int h = 0; h < ORC_MLP_H; h++) {
+    float a = M->b1[h];
+    for (int k = 0; k < ORC_MLP_IN; k++) a = a + bf16f(M->w1[h * ORC_MLP_IN + k]) * x[k];
+    h1[h] = a > 0.0f ? a : 0.0f;
+  }
+  for (int h = 0; h < ORC_MLP_H; h++) {
+    float a = M->b2[h];
+    for (int k = 0; k < ORC_MLP_H; k++) a = a + bf16f(M->w2[h * ORC_MLP_H + k]) * h1[k];
+    h2[h] = a > 0.0f ? a : 0.0f;
+  }
+  for (int o = 0; o < ORC_MLP_OUT; o++) {
+    float a = M->b3[o];
+    for (int k = 0; k < ORC_MLP_H; k++) a = a + bf16f(M->w3[o * ORC_MLP_H + k]) * h2[k];
+    z[o] = a;
+  }
+}
+
+void orc_mlp_probs(const float* z, uint32_t valid, double* q) {
+  double zmax = 0.0;
+  int any = 0;
+  for (int v = 0; v < ORC_MLP_OUT; v++)
+    if ((valid >> v) & 1u) { if (!any || (double)z[v] > zmax) zmax = (double)z[v]; any = 1; }
+  double S = 0.0;
+  for (int v = 0; v < ORC_MLP_OUT; v++) { q[v] = ((valid >> v) & 1u) ? orc_exp((double)z[v] - zmax) : 0.0; S = S + q[v]; }
+  for (int v = 0; v < ORC_MLP_OUT; v++) q[v] = S > 0.0 ? q[v] / S : 0.0;
+}
+
+/* probability that the mixture proposes valid variable v: mix * q[v] + (1 - mix) / p */
+static double mix_prob(const orc_model* M, const double* q, int v, int p) {
+  return M->mix * q[v] + (1.0 - M->mix) * (1.0 / (double)p);
+}
+
+static int count_rows(const uint8_t* lf, int n, int a, int b) {
+  int c = 0;
+  for (int i = 0; i < n; i++) c += (lf[i] == a || lf[i] == b);
+  return c;
+}
+
+/* Proposal with the learned model (mirrors the device): BART's proposal (propose()) with the birth variable drawn
+ * from the mixture and the proposal-ratio correction folded into pr.  feat/valid/vout receive the birth node's
+ * features (for training examples). */
+static oprop propose_model(const otree* t, const double* PG, const int* nc, int p, const double* u4, const double* u2,
+                           const orc_model* M, const uint8_t* lf, int n, float* feat, uint32_t* valid_out) {
+  const double pb = 0.5;
+  uint64_t goodm = 0, nogm = 0;
+  for (int s = 0; s < ORC_NODES; s++) {
+    int isleaf = (int)BIT(t->leaf, s), isused = (int)BIT(t->used, s);
+    if (isused && isleaf && t->ngv[s] > 0) goodm |= 1ull << s;
+    if (isused && !isleaf && BIT(t->leaf, (int)t->l[s]) && BIT(t->leaf, (int)t->r[s])) nogm |= 1ull << s;
+  }
+  int ngood = popc64(goodm), nnogs = popc64(nogm);
+  int single = (t->used == 1ull);
+  double PBx = ngood == 0 ? 0 : (single ? 1 : pb);
+  oprop o = {0, 0, 0, 0, 0.0};
+  *valid_out = 0;
+  if (u4[0] < PBx) {
+    int nx = select_kth(goodm, (int)(u4[1] * ngood));
+    float z[ORC_MLP_OUT];
+    double q[ORC_MLP_OUT];
+    uint32_t valid = orc_features(t, nx, count_rows(lf, n, nx, nx), -1, nc, p, feat);
+    *valid_out = valid;
+    orc_mlp_logits(M, feat, z);
+    orc_mlp_probs(z, valid, q);
+    int v;
+    if (u2[0] < M->mix && valid) {
+      double c = 0.0;
+      v = -1;
+      int last = 0;
+      for (int k = 0; k < ORC_MLP_OUT; k++)
+        if ((valid >> k) & 1u) { c = c + q[k]; last = k; if (v < 0 && u2[1] < c) v = k; }
+      if (v < 0) v = last;
+    } else {
+      v = (int)(u4[2] * p); if (v >= p) v = p - 1;
+    }
+    int bL, bU;
+    node_range(t, nx, v, nc[v], &bL, &bU);
+    if (bU >= bL && (int)t->d[nx] + 1 < ORC_MAXDEPTH) {
+      int c = bL + (int)(u4[3] * (bU - bL + 1)); if (c > bU) c = bU;
+      int dnx = t->d[nx];
+      double PGnx = PG[dnx], PGly, PGry;
+      if (t->ngv[nx] > 1) { PGly = PGry = PG[dnx + 1]; }
+      else { PGly = (c - 1 < bL) ? 0 : PG[dnx + 1]; PGry = (bU < c + 1) ? 0 : PG[dnx + 1]; }
+      double PDy = (ngood > 1) ? 1 - pb : ((PGry == 0 && PGly == 0) ? 1 : 1 - pb);
+      double Pnogy;
+      if (nx == 0) Pnogy = 1;
+      else {
+        int pa = t->par[nx];
+        int panog = BIT(t->leaf, (int)t->l[pa]) && BIT(t->leaf, (int)t->r[pa]);
+        Pnogy = panog ? (double)1 / nnogs : (double)1 / (nnogs + 1);
+      }
+      double Pbotx = (double)1 / ngood;
+      o.pr = (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
+      o.pr = o.pr * ((1.0 / (double)p) / mix_prob(M, q, v, p));
+      o.mode = 1; o.nx = nx; o.v = v; o.c = c;
+    }
+  } else if (nnogs > 0) {
+    int nx = select_kth(nogm, (int)(u4[1] * nnogs));
+    int dny = t->d[nx], l = t->l[nx], r = t->r[nx];
+    double PGny = PG[dny];
+    double PGlx = t->ngv[l] > 0 ? PG[dny + 1] : 0, PGrx = t->ngv[r] > 0 ? PG[dny + 1] : 0;
+    double PBy = (nx == 0) ? 1 : pb;
+    int ng2 = ngood - (t->ngv[l] > 0) - (t->ngv[r] > 0) + 1;
+    double Pboty = (double)1 / ng2, PDx = 1 - PBx, Pnogx = (double)1 / nnogs;
+    o.pr = ((1 - PGny) * PBy * Pboty) / (PGny * (1 - PGlx) * (1 - PGrx) * PDx * Pnogx);
+    /* reverse move: the birth of nx's split in the tree without it */
+    float fx[ORC_MLP_IN], z[ORC_MLP_OUT];
+    double q[ORC_MLP_OUT];
+    uint32_t valid = orc_features(t, nx, count_rows(lf, n, l, r), nx, nc, p, fx);
+    orc_mlp_logits(M, fx, z);
+    orc_mlp_probs(z, valid, q);
+    o.pr = o.pr * (mix_prob(M, q, (int)t->v[nx], p) * (double)p);
+    o.mode = 2; o.nx = nx;
+  }
+  return o;
+}
+
+double orc_mlp_loss_grad(const orc_model* M, const float* X, const int* y, const uint32_t* mask, int B,
+                         double* gw1, double* gb1, double* gw2, double* gb2, double* gw3, double* gb3) {
+  const int I = ORC_MLP_IN, H = ORC_MLP_H, O = ORC_MLP_OUT;
+  memset(gw1, 0, sizeof(double) * H * I); memset(gb1, 0, sizeof(double) * H);
+  memset(gw2, 0, sizeof(double) * H * H); memset(gb2, 0, sizeof(double) * H);
+  memset(gw3, 0, sizeof(double) * O * H); memset(gb3, 0, sizeof(double) * O);
+  double loss = 0.0;
+  for (int b = 0; b < B; b++) {
+    const float* x = X + (size_t)b * I;
+    double a1[ORC_MLP_H], h1[ORC_MLP_H], a2[ORC_MLP_H], h2[ORC_MLP_H], z[ORC_MLP_OUT], g[ORC_MLP_OUT];
+    for (int h = 0; h < H; h++) {
+      double a = M->b1[h];
+      for (int k = 0; k < I; k++) a += (double)bf16f(M->w1[h * I + k]) * x[k];
+      a1[h] = a; h1[h] = a > 0 ? a : 0;
+    }
+    for (int h = 0; h < H; h++) {
+      double a = M->b2[h];
+      for (int k = 0; k < H; k++) a += (double)bf16f(M->w2[h * H + k]) * h1[k];
+      a2[h] = a; h2[h] = a > 0 ? a : 0;
+    }
+    double zmax = -1e300;
+    for (int o = 0; o < O; o++) {
+      double a = M->b3[o];
+      for (int k = 0; k < H; k++) a += (double)bf16f(M->w3[o * H + k]) * h2[k];
+      z[o] = a;
+      if (((mask[b] >> o) & 1u) && a > zmax) zmax = a;
+    }
+    double S = 0.0;
+    for (int o = 0; o < O; o++) S += ((mask[b] >> o) & 1u) ? exp(z[o] - zmax) : 0.0;
+    loss += -(z[y[b]] - zmax - log(S));
+    for (int o = 0; o < O; o++) g[o] = (((mask[b] >> o) & 1u) ? exp(z[o] - zmax) / S : 0.0) - (o == y[b] ? 1.0 : 0.0);
+    double d2[ORC_MLP_H], d1[ORC_MLP_H];
+    for (int k = 0; k < H; k++) d2[k] = 0;
+    for (int o = 0; o < O; o++) {
+      gb3[o] += g[o];
+      for (int k = 0; k < H; k++) { gw3[o * H + k] += g[o] * h2[k]; d2[k] += g[o] * (double)bf16f(M->w3[o * H + k]); }
+    }
+    for (int k = 0; k < H; k++) d2[k] = a2[k] > 0 ? d2[k] : 0;
+    for (int k = 0; k < H; k++) d1[k] = 0;
+    for (int h = 0; h < H; h++) {
+      gb2[h] += d2[h];
+      for (int k = 0; k < H; k++) { gw2[h * H + k] += d2[h] * h1[k]; d1[k] += d2[h] * (double)bf16f(M->w2[h * H + k]); }
+    }
+    for (int k = 0; k < H; k++) d1[k] = a1[k] > 0 ? d1[k] : 0;
+    for (int h = 0; h < H; h++) {
+      gb1[h] += d1[h];
+      for (int k = 0; k < I; k++) gw1[h * I + k] += d1[h] * x[k];
+    }
+  }
+  const double inv = 1.0 / (B > 0 ? B : 1);
+  for (int k = 0; k < H * I; k++) gw1[k] *= inv;
+  for (int k = 0; k < H; k++) { gb1[k] *= inv; gb2[k] *= inv; }
+  for (int k = 0; k < H * H; k++) gw2[k] *= inv;
+  for (int k = 0; k < O * H; k++) gw3[k] *= inv;
+  for (int k = 0; k < O; k++) gb3[k] *= inv;
+  return loss * inv;
+}
+
 /* Birth mutation (bart_kernel.cpp:489-501); returns 0 on node-cap. */
 static int do_birth(otree* t, int nx, int v, int c, const int* nc, int p, int* L_out, int* R_out) {
   int L = first_free(t->used, -1), R = first_free(t->used, L);
@@ -606,7 +816,21 @@ static int fit_dev(const orc_chain* C, orc_out* o) {
       uint32_t x[4];
       philox_seed(seed, 0u, (uint32_t)j, (uint32_t)it, ORC_TAG_PROP, x);
       dunif du = {{u32d(x[0]), u32d(x[1]), u32d(x[2]), u32d(x[3])}, 0};
-      oprop cp = propose(t, PG, nc, p, dunif_cb, &du, 1);
+      oprop cp;
+      float feat[ORC_MLP_IN];
+      uint32_t fvalid = 0;
+      if (C->model && C->model->mix > 0.0) {
+        uint32_t x2[4];
+        philox_seed(seed, 0u, (uint32_t)j, (uint32_t)it, ORC_TAG_PROP2, x2);
+        const double u2[2] = {u32d(x2[0]), u32d(x2[1])};
+        cp = propose_model(t, PG, nc, p, du.u, u2, C->model, LF + (size_t)j * n, n, feat, &fvalid);
+      } else {
+        cp = propose(t, PG, nc, p, dunif_cb, &du, 1);
+        if (o->train_cap > 0 && cp.mode == 1) {
+          /* the birth node is the one propose() chose */
+          fvalid = orc_features(t, cp.nx, count_rows(LF + (size_t)j * n, n, cp.nx, cp.nx), -1, nc, p, feat);
+        }
+      }
       orc_prop cpp = {cp.mode, cp.nx, cp.v, cp.c};
       float thc[ORC_NODES];
       for (int s = 0; s < ORC_NODES; s++) thc[s] = t->th[s];
@@ -633,6 +857,12 @@ static int fit_dev(const orc_chain* C, orc_out* o) {
                 S0[L] = st.sL0; S1[L] = st.sL1; S0[Rr] = st.sR0; S1[Rr] = st.sR1;
                 nu_.mode = 1; nu_.L = L; nu_.R = Rr;
                 n_birth++;
+                if (o->train_cap > 0 && o->train_count < o->train_cap) {
+                  memcpy(o->train_x + (size_t)o->train_count * ORC_MLP_IN, feat, sizeof feat);
+                  o->train_y[o->train_count] = cp.v;
+                  o->train_mask[o->train_count] = fvalid;
+                  o->train_count++;
+                }
               }
             }
           }

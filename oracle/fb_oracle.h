@@ -36,8 +36,22 @@ enum { ORC_MODE_REF = 0, ORC_MODE_DEV = 1 };
 
 /* Philox counter tags (word 3 of the counter) used by the DEV arithmetic. */
 enum { ORC_TAG_PROP = 1, ORC_TAG_MH = 2, ORC_TAG_MU = 3, ORC_TAG_SIG_N = 4, ORC_TAG_SIG_U = 5, ORC_TAG_Z_N = 6,
-       ORC_TAG_Z_E = 7 };
+       ORC_TAG_Z_E = 7, ORC_TAG_PROP2 = 8 };
 #define ORC_INIT_SWEEP 0xFFFFFFFFu
+
+/* Learned split-variable proposal (DEV mode): an MLP of ORC_MLP_IN node features -> ORC_MLP_H -> ORC_MLP_H ->
+ * ORC_MLP_OUT logits (ReLU between), BF16 weights, FP32 arithmetic without fused multiply-add.  A birth draws its
+ * variable from the model's masked softmax with probability mix, else uniformly as BART does; the MH ratio carries
+ * the exact proposal probabilities (birth and reverse death), so the chain targets the same posterior. */
+#define ORC_MLP_IN 98
+#define ORC_MLP_H 64
+#define ORC_MLP_OUT 32
+typedef struct {
+  const uint16_t* w1; const float* b1;   /* [H][IN] bf16, [H] */
+  const uint16_t* w2; const float* b2;   /* [H][H], [H] */
+  const uint16_t* w3; const float* b3;   /* [OUT][H], [OUT] */
+  double mix;                            /* probability of the model component (0: plain proposal) */
+} orc_model;
 
 typedef struct {
   int n, p, m, nskip, ndpost;
@@ -52,6 +66,7 @@ typedef struct {
   int probit;
   int fx_shift;           /* DEV: w and w*r are summed as llrint(x * 2^fx_shift) */
   int rss_shift;          /* DEV: w*e^2 is summed as llrint(x * 2^rss_shift) */
+  const orc_model* model; /* DEV: learned proposal, or NULL */
 } orc_chain;
 
 typedef struct {
@@ -61,6 +76,12 @@ typedef struct {
   uint64_t* trees;        /* [ndpost][m][64] packed nodes (bart_kernel.cpp:559-571); may be NULL */
   int moves[3];           /* births, deaths, node-cap hits */
   int rtnorm_caps;        /* DEV: truncated-normal draws that hit their iteration cap */
+  /* DEV: accepted births as training examples (features at the node before the birth, split variable, mask of the
+   * variables with a non-empty cut range there), in step order; train_cap 0 disables */
+  float* train_x;         /* [train_cap][ORC_MLP_IN] */
+  int* train_y;
+  uint32_t* train_mask;
+  int train_cap, train_count;
 } orc_out;
 
 /* Whole-chain sampler.  Returns 0 on success, <0 on a bad shape. */
@@ -81,6 +102,14 @@ void orc_pass_dev(int n, uint8_t* leaf_prev, const uint8_t* leaf_cur, float* r, 
 
 /* ---------------------------------------------------------------- DEV arithmetic primitives (exported for tests) */
 void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* MLP forward on one feature vector: logits [ORC_MLP_OUT]. */
+void orc_mlp_logits(const orc_model* M, const float* x, float* z);
+/* Masked softmax of the logits in FP64 with orc_exp; q[v] = 0 for masked v. */
+void orc_mlp_probs(const float* z, uint32_t valid, double* q);
+/* Mean masked cross-entropy over a batch and its gradients with respect to the (BF16-valued) weights and biases,
+ * computed in FP64 from the same BF16 weights (the checker of the device training kernels). */
+double orc_mlp_loss_grad(const orc_model* M, const float* X, const int* y, const uint32_t* mask, int B,
+                         double* gw1, double* gb1, double* gw2, double* gb2, double* gw3, double* gb3);
 double orc_log(double x);
 double orc_exp(double x);
 double orc_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag);

@@ -34,12 +34,31 @@ class _Chain(C.Structure):
                 ("numcut", C.c_void_p), ("pgtab", C.c_void_p),
                 ("tau", C.c_double), ("lambda_", C.c_double), ("nu", C.c_double), ("sigest", C.c_double),
                 ("offset", C.c_double), ("seed", C.c_uint64), ("probit", C.c_int), ("fx_shift", C.c_int),
-                ("rss_shift", C.c_int)]
+                ("rss_shift", C.c_int), ("model", C.c_void_p)]
 
 
 class _Out(C.Structure):
     _fields_ = [("sigma", C.c_void_p), ("fmean", C.c_void_p), ("yhat", C.c_void_p), ("trees", C.c_void_p),
-                ("moves", C.c_int * 3), ("rtnorm_caps", C.c_int)]
+                ("moves", C.c_int * 3), ("rtnorm_caps", C.c_int), ("train_x", C.c_void_p), ("train_y", C.c_void_p),
+                ("train_mask", C.c_void_p), ("train_cap", C.c_int), ("train_count", C.c_int)]
+
+
+MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
+
+
+class _Model(C.Structure):
+    _fields_ = [("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_void_p), ("mix", C.c_double)]
+
+
+def _model_struct(model: dict, keep: list):
+    """orc_model from a dict of w1 [64][98], w2 [64][64], w3 [32][64] (uint16 BF16 bits), b1, b2, b3 (float32), mix."""
+    arrs = {}
+    for k, dt in (("w1", np.uint16), ("w2", np.uint16), ("w3", np.uint16), ("b1", np.float32), ("b2", np.float32),
+                  ("b3", np.float32)):
+        arrs[k] = np.ascontiguousarray(model[k], dtype=dt)
+        keep.append(arrs[k])
+    return _Model(*(arrs[k].ctypes.data for k in ("w1", "b1", "w2", "b2", "w3", "b3")), float(model.get("mix", 0.5)))
 
 
 class _Upd(C.Structure):
@@ -94,6 +113,10 @@ def lib():
         L.orc_compile_trees.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(_CT)]
         L.orc_compile_trees.restype = C.c_int
         L.orc_ct_free.argtypes = [C.POINTER(_CT)]
+        L.orc_mlp_logits.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_mlp_logits.restype = None
+        L.orc_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 6
+        L.orc_mlp_loss_grad.restype = C.c_double
         L.orc_predict_draw.argtypes = [C.POINTER(_CT), C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, _f64p]
         L.orc_predict_draw.restype = C.c_int
         L.orc_trees_text.argtypes = [_u64p, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
@@ -125,9 +148,10 @@ def _keep(*arrs):
     return [np.ascontiguousarray(a) for a in arrs]
 
 
-def fit(ch: dict, mode: int, want_trees: bool = True) -> dict:
+def fit(ch: dict, mode: int, want_trees: bool = True, model: dict | None = None, train_cap: int = 0) -> dict:
     """Runs one chain in the oracle.  ch keys: q [p][n] u8, y, wt, ybin, numcut, pgtab, tau, lambda, nu, sigest,
-    offset, seed, probit, nskip, ndpost, ntree, fx_shift, rss_shift."""
+    offset, seed, probit, nskip, ndpost, ntree, fx_shift, rss_shift.  DEV mode: `model` = learned proposal (see
+    _model_struct); train_cap > 0 collects accepted births as training examples (train_x, train_y, train_mask)."""
     q = np.ascontiguousarray(ch["q"], dtype=np.uint8)
     p, n = q.shape
     m, nskip, ndpost = int(ch["ntree"]), int(ch["nskip"]), int(ch["ndpost"])
@@ -140,18 +164,51 @@ def fit(ch: dict, mode: int, want_trees: bool = True) -> dict:
     c = _Chain(n, p, m, nskip, ndpost, q.ctypes.data, y.ctypes.data, wt.ctypes.data, ybin.ctypes.data,
                numcut.ctypes.data, pg.ctypes.data, ch["tau"], ch["lambda"], ch["nu"], ch["sigest"],
                ch.get("offset", 0.0), int(ch["seed"]) & 0xFFFFFFFFFFFFFFFF, probit, int(ch.get("fx_shift", 32)),
-               int(ch.get("rss_shift", 24)))
+               int(ch.get("rss_shift", 24)), None)
+    keep: list = []
+    if model is not None:
+        ms = _model_struct(model, keep)
+        keep.append(ms)
+        c.model = C.cast(C.pointer(ms), C.c_void_p)
     S = nskip + ndpost
     sigma = np.zeros(S)
     fmean = np.zeros(n)
     yhat = np.zeros((ndpost, n))
     trees = np.zeros((ndpost, m, NODES), dtype=np.uint64) if want_trees or mode == MODE_REF else None
+    tx = np.zeros((max(train_cap, 1), MLP_IN), dtype=np.float32)
+    ty = np.zeros(max(train_cap, 1), dtype=np.int32)
+    tm = np.zeros(max(train_cap, 1), dtype=np.uint32)
     o = _Out(sigma.ctypes.data, fmean.ctypes.data, yhat.ctypes.data, trees.ctypes.data if trees is not None else None)
+    o.train_x, o.train_y, o.train_mask, o.train_cap = tx.ctypes.data, ty.ctypes.data, tm.ctypes.data, int(train_cap)
     rc = lib().orc_fit(C.byref(c), mode, C.byref(o))
     if rc != 0:
         raise ValueError(f"orc_fit returned {rc}")
+    k = o.train_count
     return dict(sigma=sigma, fmean=fmean, yhat=yhat, trees=trees, moves=np.array(list(o.moves)),
-                rtnorm_caps=o.rtnorm_caps)
+                rtnorm_caps=o.rtnorm_caps, train_x=tx[:k], train_y=ty[:k], train_mask=tm[:k])
+
+
+def mlp_logits(model: dict, x: np.ndarray) -> np.ndarray:
+    keep: list = []
+    ms = _model_struct(model, keep)
+    xs = np.ascontiguousarray(x, dtype=np.float32)
+    z = np.zeros(MLP_OUT, dtype=np.float32)
+    lib().orc_mlp_logits(C.byref(ms), xs.ctypes.data, z.ctypes.data)
+    return z
+
+
+def mlp_loss_grad(model: dict, X, y, mask) -> tuple[float, dict]:
+    """Mean masked cross-entropy and its FP64 gradients (the checker of the device training kernels)."""
+    keep: list = []
+    ms = _model_struct(model, keep)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.int32)
+    mask = np.ascontiguousarray(mask, dtype=np.uint32)
+    g = {k: np.zeros(sh) for k, sh in (("w1", (MLP_H, MLP_IN)), ("b1", MLP_H), ("w2", (MLP_H, MLP_H)), ("b2", MLP_H),
+                                      ("w3", (MLP_OUT, MLP_H)), ("b3", MLP_OUT))}
+    loss = lib().orc_mlp_loss_grad(C.byref(ms), X.ctypes.data, y.ctypes.data, mask.ctypes.data, len(y),
+                                   *(g[k].ctypes.data for k in ("w1", "b1", "w2", "b2", "w3", "b3")))
+    return float(loss), g
 
 
 def ref_fit(ch: dict) -> dict:

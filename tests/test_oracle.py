@@ -144,3 +144,41 @@ def test_text_compile_predict_roundtrip(orc):
     internal = np.array([[((a["trees"][d, j] >> np.uint64(16)) & np.uint64(255)) != 0 for j in range(10)]
                          for d in range(5)]).reshape(5, -1).sum(axis=1)
     assert np.array_equal(vc.sum(axis=1), internal)
+
+
+def _rand_model(seed, scale=0.3, mix=0.5):
+    rng = np.random.default_rng(seed)
+    bf = lambda a: ((np.asarray(a, np.float32).view(np.uint32).astype(np.uint64) + 0x7FFF
+                     + ((np.asarray(a, np.float32).view(np.uint32).astype(np.uint64) >> 16) & 1)) >> 16).astype(np.uint16)
+    return dict(w1=bf(rng.normal(0, scale, (64, 98))), b1=rng.normal(0, 0.1, 64).astype(np.float32),
+                w2=bf(rng.normal(0, scale, (64, 64))), b2=rng.normal(0, 0.1, 64).astype(np.float32),
+                w3=bf(rng.normal(0, scale, (32, 64))), b3=rng.normal(0, 0.5, 32).astype(np.float32), mix=mix)
+
+
+def test_oracle_model_proposal_and_collection(orc):
+    """mix 0 is BART's proposal bit for bit; collected examples are the accepted births with valid labels."""
+    ch = W.fwbart_friedman(n=300, p=7, seed=5, ntree=15, nskip=20, ndpost=10)
+    plain = orc.fit(ch, orc.MODE_DEV, train_cap=10000)
+    m0 = orc.fit(ch, orc.MODE_DEV, model=_rand_model(1, mix=0.0))
+    assert np.array_equal(plain["sigma"], m0["sigma"]) and np.array_equal(plain["trees"], m0["trees"])
+    assert len(plain["train_y"]) == plain["moves"][0] > 0
+    assert all((mk >> yy) & 1 for mk, yy in zip(plain["train_mask"], plain["train_y"]))
+    m5 = orc.fit(ch, orc.MODE_DEV, model=_rand_model(1, mix=0.5))
+    assert np.isfinite(m5["sigma"]).all() and m5["moves"][0] > 0
+
+
+def test_oracle_mlp_gradient_finite_differences(orc):
+    ch = W.fwbart_friedman(n=300, p=7, seed=5, ntree=15, nskip=20, ndpost=10)
+    d = orc.fit(ch, orc.MODE_DEV, train_cap=10000)
+    x, y, m = d["train_x"][:40], d["train_y"][:40], d["train_mask"][:40]
+    model = _rand_model(2, scale=0.2)
+    loss, g = orc.mlp_loss_grad(model, x, y, m)
+    for key, idx in (("b3", 3), ("b2", 10), ("b1", 7), ("b3", 0)):
+        h = 1e-3
+        mp = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in model.items()}
+        mm = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in model.items()}
+        mp[key][idx] += h
+        mm[key][idx] -= h
+        fd = (orc.mlp_loss_grad(mp, x, y, m)[0] - orc.mlp_loss_grad(mm, x, y, m)[0]) / (
+            float(mp[key][idx]) - float(mm[key][idx]))
+        assert abs(fd - g[key][idx]) <= 2e-3 + 2e-2 * abs(g[key][idx]), (key, idx, fd, g[key][idx])
