@@ -505,6 +505,88 @@ def bench_predict(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------ learned proposal
+LRN_N, LRN_P, LRN_CHAINS, LRN_TRAIN = 65_536, 32, 16, 200_000
+LRN_METRIC = "ESS/s of sigma and f, learned vs plain proposal (16 fwbart chains, n 65,536, p 32, 27 noise predictors)"
+
+
+def bench_learned(args):
+    """Sparse-signal configuration: Friedman-5 on x1..x5 of 32 uniform predictors, numcut 255, 16 chains, ntree 200,
+    nskip 1000, ndpost 100.  A plain batch (different seeds) supplies accepted births as training examples; the MLP
+    trains on 200,000 of them on the device; then plain and learned batches run from the same seeds, timed with CUDA
+    events, and their ESS/s (sigma; median over rows of f) and posterior agreement are reported."""
+    import torch
+    import fastbart_b200 as F
+    from fastbart_b200 import diagnostics, workloads as W
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    S = NSKIP + NDPOST
+
+    def chains(seed0):
+        out = W.friedman_large(nchains=LRN_CHAINS, n=LRN_N, p=LRN_P, seed=0, nskip=NSKIP, ndpost=NDPOST, ntree=NTREE)
+        for k, c in enumerate(out):
+            c["seed"] = seed0 + k
+        return out
+
+    stream = torch.cuda.current_stream()
+
+    def timed(b, steps, warmup):
+        for _ in range(warmup):
+            b.run(stream.cuda_stream)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, c in evs:
+            a.record(stream)
+            b.run(stream.cuda_stream)
+            c.record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(c) for a, c in evs) / 1000.0 / steps
+
+    col = F.Batch(chains(900), NSKIP, NDPOST)
+    col.collect(2 * LRN_TRAIN)
+    col.run(stream.cuda_stream)
+    col.sync()
+    x, y, m, births = col.training_data()
+    col.close()
+    k = min(LRN_TRAIN, len(y))
+    t = time.perf_counter()
+    model, losses = F.train_proposal(x[:k], y[:k], m[:k], epochs=10, batch=1024, lr=3e-3, seed=1)
+    train_s = time.perf_counter() - t
+    res = {}
+    steps = max(1, min(args.steps, 2))
+    for name, mdl in (("plain", None), ("learned", dict(model, mix=0.5))):
+        b = F.Batch(chains(100), NSKIP, NDPOST)
+        if mdl is not None:
+            b.set_proposal(mdl)
+        sec = timed(b, steps, 1)
+        outs = b.download(trees=False)
+        b.close()
+        es = [diagnostics.chain_ess(o["sigma"][NSKIP:], o["yhat"]) for o in outs]
+        res[name] = {"seconds_per_batch": sec, "chain_sweeps_per_s": LRN_CHAINS * S / sec,
+                     "ess_sigma_per_s": float(sum(e["sigma"] for e in es) / sec),
+                     "ess_f_median_per_s": float(sum(e["f_median"] for e in es) / sec),
+                     "births": int(sum(o["moves"][0] for o in outs)),
+                     "fmean": np.mean([o["yhat_mean"] for o in outs], axis=0),
+                     "sigma": float(np.mean([o["sigma"][NSKIP:].mean() for o in outs]))}
+    corr = float(np.corrcoef(res["plain"]["fmean"], res["learned"]["fmean"])[0, 1])
+    sig = res["learned"]["sigma"] / res["plain"]["sigma"]
+    for r in res.values():
+        del r["fmean"]
+    line = {"metric": LRN_METRIC, "value": res["learned"]["ess_f_median_per_s"] / res["plain"]["ess_f_median_per_s"],
+            "unit": "x (ESS/s of f, learned / plain)", "n_gpus": 1, "steps": steps, "warmup": 1,
+            "ms_per_step": 1000 * res["learned"]["seconds_per_batch"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64-fixed+f32+f64 (MLP bf16/f32)", "data": "synthetic",
+            "config": {"workload": "friedman_sparse_16x65536", "chains": LRN_CHAINS, "n": LRN_N, "p": LRN_P,
+                       "numcut": 255, "ntree": NTREE, "nskip": NSKIP, "ndpost": NDPOST, "mix": 0.5,
+                       "training_examples": int(k), "accepted_births_collected": int(births)},
+            "sigma_ratio": float(res["learned"]["ess_sigma_per_s"] / res["plain"]["ess_sigma_per_s"]),
+            "plain": res["plain"], "learned": res["learned"],
+            "training": {"seconds": train_s, "epochs": 10, "loss_first": float(losses[0]),
+                         "loss_last": float(losses[-1]), "uniform_loss": float(np.log(LRN_P)),
+                         "signal_fraction_of_births": float(np.mean(y[:k] < 5))},
+            "agreement": {"corr_fmean": corr, "sigma_ratio": float(sig)}, "gpu_launches": 2 * steps + 2}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -515,12 +597,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="titer96", choices=["titer96", "small", "predict"])
+    ap.add_argument("--workload", default="titer96", choices=["titer96", "small", "predict", "learned"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "predict":
         return bench_predict(args)
+    if args.workload == "learned":
+        return bench_learned(args)
     set_workload(args.workload)
     if args.impl == "reference":
         return bench_reference(args)
