@@ -51,7 +51,7 @@ class Chain(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("nskip", C.c_int), ("ndpost", C.c_int), ("threads", C.c_int), ("sweeps_per_launch", C.c_int),
-                ("device", C.c_int)]
+                ("device", C.c_int), ("cluster", C.c_int)]
 
 
 class ChainOut(C.Structure):

@@ -62,18 +62,18 @@ def _collect(o: dict, s: _lib.ChainOut) -> dict:
     return o
 
 
-def _options(nskip, ndpost, threads=0, sweeps_per_launch=0, device=0) -> _lib.Options:
-    return _lib.Options(int(nskip), int(ndpost), int(threads), int(sweeps_per_launch), int(device))
+def _options(nskip, ndpost, threads=0, sweeps_per_launch=0, device=0, cluster=0) -> _lib.Options:
+    return _lib.Options(int(nskip), int(ndpost), int(threads), int(sweeps_per_launch), int(device), int(cluster))
 
 
 def fit_batch(chains: Sequence[dict], nskip: int, ndpost: int, threads: int = 0, sweeps_per_launch: int = 0,
-              device: int = 0, trees: bool = True) -> list:
+              device: int = 0, trees: bool = True, cluster: int = 0) -> list:
     """Runs prepared chains (dicts as built by workloads.fwbart_chain / fpbart_chain) in one device batch."""
     keep: list = []
     arr = (_lib.Chain * len(chains))(*[_as_chain(c, keep) for c in chains])
     outs = [_alloc_out(c, nskip, ndpost, trees) for c in chains]
     oarr = (_lib.ChainOut * len(chains))(*[s for _, s in outs])
-    opt = _options(nskip, ndpost, threads, sweeps_per_launch, device)
+    opt = _options(nskip, ndpost, threads, sweeps_per_launch, device, cluster)
     check(_lib.lib().fb_fit_batch(arr, len(chains), C.byref(opt), oarr))
     return [_collect(o, oarr[k]) for k, (o, _) in enumerate(outs)]
 
@@ -82,12 +82,12 @@ class Batch:
     """Staged batch: inputs uploaded once; run() repeats the full MCMC on the device; download() copies outputs."""
 
     def __init__(self, chains: Sequence[dict], nskip: int, ndpost: int, threads: int = 0, sweeps_per_launch: int = 0,
-                 device: int = 0):
+                 device: int = 0, cluster: int = 0):
         self._keep: list = []
         self.chains = list(chains)
         self.nskip, self.ndpost = int(nskip), int(ndpost)
         arr = (_lib.Chain * len(chains))(*[_as_chain(c, self._keep) for c in chains])
-        opt = _options(nskip, ndpost, threads, sweeps_per_launch, device)
+        opt = _options(nskip, ndpost, threads, sweeps_per_launch, device, cluster)
         h = C.c_void_p()
         check(_lib.lib().fb_batch_create(arr, len(chains), C.byref(opt), C.byref(h)))
         self._h = h

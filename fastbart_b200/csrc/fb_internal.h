@@ -73,8 +73,9 @@ struct DBufs {
   int* queue;
   int nchains;
   int m_max;
-  int n_pad_max;
+  int n_pad_max;                   // rows of one CTA's slice (shared-memory capacity)
   int rows_in_smem;
+  int cluster;                     // CTAs per chain (a thread-block cluster when > 1)
   // learned split-variable proposal (null mw1: BART's uniform proposal)
   const uint16_t* mw1; const float* mb1;   // [MLP_H][MLP_IN] bf16, [MLP_H]
   const uint16_t* mw2; const float* mb2;   // [MLP_H][MLP_H], [MLP_H]
@@ -93,8 +94,10 @@ struct DBufs {
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem);
 // groups of 4 rows per row thread held in registers (1, 2, 4, 8), or 0 when the rows stream from L2 in the pass
 int sampler_gmax(int threads, int n_pad_max);
-int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, void* stream);
-int sampler_max_grid(int threads, size_t smem, int device, int gmax);
+int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
+                   void* stream);
+// CTAs that can be resident at once (a multiple of cluster), 0 when none
+int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster);
 
 // Per-tree pass on explicit state (diagnostics / parity tests): one CTA.
 struct DPassArgs {

@@ -99,6 +99,8 @@ struct fb_batch {
   long long rows = 0, qbytes = 0, leafbytes = 0, ntrees = 0, nsig = 0, nyhat = 0, ntout = 0;
   cudaStream_t stream = nullptr;
   void* model_mem = nullptr;   // learned proposal weights (owned; also listed in allocs)
+  int cluster = 1;             // CTAs per chain
+  int slice_rows = 0;          // rows of one CTA's slice (shared-memory capacity)
   int collect_cap = 0;         // allocated capacity of the training-example buffers
   ~fb_batch() {
     int cur = 0;
@@ -174,16 +176,31 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
     T = nchains <= nsm ? 512 : 256;   // one chain per SM: widest CTA; more chains than SMs: two CTAs per SM
   }
-  int optin = 0;
+  int optin = 0, nsm = 148;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt->device) != cudaSuccess) optin = 232448;
-  int rows_in_smem = 1;
-  size_t smem = sampler_smem_bytes(T, m_max, n_pad_max, 1);
-  if (smem > (size_t)optin) { rows_in_smem = 0; smem = sampler_smem_bytes(T, m_max, n_pad_max, 0); }
-  if (smem > (size_t)optin) { delete b; return fail(FB_ERR_LIMIT, "shared memory %zu exceeds %d", smem, optin); }
-  const int gmax = sampler_gmax(T, n_pad_max);
-  const int maxgrid = sampler_max_grid(T, smem, opt->device, gmax);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
+  // CTAs per chain: a cluster splits each chain's rows over CS SMs when SMs would otherwise idle (or as requested)
+  int CS = 1;
+  if (opt->cluster > 0) CS = std::min(opt->cluster, 8);
+  else
+    for (int c : {8, 4, 2})
+      if ((long long)nchains * c <= nsm && n_pad_max / c >= 2048) { CS = c; break; }
+  int rows_in_smem = 1, gmax = 0, maxgrid = 0;
+  size_t smem = 0;
+  for (;;) {
+    const int cap = 4 * ((n_pad_max / 4 + CS - 1) / CS);   // rows of one CTA's slice
+    rows_in_smem = 1;
+    smem = sampler_smem_bytes(T, m_max, cap, 1);
+    if (smem > (size_t)optin) { rows_in_smem = 0; smem = sampler_smem_bytes(T, m_max, cap, 0); }
+    if (smem > (size_t)optin) { delete b; return fail(FB_ERR_LIMIT, "shared memory %zu exceeds %d", smem, optin); }
+    gmax = sampler_gmax(T, cap);
+    maxgrid = sampler_max_grid(T, smem, opt->device, gmax, CS);   // CTAs (whole clusters) that can be resident
+    if (maxgrid > 0 || CS == 1) { b->slice_rows = cap; break; }
+    CS = 1;   // clusters of this shape cannot be resident: one CTA per chain
+  }
   if (maxgrid <= 0) { delete b; return fail(FB_ERR_CUDA, "sampler kernel cannot be resident with %zu bytes of shared memory", smem); }
-  b->threads = T; b->smem = smem; b->grid = std::min(nchains, maxgrid); b->gmax = gmax;
+  b->cluster = CS;
+  b->threads = T; b->smem = smem; b->grid = std::min(nchains * CS, maxgrid); b->gmax = gmax;
   b->spl = opt->sweeps_per_launch > 0 ? opt->sweeps_per_launch : S;
   b->launches = (S + b->spl - 1) / b->spl;
 
@@ -201,8 +218,8 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   fb_status s = FB_OK;
   if ((s = A(&dch, nchains)) || (s = A(&dst, nchains)) || (s = A(&dq, b->qbytes)) || (s = A(&dyin, b->rows)) ||
       (s = A(&dyw, b->rows)) || (s = A(&dw, b->rows)) || (s = A(&dyb, b->rows)) || (s = A(&drs, b->rows)) || (s = A(&dws, b->rows)) ||
-      (s = A(&dleaf, b->leafbytes)) || (s = A(&dtr, b->ntrees)) || (s = A(&ds0, b->ntrees * LEAF_STAT_WORDS)) ||
-      (s = A(&dth, b->ntrees * NODES)) || (s = A(&dtm, b->rows)) || (s = A(&dsig, b->nsig)) ||
+      (s = A(&dleaf, b->leafbytes)) || (s = A(&dtr, b->ntrees * CS)) ||
+      (s = A(&ds0, b->ntrees * CS * LEAF_STAT_WORDS)) || (s = A(&dth, b->ntrees * CS * NODES)) || (s = A(&dtm, b->rows)) || (s = A(&dsig, b->nsig)) ||
       (s = A(&dyh, b->nyhat)) || (s = A(&dto, b->ntout)) || (s = A(&dord, nchains)) || (s = A(&dqueue, 1))) {
     delete b;
     return s;
@@ -234,7 +251,7 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   d.chains = dch; d.states = dst; d.q = dq; d.yin = dyin; d.ywork = dyw; d.win = dw; d.ybin = dyb; d.rsave = drs; d.wsave = dws;
   d.leaf = dleaf; d.trees = dtr; d.s0 = ds0; d.th = dth; d.tm = dtm; d.sigma_out = dsig; d.yhat_out = dyh;
   d.trees_out = dto; d.order = dord; d.queue = dqueue; d.nchains = nchains; d.m_max = m_max;
-  d.n_pad_max = n_pad_max; d.rows_in_smem = rows_in_smem;
+  d.n_pad_max = b->slice_rows; d.rows_in_smem = rows_in_smem; d.cluster = CS;
   *out = b;
   return FB_OK;
 }
@@ -248,7 +265,7 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
     return fail(FB_ERR_CUDA, "cannot reset the training-example counter");
   for (int it0 = 0; it0 < S; it0 += b->spl) {
     const int it1 = std::min(S, it0 + b->spl);
-    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, b->gmax, stream) != 0)
+    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, b->gmax, b->cluster, stream) != 0)
       return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   return FB_OK;

@@ -33,6 +33,7 @@
 //   * Random numbers: Philox4x32-10 keyed by the chain seed, counter = (draw index, tree or row, sweep, purpose).
 //   * All control arithmetic is IEEE FP64 through fb_math.cuh; the file is compiled with -fmad=false.  The oracle's
 //     DEV mode (oracle/fb_oracle.c) restates exactly this arithmetic on the CPU.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -106,7 +107,7 @@ struct PassU {
   unsigned long long* ovb;    // [64] leaves with compact index >= NBS
   long long* tot;             // [TOT] CTA totals
   float DL, DR;
-  int n, ngroups, rt, RT, nleaf;
+  int n, g0, g1, rt, RT, nleaf;   // rows: groups [g0, g1) of this CTA (r and ws are indexed from group g0)
   int apply, pmode, pnx, pc, pL, pR, pl, pr;
   int cmode, cnx, cc;
 };
@@ -126,8 +127,8 @@ __device__ __forceinline__ void pass_group(const PassU& P, int g, const GroupWor
   const float* __restrict__ wp = P.ws;
   const float* __restrict__ Dp = P.D;
   const float2* __restrict__ tcp = P.tc;
-  const float4 r4 = reinterpret_cast<const float4*>(rp)[g];
-  const float4 w4 = reinterpret_cast<const float4*>(wp)[g];
+  const float4 r4 = reinterpret_cast<const float4*>(rp)[g - P.g0];
+  const float4 w4 = reinterpret_cast<const float4*>(wp)[g - P.g0];
   float rr[4] = {r4.x, r4.y, r4.z, r4.w};
   const float ww[4] = {w4.x, w4.y, w4.z, w4.w};
   if (P.apply) {
@@ -146,7 +147,7 @@ __device__ __forceinline__ void pass_group(const PassU& P, int g, const GroupWor
       if (byte_of(mv, e)) delta = byte_of(side, e) ? P.DL : P.DR;
       rr[e] = __fsub_rn(rr[e], delta);
     }
-    reinterpret_cast<float4*>(rp)[g] = make_float4(rr[0], rr[1], rr[2], rr[3]);
+    reinterpret_cast<float4*>(rp)[g - P.g0] = make_float4(rr[0], rr[1], rr[2], rr[3]);
     if (lpn != W.lp) *reinterpret_cast<uint32_t*>(P.leaf_prev + 4 * g) = lpn;
   }
   // rows of a birth proposal's node that go left (padding rows beyond n excluded)
@@ -204,7 +205,7 @@ __device__ __forceinline__ void reduce_totals(long long* bins, int RT, int nleaf
 __device__ void pass_rows_stream(const PassU& P) {
   long long sl0 = 0, sl1 = 0;
   int nl = 0;
-  for (int g = P.rt; g < P.ngroups; g += P.RT) {
+  for (int g = P.g0 + P.rt; g < P.g1; g += P.RT) {
     GroupWords W;
     W.lc = ld_u32(P.leaf_cur + 4 * g);
     W.lp = P.apply ? ld_u32(P.leaf_prev + 4 * g) : 0u;
@@ -225,8 +226,8 @@ __device__ __forceinline__ void pass_rows_regs(const PassU& P, bool first, uint3
   int nl = 0;
 #pragma unroll
   for (int k = 0; k < G; k++) {
-    const int g = P.rt + k * P.RT;
-    if (g < P.ngroups) {
+    const int g = P.g0 + P.rt + k * P.RT;
+    if (g < P.g1) {
       GroupWords W;
       if (first) {
         W.lc = ld_u32(P.leaf_cur + 4 * g);
@@ -245,8 +246,8 @@ __device__ __forceinline__ void pass_rows_regs(const PassU& P, bool first, uint3
   // the next tree's words: in flight while the control phase runs
 #pragma unroll
   for (int k = 0; k < G; k++) {
-    const int g = P.rt + k * P.RT;
-    if (g < P.ngroups && P.leaf_next) {
+    const int g = P.g0 + P.rt + k * P.RT;
+    if (g < P.g1 && P.leaf_next) {
       nlc[k] = ld_u32(P.leaf_next + 4 * g);
       nqc[k] = P.qnext ? __ldg(reinterpret_cast<const uint32_t*>(P.qnext + 4 * g)) : 0u;
     }
@@ -380,6 +381,43 @@ __device__ __forceinline__ double mix_prob(double mix, const double* q, int v, i
 // (else uniformly, as BART), and pr carries the proposal-probability correction of the birth, or of the reverse birth
 // of a death, so the chain keeps BART's target.  cnt: the tree's per-slot row counts.  When training examples are
 // collected, the birth node's features go to feat / *fvalid.
+// Birth variable from the learned model's mixture (see propose); *corr receives the proposal-ratio correction of the
+// drawn variable, feat / *fvalid the node's features when they are collected.
+__device__ __noinline__ int model_birth_var(const DTree* t, int nx, int cnt_nx, const DChain& C, const DBufs& B, int j,
+                                            int it, double uv, double* corr, float* feat, unsigned* fvalid) {
+  float xf[MLP_IN];
+  double q[MLP_OUT];
+  const unsigned valid = node_features(t, nx, cnt_nx, -1, C, xf);
+  model_probs(B, xf, valid, q);
+  const fbm::U4 y2 = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP2, C.seed);
+  const double umix = fbm::u32d(y2.x), uvm = fbm::u32d(y2.y);
+  int v;
+  if (umix < B.mix && valid) {
+    double cum = 0.0;
+    int last = 0;
+    v = -1;
+    for (int k = 0; k < MLP_OUT; k++)
+      if ((valid >> k) & 1u) { cum = cum + q[k]; last = k; if (v < 0 && uvm < cum) v = k; }
+    if (v < 0) v = last;
+  } else {
+    v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
+  }
+  *corr = ((valid >> v) & 1u) ? (1.0 / (double)C.p) / mix_prob(B.mix, q, v, C.p) : 1.0;
+  if (feat) { for (int k = 0; k < MLP_IN; k++) feat[k] = xf[k]; *fvalid = valid; }
+  return v;
+}
+
+// Proposal-ratio correction of a death of nx: the model's probability of the reverse birth (nx's split, in the tree
+// without it) over BART's.
+__device__ __noinline__ double model_death_corr(const DTree* t, int nx, int cnt_lr, const DChain& C, const DBufs& B) {
+  float xf[MLP_IN];
+  double q[MLP_OUT];
+  const unsigned valid = node_features(t, nx, cnt_lr, nx, C, xf);
+  model_probs(B, xf, valid, q);
+  return mix_prob(B.mix, q, (int)t->v[nx], C.p) * (double)C.p;
+}
+
+template <bool LP>
 __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cnt, int j, int it, Masks& mk,
                         float* feat, unsigned* fvalid) {
   const double pb = 0.5;
@@ -400,7 +438,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
   const double PBx = ngood == 0 ? 0 : (single ? 1 : pb);
   const fbm::U4 x = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP, C.seed);
   const double ub = fbm::u32d(x.x), un = fbm::u32d(x.y), uv = fbm::u32d(x.z), uc = fbm::u32d(x.w);
-  const bool model = B.mw1 != nullptr && B.mix > 0.0;
+  const bool model = LP && B.mw1 != nullptr && B.mix > 0.0;
   Prop P;
   P.mode = 0; P.nx = 0; P.v = 0; P.c = 0; P.l = 0; P.r = 0; P.pad0 = P.pad1 = 0; P.logpr = 0; P.lu = 0;
   double pr = 0;
@@ -408,28 +446,15 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
     const int nx = select_kth(goodm, (int)(un * ngood));
     int v;
     double corr = 1.0;
-    if (model) {
-      float xf[MLP_IN];
-      double q[MLP_OUT];
-      const unsigned valid = node_features(t, nx, cnt[nx], -1, C, xf);
-      model_probs(B, xf, valid, q);
-      const fbm::U4 y2 = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP2, C.seed);
-      const double umix = fbm::u32d(y2.x), uvm = fbm::u32d(y2.y);
-      if (umix < B.mix && valid) {
-        double cum = 0.0;
-        int last = 0;
-        v = -1;
-        for (int k = 0; k < MLP_OUT; k++)
-          if ((valid >> k) & 1u) { cum = cum + q[k]; last = k; if (v < 0 && uvm < cum) v = k; }
-        if (v < 0) v = last;
+    if constexpr (LP) {
+      if (model) {
+        v = model_birth_var(t, nx, cnt[nx], C, B, j, it, uv, &corr, feat, fvalid);
       } else {
         v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
+        if (feat) *fvalid = node_features(t, nx, cnt[nx], -1, C, feat);
       }
-      if ((valid >> v) & 1u) corr = (1.0 / (double)C.p) / mix_prob(B.mix, q, v, C.p);
-      if (feat) { for (int k = 0; k < MLP_IN; k++) feat[k] = xf[k]; *fvalid = valid; }
     } else {
       v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
-      if (feat) *fvalid = node_features(t, nx, cnt[nx], -1, C, feat);
     }
     int bL, bU;
     node_range(t, nx, v, C.numcut[v], bL, bU);
@@ -462,12 +487,8 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
     const int ng2 = ngood - (t->ngv[l] > 0) - (t->ngv[r] > 0) + 1;
     const double Pboty = (double)1 / ng2, PDx = 1 - PBx, Pnogx = (double)1 / nnogs;
     pr = ((1 - PGny) * PBy * Pboty) / (PGny * (1 - PGlx) * (1 - PGrx) * PDx * Pnogx);
-    if (model) {   // the reverse move: birth of nx's split in the tree without it
-      float xf[MLP_IN];
-      double q[MLP_OUT];
-      const unsigned valid = node_features(t, nx, cnt[l] + cnt[r], nx, C, xf);
-      model_probs(B, xf, valid, q);
-      pr = pr * (mix_prob(B.mix, q, (int)t->v[nx], C.p) * (double)C.p);
+    if constexpr (LP) {
+      if (model) pr = pr * model_death_corr(t, nx, cnt[l] + cnt[r], C, B);   // the reverse birth
     }
     P.mode = 2; P.nx = (uint8_t)nx; P.l = (uint8_t)l; P.r = (uint8_t)r;
   }
@@ -506,6 +527,9 @@ struct Smem {
   unsigned long long* ovb;      // [2][64]
   long long* red;               // [NW]
   Ctl* ctl;
+  long long* ctot;              // [2][TOT] cluster totals (sum over the cluster's CTAs)
+  unsigned long long* covb;     // [2][64]
+  long long* xch;               // [2][4] per-CTA values exchanged across the cluster (rss, latent-z caps, sum w)
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -529,9 +553,12 @@ __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_
   off[13] = o; o += align_up((size_t)NW * 8, 16);                            // red
   off[14] = o; o += align_up(sizeof(Ctl), 16);                               // ctl
   off[15] = o; o += (size_t)m_max * ZMAX * 8;                                // zall
+  off[16] = o; o += 2 * TOT * 8;                                             // ctot[2]
+  off[17] = o; o += 2 * NODES * 8;                                           // covb[2]
+  off[18] = o; o += 2 * 4 * 8;                                               // xch[2][4]
   return o;
 }
-constexpr int NOFF = 16;
+constexpr int NOFF = 19;
 
 __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max, int rows_in_smem) {
   size_t off[NOFF];
@@ -553,6 +580,9 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.red = reinterpret_cast<long long*>(base + off[13]);
   S.ctl = reinterpret_cast<Ctl*>(base + off[14]);
   S.zall = reinterpret_cast<double*>(base + off[15]);
+  S.ctot = reinterpret_cast<long long*>(base + off[16]);
+  S.covb = reinterpret_cast<unsigned long long*>(base + off[17]);
+  S.xch = reinterpret_cast<long long*>(base + off[18]);
   return S;
 }
 
@@ -589,20 +619,26 @@ __device__ __forceinline__ void fetch_tree(const Smem& S, const DTree* trees, co
   cp_async_commit();
 }
 
+// An accepted birth of tree j becomes a training example (control warp).
+__device__ __noinline__ void collect_example(const DBufs& B, const DChain& C, int j, int v, int lane) {
+  int idx = 0;
+  if (lane == 0) idx = atomicAdd(B.train_count, 1);
+  idx = __shfl_sync(0xffffffffu, idx, 0);
+  if (idx < B.train_cap) {
+    const float* f = B.feat + (C.off_tree + j) * MLP_IN;
+    for (int k = lane; k < MLP_IN; k += 32) B.train_x[(long long)idx * MLP_IN + k] = f[k];
+    if (lane == 0) { B.train_y[idx] = v; B.train_mask[idx] = B.feat_valid[C.off_tree + j]; }
+  }
+}
+
 // apply the decided move of tree j (ctl) to its topology and leaf statistics in buffer j & 1 and write the tree back
 // (control warp)
+template <bool LP>
 __device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTree* trees, long long* s0g, int j,
-                            int lane) {
+                            int lane, bool lead) {
   const Ctl& ctl = *S.ctl;
-  if (B.train_cap > 0 && ctl.pmode == 1) {   // an accepted birth becomes a training example
-    int idx = 0;
-    if (lane == 0) idx = atomicAdd(B.train_count, 1);
-    idx = __shfl_sync(0xffffffffu, idx, 0);
-    if (idx < B.train_cap) {
-      const float* f = B.feat + (C.off_tree + j) * MLP_IN;
-      for (int k = lane; k < MLP_IN; k += 32) B.train_x[(long long)idx * MLP_IN + k] = f[k];
-      if (lane == 0) { B.train_y[idx] = ctl.pv; B.train_mask[idx] = B.feat_valid[C.off_tree + j]; }
-    }
+  if constexpr (LP) {
+    if (B.train_cap > 0 && lead && ctl.pmode == 1) collect_example(B, C, j, ctl.pv, lane);
   }
   DTree* t = S.tree + (j & 1);
   long long* s0 = S.s0t + (j & 1) * LST;
@@ -632,44 +668,113 @@ __device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTre
 }
 
 // ------------------------------------------------------------------------------------------------ one chain
-template <int G>
+namespace cg = cooperative_groups;
+
+// Proposals of every tree of sweep it (one thread per tree) with the leaf-mu normals drawn ahead.
+template <bool LP>
+__device__ __forceinline__ void proposals_body(const Smem& S, const DBufs& B, const DChain& C, DTree* trees,
+                                               const long long* s0g, int it, bool lead) {
+  const int m = C.m;
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    Masks mk;
+    float* featj = (LP && B.train_cap > 0 && lead) ? B.feat + (C.off_tree + j) * MLP_IN : nullptr;
+    const Prop P = propose<LP>(trees + j, C, B, reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES), j, it,
+                               mk, featj, B.feat_valid + (C.off_tree + j));
+    S.prop[j] = P;
+    S.masks[j] = mk;
+    int k = 0;
+    for (unsigned long long cm = P.cand; cm && k < ZMAX; cm &= cm - 1ull, k++) {
+      const int sl = __ffsll((long long)cm) - 1;
+      S.zall[j * ZMAX + k] = fbm::fb_normal(C.seed, (uint32_t)sl << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
+    }
+  }
+}
+// Out of line for the learned-proposal kernels: the model's calls then save only this function's few live
+// registers, not the chain loop's.
+__device__ __noinline__ void proposals_model(const Smem& S, const DBufs& B, const DChain& C, DTree* trees,
+                                             const long long* s0g, int it, bool lead) {
+  proposals_body<true>(S, B, C, trees, s0g, it, lead);
+}
+
+// Sums of the cluster's per-CTA pass totals (tot, ovb of buffer cur) into ctot / covb; after a cluster barrier.
+__device__ __forceinline__ void cluster_totals(const Smem& S, int cur, int CS) {
+  cg::cluster_group cl = cg::this_cluster();
+  for (int k = threadIdx.x; k < TOT + NODES; k += blockDim.x) {
+    if (k < TOT) {
+      long long t = 0;
+      for (int r = 0; r < CS; r++) t += *cl.map_shared_rank(S.tot + cur * TOT + k, r);
+      S.ctot[cur * TOT + k] = t;
+    } else {
+      const int s = k - TOT;
+      unsigned long long t = 0;
+      for (int r = 0; r < CS; r++) t += *cl.map_shared_rank(S.ovb + cur * NODES + s, r);
+      S.covb[cur * NODES + s] = t;
+    }
+  }
+}
+
+// Sum over the cluster of one exchanged value (slot k of xch) of every CTA; after a cluster barrier.
+__device__ __forceinline__ long long cluster_value(const Smem& S, int k, int CS) {
+  cg::cluster_group cl = cg::this_cluster();
+  long long t = 0;
+  for (int r = 0; r < CS; r++) t += *cl.map_shared_rank(S.xch + k, r);
+  return t;
+}
+
+// One chain.  With B.cluster = CS > 1 the chain runs on a cluster of CS CTAs: each CTA owns a contiguous slice of the
+// rows (groups [g0, g1)) in its shared memory and runs every control step itself on identical inputs (the proposals,
+// Metropolis-Hastings, leaf draws and sigma come out bit-identical in every CTA, each on its own copy of the trees);
+// only the exact integer pass totals and the end-of-sweep rss cross the cluster, through distributed shared memory,
+// once per tree step.  Integer sums do not depend on order, so the results equal the one-CTA run bit for bit.
+template <int G, bool CL, bool LP>
 __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& S) {
   const DChain& C = B.chains[ci];
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const int RT = T - 32;
   const int n = C.n, m = C.m, n_pad = C.n_pad, ngroups = n_pad / 4;
+  const int CS = CL ? B.cluster : 1;
+  const int crank = CL ? (int)cg::this_cluster().block_rank() : 0;
+  const bool lead = crank == 0;   // writes the chain's outputs
+  const int per = (ngroups + CS - 1) / CS;
+  const int g0 = min(ngroups, crank * per), g1 = min(ngroups, g0 + per);
+  const int ns = 4 * (g1 - g0);   // this CTA's rows (padded)
   const unsigned long long seed = C.seed;
   const double t2 = C.tau * C.tau, a_prior = 1.0 / t2;
   const double sci = pow2(-C.fx_shift), rscale = pow2(C.rss_shift), rsci = pow2(-C.rss_shift);
   const float scale = (float)pow2(C.fx_shift);
   const uint8_t* q = B.q + C.off_q;
   uint8_t* leaf = B.leaf + C.off_leaf;
-  DTree* trees = B.trees + C.off_tree;
-  long long* s0g = B.s0 + C.off_tree * LST;
-  float* thg = B.th + C.off_tree * NODES;
+  const long long tb = C.off_tree * CS + (long long)crank * m;   // this CTA's copy of the chain's trees
+  DTree* trees = B.trees + tb;
+  long long* s0g = B.s0 + tb * LST;
+  float* thg = B.th + tb * NODES;
   double* ywork = B.ywork + C.off_row;
   const float* wg = B.win + C.off_row;
-  float* rg = B.rsave + C.off_row;
-  float* wsg = B.wsave + C.off_row;
+  float* rg = B.rsave + C.off_row + 4 * g0;   // this CTA's rows
+  float* wsg = B.wsave + C.off_row + 4 * g0;
   double* tm = B.tm + C.off_row;
-  float* r = B.rows_in_smem ? S.r : rg;
+  float* r = B.rows_in_smem ? S.r : rg;       // indexed from row 4 * g0
   float* ws = B.rows_in_smem ? S.ws : wsg;
   Ctl& ctl = *S.ctl;
   DState& st = B.states[ci];
-  const bool regs = G > 0 && ngroups <= G * RT;   // register-held words for this chain
+  const bool regs = G > 0 && (g1 - g0) <= G * RT;   // register-held words for this CTA's groups
 
   // ---------------------------------------------------------------- chain start or resume
   if (tid == 0) {
     if (it0 == 0) { ctl.sigma = C.sigest; ctl.births = ctl.deaths = ctl.caps = ctl.rtcaps = 0; }
-    else { ctl.sigma = st.sigma; ctl.births = st.births; ctl.deaths = st.deaths; ctl.caps = st.caps; ctl.rtcaps = st.rtcaps; }
+    else {
+      ctl.sigma = st.sigma; ctl.births = st.births; ctl.deaths = st.deaths; ctl.caps = st.caps;
+      ctl.rtcaps = lead ? st.rtcaps : 0;   // latent-z caps are counted per CTA and summed at the end
+    }
     ctl.pmode = 0;
   }
   for (int k = tid; k < (NBS + NSPLIT) * RT; k += T) S.bins[k] = 0;
   __syncthreads();
-  for (int i = tid; i < n_pad; i += T) ws[i] = __fmul_rn(wg[i], scale);   // exact: power-of-two scaling
+  for (int li = tid; li < ns; li += T) ws[li] = __fmul_rn(wg[4 * g0 + li], scale);   // exact: power-of-two scaling
   if (it0 == 0) {
     int caps = 0;
-    for (int i = tid; i < n_pad; i += T) {
+    for (int li = tid; li < ns; li += T) {
+      const int i = 4 * g0 + li;
       double y = 0.0;
       if (i < n) {
         if (C.probit)
@@ -678,16 +783,23 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         else y = B.yin[C.off_row + i];
       }
       ywork[i] = y;
-      r[i] = (float)y;
+      r[li] = (float)y;
       tm[i] = 0.0;
     }
     if (caps) atomicAdd(&ctl.rtcaps, caps);
-    for (long long k = tid; k < (long long)m * n_pad / 16; k += T)
-      reinterpret_cast<uint4*>(leaf)[k] = make_uint4(0u, 0u, 0u, 0u);
+    const int sg = g1 - g0;   // this CTA's groups of every tree's leaf ids
+    for (long long k = tid; k < (long long)m * sg; k += T)
+      *reinterpret_cast<uint32_t*>(leaf + (k / sg) * n_pad + 4 * (g0 + k % sg)) = 0u;
     for (int k = tid; k < m * NODES; k += T) S.th[k] = 0.0f;
     long long sw = 0;
-    for (int i = tid; i < n; i += T) sw += __float2ll_rn(__fmul_rn(wg[i], scale));
-    const long long swt = block_sum64(sw, S.red);
+    for (int li = tid; li < ns; li += T)
+      if (4 * g0 + li < n) sw += __float2ll_rn(__fmul_rn(wg[4 * g0 + li], scale));
+    long long swt = block_sum64(sw, S.red);
+    if (CL) {   // sum of w over the whole chain
+      if (tid == 0) S.xch[4 + 2] = swt;
+      cg::this_cluster().sync();
+      swt = cluster_value(S, 4 + 2, CS);
+    }
     // root-only trees: every word zero except ngv[0] (byte 384), used (byte 448) and leaf (byte 456)
     constexpr int TWORDS = (int)(sizeof(DTree) / 4);
     for (int k = tid; k < m * TWORDS; k += T) {
@@ -706,7 +818,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     }
   } else {
     if (B.rows_in_smem)
-      for (int i = tid; i < n_pad; i += T) S.r[i] = rg[i];
+      for (int li = tid; li < ns; li += T) S.r[li] = rg[li];
     for (int k = tid; k < m * NODES; k += T) S.th[k] = thg[k];
   }
   __syncthreads();
@@ -717,19 +829,8 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   for (int it = it0; it < it1; it++) {
     const double inv_s2 = 1.0 / (ctl.sigma * ctl.sigma);
     // ---------------------------------------------------------------- proposals, one thread per tree
-    for (int j = tid; j < m; j += T) {
-      Masks mk;
-      float* featj = B.train_cap > 0 ? B.feat + (C.off_tree + j) * MLP_IN : nullptr;
-      const Prop P = propose(trees + j, C, B, reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES), j, it,
-                             mk, featj, B.feat_valid + (C.off_tree + j));
-      S.prop[j] = P;
-      S.masks[j] = mk;
-      int k = 0;
-      for (unsigned long long cm = P.cand; cm && k < ZMAX; cm &= cm - 1ull, k++) {
-        const int sl = __ffsll((long long)cm) - 1;
-        S.zall[j * ZMAX + k] = fbm::fb_normal(seed, (uint32_t)sl << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
-      }
-    }
+    if constexpr (LP) proposals_model(S, B, C, trees, s0g, it, lead);
+    else proposals_body<false>(S, B, C, trees, s0g, it, lead);
     for (int k = tid; k < 2 * TOT; k += T) S.tot[k] = 0;
     for (int k = tid; k < 2 * NODES; k += T) S.ovb[k] = 0ull;
     __syncthreads();
@@ -742,6 +843,10 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       cp_async_wait_all();
     }
     __syncthreads();
+    // the first pass of a sweep loads its words itself: the held words are dead until here (keeps them out of the
+    // registers live across the proposal step's calls)
+#pragma unroll
+    for (int k = 0; k < (G > 0 ? G : 1); k++) lcr[k] = qcr[k] = nlc[k] = nqc[k] = 0u;
     // ---------------------------------------------------------------- trees
     for (int j = 0; j < m; j++) {
       const Prop P = S.prop[j];
@@ -764,7 +869,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         U.r = r; U.ws = ws; U.D = S.D; U.tc = S.tc + cur * NODES; U.bins = S.bins; U.ovb = S.ovb + cur * NODES;
         U.tot = S.tot + cur * TOT;
         U.DL = ctl.DL; U.DR = ctl.DR;
-        U.n = n; U.ngroups = ngroups; U.rt = tid - 32; U.RT = RT; U.nleaf = ctl.nleaf[cur];
+        U.n = n; U.g0 = g0; U.g1 = g1; U.rt = tid - 32; U.RT = RT; U.nleaf = ctl.nleaf[cur];
         U.apply = j > 0; U.pmode = ctl.pmode; U.pnx = ctl.pnx; U.pc = ctl.pc; U.pL = ctl.pL; U.pR = ctl.pR;
         U.pl = ctl.pl; U.pr = ctl.pr;
         U.cmode = P.mode; U.cnx = P.nx; U.cc = P.c;
@@ -778,7 +883,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         // control warp: commit tree j-1, fetch tree j+1 into the freed buffer, draw the normals of every slot that
         // can be a leaf of tree j after its move (current leaves, the two slots a birth would take, the node a death
         // would restore)
-        if (j > 0) commit_tree(S, C, B, trees, s0g, j - 1, lane);
+        if (j > 0) commit_tree<LP>(S, C, B, trees, s0g, j - 1, lane, lead);
         if (j + 1 < m && j > 0) fetch_tree(S, trees, s0g, j + 1, lane);
         const unsigned long long cand = P.cand;
         if (__popcll(cand) > ZMAX)
@@ -791,13 +896,17 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       }
       __syncthreads();
       reduce_totals(S.bins, RT, ctl.nleaf[cur], P.mode, S.tot + cur * TOT);
+      if (CL) {   // the chain's totals: every CTA's partial totals, read through distributed shared memory
+        cg::this_cluster().sync();
+        cluster_totals(S, cur, CS);
+      }
       __syncthreads();
       // ------------------------------------------------------------ phase B: MH and leaf draws, one thread per slot
       if (tid < NODES) {
         const int s = tid;
         const Masks mk = S.masks[j];
-        const long long* tot = S.tot + cur * TOT;
-        const unsigned long long* ovb = S.ovb + cur * NODES;
+        const long long* tot = (CL ? S.ctot : S.tot) + cur * TOT;
+        const unsigned long long* ovb = (CL ? S.covb : S.ovb) + cur * NODES;
         const float2* tcj = S.tc + cur * NODES;
         const long long* s0 = S.s0t + cur * LST;
         const int* cnt = reinterpret_cast<const int*>(s0 + NODES);
@@ -892,7 +1001,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       __syncthreads();
     }
     // ---------------------------------------------------------------- end of sweep
-    if (warp == 0) commit_tree(S, C, B, trees, s0g, m - 1, lane);
+    if (warp == 0) commit_tree<LP>(S, C, B, trees, s0g, m - 1, lane, lead);
     __syncthreads();
     const bool keep = it >= C.nskip;
     const int dr = it - C.nskip;
@@ -904,7 +1013,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
                      pl4 = bcast4(ctl.pl), pr4 = bcast4(ctl.pr);
       uint8_t* lp = leaf + (long long)(m - 1) * n_pad;
       const uint8_t* qp = q + (long long)ctl.pv * n_pad;
-      for (int g = tid; g < ngroups; g += T) {
+      for (int g = g0 + tid; g < g1; g += T) {
         const uint32_t lp4 = ld_u32(lp + 4 * g);
         uint32_t lpn = lp4;
         if (pmode == 1) {
@@ -936,7 +1045,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           f2 += (double)thj[(l4 >> 16) & 255u]; f3 += (double)thj[l4 >> 24];
         }
         const double fe[4] = {f0, f1, f2, f3};
-        const float4 w4 = reinterpret_cast<const float4*>(ws)[g];
+        const float4 w4 = reinterpret_cast<const float4*>(ws)[g - g0];
         const float wwe[4] = {w4.x, w4.y, w4.z, w4.w};
         float rn[4];
 #pragma unroll
@@ -963,20 +1072,25 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
             }
           }
         }
-        reinterpret_cast<float4*>(r)[g] = make_float4(rn[0], rn[1], rn[2], rn[3]);
+        reinterpret_cast<float4*>(r)[g - g0] = make_float4(rn[0], rn[1], rn[2], rn[3]);
       }
     }
     if (caps) atomicAdd(&ctl.rtcaps, caps);
-    const long long rss = C.probit ? 0 : block_sum64(rssfx, S.red);
+    long long rss = C.probit ? 0 : block_sum64(rssfx, S.red);
+    if (CL && !C.probit) {   // the chain's rss: every CTA's partial sum
+      if (tid == 0) S.xch[(it & 1) * 4] = rss;
+      cg::this_cluster().sync();
+      if (tid == 0) rss = cluster_value(S, (it & 1) * 4, CS);
+    }
     if (tid == 0) {
       if (!C.probit) {
         const double rssd = (double)rss * rsci;
         ctl.sigma = sqrt((C.nu * C.lambda + rssd) / (2.0 * fbm::fb_gamma(seed, (uint32_t)it, ((double)n + C.nu) / 2.0)));
       }
-      B.sigma_out[C.off_sigma + it] = ctl.sigma;
+      if (lead) B.sigma_out[C.off_sigma + it] = ctl.sigma;
       ctl.pmode = 0;
     }
-    if (keep) {   // kept draw: packed nodes (src/bart_kernel.cpp:559-571)
+    if (keep && lead) {   // kept draw: packed nodes (src/bart_kernel.cpp:559-571)
       unsigned long long* out = B.trees_out + C.off_tout + (long long)dr * m * NODES;
       for (int k = tid; k < m * NODES; k += T) {
         const int j = k / NODES, s = k % NODES;
@@ -993,37 +1107,57 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   // ---------------------------------------------------------------- save state
   for (int k = tid; k < m * NODES; k += T) thg[k] = S.th[k];
   if (B.rows_in_smem)
-    for (int i = tid; i < n_pad; i += T) rg[i] = S.r[i];
-  if (tid == 0) {
-    st.sigma = ctl.sigma; st.births = ctl.births; st.deaths = ctl.deaths; st.caps = ctl.caps; st.rtcaps = ctl.rtcaps;
+    for (int li = tid; li < ns; li += T) rg[li] = S.r[li];
+  int rtcaps = ctl.rtcaps;
+  if (CL) {   // latent-z caps of the whole chain
+    __syncthreads();
+    if (tid == 0) S.xch[4 + 3] = ctl.rtcaps;
+    cg::this_cluster().sync();
+    if (tid == 0) rtcaps = (int)cluster_value(S, 4 + 3, CS);
+  }
+  if (tid == 0 && lead) {
+    st.sigma = ctl.sigma; st.births = ctl.births; st.deaths = ctl.deaths; st.caps = ctl.caps; st.rtcaps = rtcaps;
     st.it_done = it1;
   }
   __syncthreads();
+  if (CL) cg::this_cluster().sync();   // no CTA reuses or leaves its shared memory while others read it
 }
 
-template <int G>
+// G: groups of 4 rows held in registers per row thread (0: streamed); CL: a cluster of CTAs per chain; LP: learned
+// proposal or training-example collection compiled in (kept out of the plain kernels, where its calls would spill).
+template <int G, bool CL, bool LP>
 __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it0, int it1) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem);
-  for (;;) {
-    if (threadIdx.x == 0) S.ctl->chain = atomicAdd(B.queue, 1);
-    __syncthreads();
-    const int qi = S.ctl->chain;
-    __syncthreads();
-    if (qi >= B.nchains) break;
-    run_chain<G>(B, B.order[qi], it0, it1, S);
+  if constexpr (CL) {   // one chain per cluster at a time, in the host's order; every CTA of a cluster agrees
+    const int ncl = gridDim.x / B.cluster, cid = blockIdx.x / B.cluster;
+    for (int qi = cid; qi < B.nchains; qi += ncl) run_chain<G, CL, LP>(B, B.order[qi], it0, it1, S);
+  } else {
+    for (;;) {
+      if (threadIdx.x == 0) S.ctl->chain = atomicAdd(B.queue, 1);
+      __syncthreads();
+      const int qi = S.ctl->chain;
+      __syncthreads();
+      if (qi >= B.nchains) break;
+      run_chain<G, CL, LP>(B, B.order[qi], it0, it1, S);
+    }
   }
 }
 
 using KernelFn = void (*)(DBufs, int, int);
-static KernelFn kernel_for(int gmax) {
+template <bool CL, bool LP>
+static KernelFn kernel_g(int gmax) {
   switch (gmax) {
-    case 1: return sampler_kernel<1>;
-    case 2: return sampler_kernel<2>;
-    case 4: return sampler_kernel<4>;
-    case 8: return sampler_kernel<8>;
-    default: return sampler_kernel<0>;
+    case 1: return sampler_kernel<1, CL, LP>;
+    case 2: return sampler_kernel<2, CL, LP>;
+    case 4: return sampler_kernel<4, CL, LP>;
+    case 8: return sampler_kernel<8, CL, LP>;
+    default: return sampler_kernel<0, CL, LP>;
   }
+}
+static KernelFn kernel_for(int gmax, bool cluster, bool lp) {
+  if (cluster) return lp ? kernel_g<true, true>(gmax) : kernel_g<true, false>(gmax);
+  return lp ? kernel_g<false, true>(gmax) : kernel_g<false, false>(gmax);
 }
 
 int sampler_gmax(int threads, int n_pad_max) {
@@ -1037,22 +1171,52 @@ size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_sme
   return smem_layout(threads, m_max, n_pad_max, rows_in_smem, off);
 }
 
-int sampler_max_grid(int threads, size_t smem, int device, int gmax) {
-  int per_sm = 0, nsm = 0;
-  const KernelFn k = kernel_for(gmax);
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess) return -1;
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
-  return per_sm * nsm;
+int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster) {
+  // the learned-proposal kernels need the same shared memory; residency is the same for both
+  const KernelFn k = kernel_for(gmax, cluster > 1, true);
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  if (cluster <= 1) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess) return 0;
+    return per_sm * nsm;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(cluster * ((nsm + cluster - 1) / cluster), 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, k, &cfg) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return ncl * cluster;
 }
 
-int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, void* stream) {
+int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
+                   void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const KernelFn k = kernel_for(gmax);
+  const KernelFn k = kernel_for(gmax, cluster > 1, (b.mw1 != nullptr && b.mix > 0.0) || b.train_cap > 0);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
   if (cudaMemsetAsync(b.queue, 0, sizeof(int), s) != cudaSuccess) return -1;
-  k<<<grid, threads, smem, s>>>(b, it0, it1);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  if (cluster <= 1) {
+    k<<<grid, threads, smem, s>>>(b, it0, it1);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, b, it0, it1) == cudaSuccess ? 0 : -1;
 }
 
 // ------------------------------------------------------------------------------------------------ diagnostics
@@ -1104,7 +1268,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
     U.leaf_next = nullptr; U.qnext = nullptr;
     U.r = r; U.ws = ws; U.D = D; U.tc = tc; U.bins = bins; U.ovb = ovb; U.tot = tot;
     U.DL = dlr[0]; U.DR = dlr[1];
-    U.n = a.n; U.ngroups = a.n_pad / 4; U.rt = tid - 32; U.RT = RT; U.nleaf = nleaf;
+    U.n = a.n; U.g0 = 0; U.g1 = a.n_pad / 4; U.rt = tid - 32; U.RT = RT; U.nleaf = nleaf;
     U.apply = a.apply; U.pmode = a.pmode; U.pnx = a.pnx; U.pc = a.pc; U.pL = a.pL; U.pR = a.pR; U.pl = a.pl; U.pr = a.pr;
     U.cmode = a.stats ? a.cmode : 0; U.cnx = a.cnx; U.cc = a.cc;
     pass_rows_stream(U);

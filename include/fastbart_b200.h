@@ -66,6 +66,8 @@ typedef struct fb_options {
   int threads;              /* threads per CTA; 0 = automatic */
   int sweeps_per_launch;    /* 0 = the whole MCMC in one launch; k > 0 = launches of k sweeps */
   int device;               /* CUDA device ordinal */
+  int cluster;              /* CTAs per chain (a thread-block cluster sharing the rows): 0 = automatic, 1 = one CTA,
+                               2..8 = that many when they can be resident; results are identical for every value */
 } fb_options;
 
 /* Caller-owned host outputs of one chain; a NULL pointer skips that copy. */

@@ -24,8 +24,8 @@ def random_model(seed, scale=0.3, mix=0.5):
                 w3=_bf16(rng.normal(0, scale, (32, 64))), b3=rng.normal(0, 0.5, 32).astype(np.float32), mix=mix)
 
 
-def _run(ch, nskip, ndpost, model=None, collect=0):
-    b = F.Batch([ch], nskip, ndpost)
+def _run(ch, nskip, ndpost, model=None, collect=0, cluster=0):
+    b = F.Batch([ch], nskip, ndpost, cluster=cluster)
     if model is not None:
         b.set_proposal(model)
     if collect:
@@ -38,9 +38,10 @@ def _run(ch, nskip, ndpost, model=None, collect=0):
     return out, data
 
 
-def test_collected_examples_bit_exact(orc):
+@pytest.mark.parametrize("cluster", [1, 4])
+def test_collected_examples_bit_exact(orc, cluster):
     ch = W.fwbart_friedman(n=500, p=9, seed=4, ntree=25, nskip=40, ndpost=10)
-    out, (x, y, m, cnt) = _run(ch, 40, 10, collect=20000)
+    out, (x, y, m, cnt) = _run(ch, 40, 10, collect=20000, cluster=cluster)
     ref = orc.fit(ch, orc.MODE_DEV, train_cap=20000)
     assert np.array_equal(out["sigma"], ref["sigma"])          # collecting changes nothing in the chain
     assert cnt == ref["moves"][0] == len(ref["train_y"])
@@ -48,11 +49,11 @@ def test_collected_examples_bit_exact(orc):
     assert np.array_equal(x.view(np.uint32), ref["train_x"].view(np.uint32))
 
 
-@pytest.mark.parametrize("mix", [0.5, 1.0])
-def test_model_chain_bit_exact(orc, mix):
+@pytest.mark.parametrize("mix,cluster", [(0.5, 1), (1.0, 1), (0.5, 2)])
+def test_model_chain_bit_exact(orc, mix, cluster):
     ch = W.fwbart_friedman(n=400, p=12, seed=8, ntree=20, nskip=30, ndpost=10)
     model = random_model(3, mix=mix)
-    out, _ = _run(ch, 30, 10, model=model)
+    out, _ = _run(ch, 30, 10, model=model, cluster=cluster)
     ref = orc.fit(ch, orc.MODE_DEV, model=model)
     for k, r in (("sigma", "sigma"), ("yhat_mean", "fmean"), ("trees", "trees"), ("moves", "moves")):
         assert np.array_equal(np.asarray(out[k]), np.asarray(ref[r])), k

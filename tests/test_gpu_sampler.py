@@ -115,8 +115,32 @@ def test_probit_large_n_rows_in_global(orc):
     """n = 24,576 person-weeks (shared memory holds the rows) and n = 40,000 (rows stay in global memory)."""
     for n in (24576, 40000):
         ch = W.fpbart_hazard(n=n, seed=5, ntree=6, nskip=4, ndpost=3)
-        g = fit_batch([ch], 4, 3)[0]
+        g = fit_batch([ch], 4, 3, cluster=1)[0]
         _compare(g, orc.fit(ch, orc.MODE_DEV))
+
+
+@pytest.mark.parametrize("cluster,spl", [(2, 0), (3, 0), (4, 7), (8, 0)])
+def test_cluster_chains_bit_exact(orc, cluster, spl):
+    """A chain split over a thread-block cluster (rows sliced across CTAs, totals through distributed shared memory)
+    gives the one-CTA results bit for bit: weighted and probit chains, ragged n, slices with no rows (n 37 on 8 CTAs),
+    resumed launches."""
+    chains = [W.fwbart_friedman(n=5000, p=6, seed=41, ntree=20, nskip=12, ndpost=6),
+              W.fpbart_hazard(n=3001, seed=42, ntree=8, nskip=12, ndpost=6),
+              W.fwbart_friedman(n=37, p=3, seed=43, ntree=7, nskip=12, ndpost=6)]
+    outs = fit_batch(chains, 12, 6, cluster=cluster, sweeps_per_launch=spl)
+    for ch, g in zip(chains, outs):
+        o = orc.fit(ch, orc.MODE_DEV)
+        _compare(g, o)
+        assert g["rtnorm_caps"] == o["rtnorm_caps"]
+
+
+def test_cluster_rows_beyond_one_cta(orc):
+    """n = 65,536 (one CTA keeps the rows in global memory; 8 CTAs hold 8,192 rows each in shared memory)."""
+    ch = W.fwbart_friedman(n=65536, p=8, seed=44, ntree=10, nskip=3, ndpost=2)
+    one = fit_batch([ch], 3, 2, cluster=1)[0]
+    eight = fit_batch([ch], 3, 2, cluster=8)[0]
+    _compare(eight, one)
+    _compare(one, orc.fit(ch, orc.MODE_DEV))
 
 
 def _ref_pool_fit(ch):
