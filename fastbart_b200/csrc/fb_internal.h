@@ -91,7 +91,7 @@ struct DBufs {
   int train_cap;
 };
 
-size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem);
+size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster);
 // groups of 4 rows per row thread held in registers (1, 2, 4, 8), or 0 when the rows stream from L2 in the pass
 int sampler_gmax(int threads, int n_pad_max);
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,

@@ -339,25 +339,45 @@ __device__ __noinline__ unsigned node_features(const DTree* t, int nx, int cnt, 
 __device__ __forceinline__ float bf16f(uint16_t h) { return __uint_as_float((unsigned)h << 16); }
 
 // MLP forward (FP32, no fused multiply-add, fixed order) and masked softmax in FP64: q[v] for valid v, else 0.
+// Four outputs of a dense layer at once (four independent accumulators share each input load); each output is the
+// sequential sum bias + w[0] x[0] + w[1] x[1] + ... in FP32 without fused multiply-add, as the oracle computes it.
+// Weight rows are read as pairs of BF16 values (rows start on 4-byte boundaries: NIN is even).
+template <int NIN>
+__device__ __forceinline__ void dense4(const uint16_t* W, const float* bias, const float* x, int h, float (&a)[4]) {
+  const uint32_t* w[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) { a[u] = __ldg(bias + h + u); w[u] = reinterpret_cast<const uint32_t*>(W + (h + u) * NIN); }
+#pragma unroll 8
+  for (int kk = 0; kk < NIN / 2; kk++) {
+    const float xa = x[2 * kk], xb = x[2 * kk + 1];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t pw = __ldg(w[u] + kk);
+      a[u] = __fadd_rn(a[u], __fmul_rn(__uint_as_float(pw << 16), xa));
+      a[u] = __fadd_rn(a[u], __fmul_rn(__uint_as_float(pw & 0xFFFF0000u), xb));
+    }
+  }
+}
+
 __device__ __noinline__ void model_probs(const DBufs& B, const float* x, unsigned valid, double* q) {
   float h1[MLP_H], h2[MLP_H], z[MLP_OUT];
-  for (int h = 0; h < MLP_H; h++) {
-    float a = __ldg(B.mb1 + h);
-    const uint16_t* w = B.mw1 + h * MLP_IN;
-    for (int k = 0; k < MLP_IN; k++) a = __fadd_rn(a, __fmul_rn(bf16f(__ldg(w + k)), x[k]));
-    h1[h] = a > 0.0f ? a : 0.0f;
+  for (int h = 0; h < MLP_H; h += 4) {
+    float a[4];
+    dense4<MLP_IN>(B.mw1, B.mb1, x, h, a);
+#pragma unroll
+    for (int u = 0; u < 4; u++) h1[h + u] = a[u] > 0.0f ? a[u] : 0.0f;
   }
-  for (int h = 0; h < MLP_H; h++) {
-    float a = __ldg(B.mb2 + h);
-    const uint16_t* w = B.mw2 + h * MLP_H;
-    for (int k = 0; k < MLP_H; k++) a = __fadd_rn(a, __fmul_rn(bf16f(__ldg(w + k)), h1[k]));
-    h2[h] = a > 0.0f ? a : 0.0f;
+  for (int h = 0; h < MLP_H; h += 4) {
+    float a[4];
+    dense4<MLP_H>(B.mw2, B.mb2, h1, h, a);
+#pragma unroll
+    for (int u = 0; u < 4; u++) h2[h + u] = a[u] > 0.0f ? a[u] : 0.0f;
   }
-  for (int o = 0; o < MLP_OUT; o++) {
-    float a = __ldg(B.mb3 + o);
-    const uint16_t* w = B.mw3 + o * MLP_H;
-    for (int k = 0; k < MLP_H; k++) a = __fadd_rn(a, __fmul_rn(bf16f(__ldg(w + k)), h2[k]));
-    z[o] = a;
+  for (int o = 0; o < MLP_OUT; o += 4) {
+    float a[4];
+    dense4<MLP_H>(B.mw3, B.mb3, h2, o, a);
+#pragma unroll
+    for (int u = 0; u < 4; u++) z[o + u] = a[u];
   }
   double zmax = 0.0;
   bool any = false;
@@ -530,11 +550,14 @@ struct Smem {
   long long* ctot;              // [2][TOT] cluster totals (sum over the cluster's CTAs)
   unsigned long long* covb;     // [2][64]
   long long* xch;               // [2][4] per-CTA values exchanged across the cluster (rss, latent-z caps, sum w)
+  long long* xtot;              // [2][cluster][TOT] every CTA's pass totals, pushed by their owners
+  unsigned long long* xovb;     // [2][cluster][64]
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-__host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_max, int rows_in_smem, size_t* off) {
+__host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster,
+                                               size_t* off) {
   const int NW = threads / 32, RT = threads - 32;
   size_t o = 0;
   off[0] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // r
@@ -556,13 +579,16 @@ __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_
   off[16] = o; o += 2 * TOT * 8;                                             // ctot[2]
   off[17] = o; o += 2 * NODES * 8;                                           // covb[2]
   off[18] = o; o += 2 * 4 * 8;                                               // xch[2][4]
+  const size_t cs = cluster > 1 ? (size_t)cluster : 0;
+  off[19] = o; o += 2 * cs * TOT * 8;                                        // xtot[2][cluster][TOT]
+  off[20] = o; o += 2 * cs * NODES * 8;                                      // xovb[2][cluster][64]
   return o;
 }
-constexpr int NOFF = 19;
+constexpr int NOFF = 21;
 
-__device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max, int rows_in_smem) {
+__device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster) {
   size_t off[NOFF];
-  smem_layout(threads, m_max, n_pad_max, rows_in_smem, off);
+  smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off);
   Smem S;
   S.r = reinterpret_cast<float*>(base + off[0]);
   S.ws = reinterpret_cast<float*>(base + off[1]);
@@ -583,6 +609,8 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.ctot = reinterpret_cast<long long*>(base + off[16]);
   S.covb = reinterpret_cast<unsigned long long*>(base + off[17]);
   S.xch = reinterpret_cast<long long*>(base + off[18]);
+  S.xtot = reinterpret_cast<long long*>(base + off[19]);
+  S.xovb = reinterpret_cast<unsigned long long*>(base + off[20]);
   return S;
 }
 
@@ -620,7 +648,7 @@ __device__ __forceinline__ void fetch_tree(const Smem& S, const DTree* trees, co
 }
 
 // An accepted birth of tree j becomes a training example (control warp).
-__device__ __noinline__ void collect_example(const DBufs& B, const DChain& C, int j, int v, int lane) {
+__device__ __forceinline__ void collect_example(const DBufs& B, const DChain& C, int j, int v, int lane) {
   int idx = 0;
   if (lane == 0) idx = atomicAdd(B.train_count, 1);
   idx = __shfl_sync(0xffffffffu, idx, 0);
@@ -696,20 +724,30 @@ __device__ __noinline__ void proposals_model(const Smem& S, const DBufs& B, cons
   proposals_body<true>(S, B, C, trees, s0g, it, lead);
 }
 
-// Sums of the cluster's per-CTA pass totals (tot, ovb of buffer cur) into ctot / covb; after a cluster barrier.
-__device__ __forceinline__ void cluster_totals(const Smem& S, int cur, int CS) {
+// Cluster exchange of the pass totals (buffer cur), push style: every CTA stores its totals into slot [crank] of every
+// CTA's xtot / xovb (remote stores do not wait), a cluster barrier publishes them, and each CTA then sums the slots
+// in its own shared memory.  The ovb partials (leaves beyond the register bins) are exchanged only when used.
+__device__ __forceinline__ void cluster_push(const Smem& S, int cur, int CS, int crank, bool ovf) {
   cg::cluster_group cl = cg::this_cluster();
-  for (int k = threadIdx.x; k < TOT + NODES; k += blockDim.x) {
-    if (k < TOT) {
-      long long t = 0;
-      for (int r = 0; r < CS; r++) t += *cl.map_shared_rank(S.tot + cur * TOT + k, r);
-      S.ctot[cur * TOT + k] = t;
-    } else {
-      const int s = k - TOT;
-      unsigned long long t = 0;
-      for (int r = 0; r < CS; r++) t += *cl.map_shared_rank(S.ovb + cur * NODES + s, r);
-      S.covb[cur * NODES + s] = t;
-    }
+  const int k = threadIdx.x;
+  if (k < TOT) {
+    const long long v = S.tot[cur * TOT + k];
+    for (int d = 0; d < CS; d++) *cl.map_shared_rank(S.xtot + (cur * CS + crank) * TOT + k, d) = v;
+  } else if (ovf && k < TOT + NODES) {
+    const unsigned long long v = S.ovb[cur * NODES + k - TOT];
+    for (int d = 0; d < CS; d++) *cl.map_shared_rank(S.xovb + (cur * CS + crank) * NODES + k - TOT, d) = v;
+  }
+}
+__device__ __forceinline__ void cluster_sum(const Smem& S, int cur, int CS, bool ovf) {
+  const int k = threadIdx.x;
+  if (k < TOT) {
+    long long t = 0;
+    for (int r = 0; r < CS; r++) t += S.xtot[(cur * CS + r) * TOT + k];
+    S.ctot[cur * TOT + k] = t;
+  } else if (ovf && k < TOT + NODES) {
+    unsigned long long t = 0;
+    for (int r = 0; r < CS; r++) t += S.xovb[(cur * CS + r) * NODES + k - TOT];
+    S.covb[cur * NODES + k - TOT] = t;
   }
 }
 
@@ -896,9 +934,12 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       }
       __syncthreads();
       reduce_totals(S.bins, RT, ctl.nleaf[cur], P.mode, S.tot + cur * TOT);
-      if (CL) {   // the chain's totals: every CTA's partial totals, read through distributed shared memory
+      if (CL) {   // the chain's totals: every CTA's partial totals, pushed through distributed shared memory
+        const bool ovf = ctl.nleaf[cur] > NBS;
+        __syncthreads();
+        cluster_push(S, cur, CS, crank, ovf);
         cg::this_cluster().sync();
-        cluster_totals(S, cur, CS);
+        cluster_sum(S, cur, CS, ovf);
       }
       __syncthreads();
       // ------------------------------------------------------------ phase B: MH and leaf draws, one thread per slot
@@ -1128,7 +1169,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
 template <int G, bool CL, bool LP>
 __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it0, int it1) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem);
+  const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem, B.cluster);
   if constexpr (CL) {   // one chain per cluster at a time, in the host's order; every CTA of a cluster agrees
     const int ncl = gridDim.x / B.cluster, cid = blockIdx.x / B.cluster;
     for (int qi = cid; qi < B.nchains; qi += ncl) run_chain<G, CL, LP>(B, B.order[qi], it0, it1, S);
@@ -1166,14 +1207,14 @@ int sampler_gmax(int threads, int n_pad_max) {
   return g <= 1 ? 1 : g <= 2 ? 2 : g <= 4 ? 4 : g <= 8 ? 8 : 0;
 }
 
-size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem) {
+size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster) {
   size_t off[NOFF];
-  return smem_layout(threads, m_max, n_pad_max, rows_in_smem, off);
+  return smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off);
 }
 
 int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster) {
   // the learned-proposal kernels need the same shared memory; residency is the same for both
-  const KernelFn k = kernel_for(gmax, cluster > 1, true);
+  const KernelFn k = kernel_for(0, cluster > 1, true);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
@@ -1199,7 +1240,10 @@ int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
                    void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const KernelFn k = kernel_for(gmax, cluster > 1, (b.mw1 != nullptr && b.mix > 0.0) || b.train_cap > 0);
+  // learned-proposal kernels stream the leaf words (no per-thread word registers): their model calls keep the
+  // register-held variants from fitting in 128 registers without spilling in the pass
+  const bool lp = (b.mw1 != nullptr && b.mix > 0.0) || b.train_cap > 0;
+  const KernelFn k = kernel_for(lp ? 0 : gmax, cluster > 1, lp);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
   if (cudaMemsetAsync(b.queue, 0, sizeof(int), s) != cudaSuccess) return -1;
   if (cluster <= 1) {
