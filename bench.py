@@ -44,9 +44,26 @@ def workload(rank: int = 0, reps: int = 16, nskip=NSKIP, ndpost=NDPOST):
     return W.titer_bootstrap(reps=reps, seed=rank, nskip=nskip, ndpost=ndpost, ntree=NTREE)
 
 
+FULL_REF = True
+N_RANGE, P_RANGE = [3091, 4573], [15, 19]
+
+
 def set_workload(name: str):
-    """'titer96' (the benchmark) or 'small' (6 chains, one per shape, 40 sweeps: the profiling case)."""
-    global NSKIP, NDPOST, WORKLOAD_NAME, workload
+    """'titer96' (the benchmark), 'small' (6 chains, one per shape, 40 sweeps: the profiling case) or 'sparse'
+    (16 chains, n 65,536, p 32, numcut 255, Friedman-5 signal on 5 of 32 predictors: the large-n configuration, run
+    on thread-block clusters of 8 CTAs per chain)."""
+    global NSKIP, NDPOST, WORKLOAD_NAME, workload, METRIC, FULL_REF, N_RANGE, P_RANGE
+    if name == "sparse":
+        WORKLOAD_NAME, FULL_REF, N_RANGE, P_RANGE = "friedman_sparse_16x65536", False, [65536, 65536], [32, 32]
+        METRIC = "chain-sweeps/s (16 fwbart chains, n 65,536, p 32)"
+
+        def sparse(rank: int = 0, reps: int = 0, nskip=None, ndpost=None):
+            from fastbart_b200 import workloads as W
+            out = W.friedman_large(nchains=16, n=65536, p=32, seed=rank, nskip=NSKIP, ndpost=NDPOST, ntree=NTREE)
+            for k, c in enumerate(out):
+                c["seed"] = 100 + 16 * rank + k
+            return out
+        workload = sparse
     if name == "small":
         NSKIP, NDPOST, WORKLOAD_NAME = 30, 10, "titer_small_6x40"
         base = workload
@@ -156,8 +173,8 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """DRAM bytes per full-size launch from the committed ncu summary (scaled from a small capture), or None."""
-    p = os.path.join(ROOT, "profiles", "sampler_kernel_titer96.md")
+    """DRAM bytes per full-size launch of this workload from its committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", f"sampler_kernel_{WORKLOAD_NAME}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -187,7 +204,7 @@ def bench_reference(args):
             vals.append(v); walls.append(wall)
     tot = sum(walls)
     value = ncores * sweeps * args.steps / tot
-    sample = f"{ncores} chains of the 96 (one per core), {sweeps} sweeps each, per step"
+    sample = f"{ncores} chains of the {len(chains)} (one per core), {sweeps} sweeps each, per step"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -219,8 +236,9 @@ def bench_ours(args):
         pool.map(_warm_worker, range(ncores), chunksize=1)
         v, kind, wall = run_cpu_sample(pool, chains, ncores, sweeps)
         cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": kind,
-               "sample": f"{ncores} of the 96 chains, one per core, {sweeps} sweeps each ({wall:.1f} s wall)"}
-        full_ref = pool.apply_async(_full_ref_chain, (chains[0],))   # agreement check of chain 0, full length
+               "sample": f"{ncores} of the {len(chains)} chains, one per core, {sweeps} sweeps each ({wall:.1f} s wall)"}
+        if FULL_REF:
+            full_ref = pool.apply_async(_full_ref_chain, (chains[0],))   # agreement check of chain 0, full length
 
     import torch
     import torch.distributed as dist
@@ -343,9 +361,9 @@ def bench_ours(args):
                 "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64-fixed+f32+f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD_NAME, "chains_per_gpu": len(chains), "ntree": NTREE,
-                           "nskip": NSKIP, "ndpost": NDPOST, "n_range": [3091, 4573], "p_range": [15, 19],
+                           "nskip": NSKIP, "ndpost": NDPOST, "n_range": N_RANGE, "p_range": P_RANGE,
                            "l2": "flushed (512 MiB write) before every timed step", "threads": info["threads"],
-                           "grid": info["grid"], "smem_bytes": info["smem"]},
+                           "grid": info["grid"], "smem_bytes": info["smem"], "ctas_per_chain": info["cluster"]},
                 "e2e": e2e, "gpu_launches": args.steps * info["launches"], "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "ess_per_s": ess_line, "r_f_vs_reference_chain0": r_f, "wall_s": wall}
         print(json.dumps(line), flush=True)
@@ -597,7 +615,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="titer96", choices=["titer96", "small", "predict", "learned"])
+    ap.add_argument("--workload", default="titer96", choices=["titer96", "small", "sparse", "predict", "learned"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

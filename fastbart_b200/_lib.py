@@ -93,7 +93,7 @@ def lib() -> C.CDLL:
         L.fb_batch_run.argtypes = [vp, vp]
         L.fb_batch_sync.argtypes = [vp]
         L.fb_batch_download.argtypes = [vp, C.POINTER(ChainOut)]
-        L.fb_batch_launch_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(sz)]
+        L.fb_batch_launch_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(sz), C.POINTER(i)]
         L.fb_batch_destroy.argtypes = [vp]
         L.fb_batch_destroy.restype = None
         L.fb_fbart.argtypes = [vp, i, i, vp, vp, vp, vp, vp, i, i, i, d, d, d, d, C.c_uint64, i, d, vp, vp, vp, vp,

@@ -99,9 +99,9 @@ class Batch:
         check(_lib.lib().fb_batch_sync(self._h))
 
     def launch_info(self) -> dict:
-        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
-        check(_lib.lib().fb_batch_launch_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
-        return dict(launches=a.value, threads=b.value, grid=c.value, smem=d.value)
+        a, b, c, d, e = C.c_int(), C.c_int(), C.c_int(), C.c_size_t(), C.c_int()
+        check(_lib.lib().fb_batch_launch_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e)))
+        return dict(launches=a.value, threads=b.value, grid=c.value, smem=d.value, cluster=e.value)
 
     def download(self, trees: bool = True, alloc=np.empty) -> list:
         outs = [_alloc_out(c, self.nskip, self.ndpost, trees, alloc) for c in self.chains]

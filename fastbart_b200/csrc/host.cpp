@@ -180,14 +180,19 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt->device) != cudaSuccess) optin = 232448;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
   // CTAs per chain: a cluster splits each chain's rows over CS SMs when SMs would otherwise idle (or as requested)
-  int CS = 1;
-  if (opt->cluster > 0) CS = std::min(opt->cluster, 8);
-  else
-    for (int c : {8, 4})   // measured on B200: 4 or 8 CTAs gain from about 2,000 rows; 2 CTAs rarely do
-      if ((long long)nchains * c <= nsm && n_pad_max / c >= 512) { CS = c; break; }
-  int rows_in_smem = 1, gmax = 0, maxgrid = 0;
+  // Automatic choice (measured on B200): the largest cluster of 4..8 CTAs whose clusters are all resident at once,
+  // one per chain, when there are SMs to spare and at least 512 rows per CTA; otherwise one CTA per chain.
+  std::vector<int> tries;
+  if (opt->cluster > 0) tries.push_back(std::min(opt->cluster, 8));
+  else {
+    for (int c = 8; c >= 4; c--)
+      if ((long long)nchains * c <= nsm && n_pad_max / c >= 512) tries.push_back(c);
+  }
+  tries.push_back(1);
+  int CS = 1, rows_in_smem = 1, gmax = 0, maxgrid = 0;
   size_t smem = 0;
-  for (;;) {
+  for (size_t ti = 0; ti < tries.size(); ti++) {
+    CS = tries[ti];
     const int cap = 4 * ((n_pad_max / 4 + CS - 1) / CS);   // rows of one CTA's slice
     rows_in_smem = 1;
     smem = sampler_smem_bytes(T, m_max, cap, 1, CS);
@@ -195,8 +200,8 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
     if (smem > (size_t)optin) { delete b; return fail(FB_ERR_LIMIT, "shared memory %zu exceeds %d", smem, optin); }
     gmax = sampler_gmax(T, cap);
     maxgrid = sampler_max_grid(T, smem, opt->device, gmax, CS);   // CTAs (whole clusters) that can be resident
-    if (maxgrid > 0 || CS == 1) { b->slice_rows = cap; break; }
-    CS = 1;   // clusters of this shape cannot be resident: one CTA per chain
+    const bool all_resident = maxgrid >= nchains * CS;
+    if (CS == 1 || (maxgrid > 0 && (opt->cluster > 0 || all_resident))) { b->slice_rows = cap; break; }
   }
   if (maxgrid <= 0) { delete b; return fail(FB_ERR_CUDA, "sampler kernel cannot be resident with %zu bytes of shared memory", smem); }
   b->cluster = CS;
@@ -350,12 +355,14 @@ fb_status fb_batch_sync(fb_batch* b) {
   return FB_OK;
 }
 
-fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes) {
+fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes,
+                               int* cluster) {
   if (!b) return fail(FB_ERR_ARG, "batch is NULL");
   if (launches) *launches = b->launches;
   if (threads) *threads = b->threads;
   if (grid) *grid = b->grid;
   if (smem_bytes) *smem_bytes = b->smem;
+  if (cluster) *cluster = b->cluster;
   return FB_OK;
 }
 

@@ -92,8 +92,10 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
 fb_status fb_batch_run(fb_batch* b, void* cuda_stream);        /* enqueues on cuda_stream (NULL: default stream) */
 fb_status fb_batch_sync(fb_batch* b);
 fb_status fb_batch_download(fb_batch* b, fb_chain_out* outs);
-/* number of sampler kernel launches per fb_batch_run, and the dynamic shared memory / threads / grid of each */
-fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes);
+/* number of sampler kernel launches per fb_batch_run, the dynamic shared memory / threads / grid of each, and the
+ * CTAs per chain (thread-block cluster size; 1 without clusters).  Outputs may be NULL. */
+fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes,
+                               int* cluster);
 void fb_batch_destroy(fb_batch* b);
 
 /* ---------------------------------------------------------------------------- learned split-variable proposal */
