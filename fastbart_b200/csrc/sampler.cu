@@ -64,6 +64,7 @@ struct Ctl {                  // CTA-shared control state
   int nleaf[2];                             // leaves of the tree whose table is in buffer 0 / 1
   int births, deaths, caps, rtcaps;
   int chain;
+  int accept;                               // MH decision of the current tree (handed from warp 2 to warps 0-1)
   double sigma;
 };
 
@@ -943,7 +944,11 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       }
       __syncthreads();
       // ------------------------------------------------------------ phase B: MH and leaf draws, one thread per slot
-      if (tid < NODES) {
+      // With at least 3 warps, warp 2 evaluates Metropolis-Hastings while warps 0-1 draw every slot's leaf value for
+      // the outcome in which that slot is a leaf (a slot is a leaf with the same statistics in both outcomes, or in
+      // one outcome only), so the two overlap; a named barrier of the 3 warps then hands over the decision.
+      const bool sep = T >= 96;
+      if (tid < (sep ? NODES + 32 : NODES)) {
         const int s = tid;
         const Masks mk = S.masks[j];
         const long long* tot = (CL ? S.ctot : S.tot) + cur * TOT;
@@ -963,81 +968,99 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           sL0 = tot[NBS + 0]; sL1 = tot[NBS + 1]; nL = (int)tot[NBS + 2];
           sR0 = s0[P.nx] - sL0; sR1 = s1of(P.nx) - sL1; nR = cnt[P.nx] - nL;
         }
-        bool eval = false;
-        double bl = 0, Ml = 0, br = 0, Mr = 0;
-        if (P.mode == 1 && nL >= 5 && nR >= 5) {
-          eval = true;
-          bl = (double)sL0 * sci * inv_s2; Ml = (double)sL1 * sci * inv_s2;
-          br = (double)sR0 * sci * inv_s2; Mr = (double)sR1 * sci * inv_s2;
-        } else if (P.mode == 2) {
-          eval = true;
-          bl = (double)s0[P.l] * sci * inv_s2; Ml = (double)s1of(P.l) * sci * inv_s2;
-          br = (double)s0[P.r] * sci * inv_s2; Mr = (double)s1of(P.r) * sci * inv_s2;
-        }
+        const bool eval = (P.mode == 1 && nL >= 5 && nR >= 5) || P.mode == 2;
         bool accept = false;
-        if (eval) {
-          // lanes 0..2 of each of the two warps evaluate the three log marginal likelihoods at one call site:
-          // birth (l, r, l+r), death (l+r, l, r), in the order the ratio adds them
-          const int which = P.mode == 1 ? lane : (lane == 0 ? 2 : lane - 1);
-          const double hb = which == 0 ? bl : (which == 1 ? br : bl + br);
-          const double hM = which == 0 ? Ml : (which == 1 ? Mr : Ml + Mr);
-          double hv = 0.0;
-          if (lane < 3) hv = lh(hb, hM, t2);
-          const double h0 = __shfl_sync(0xffffffffu, hv, 0), h1 = __shfl_sync(0xffffffffu, hv, 1),
-                       h2 = __shfl_sync(0xffffffffu, hv, 2);
-          double lalpha = (P.mode == 1) ? P.logpr + h0 + h1 - h2 : P.logpr + h0 - h1 - h2;
-          if (lalpha > 0) lalpha = 0;
-          accept = P.lu < lalpha;
-        }
-        int nmode = 0, L = 0, R = 0;
-        bool cap = false;
-        unsigned long long used = mk.used, leafm = mk.leaf;
-        if (accept && P.mode == 1) {
-          L = first_free(used, -1);
-          R = L >= 0 ? first_free(used, L) : -1;
-          if (L < 0 || R < 0) { cap = true; L = R = 0; }
-          else {
-            nmode = 1;
-            used |= (1ull << L) | (1ull << R);
-            leafm = (leafm & ~(1ull << P.nx)) | (1ull << L) | (1ull << R);
+        if (!sep || warp == 2) {
+          if (eval) {
+            double bl, Ml, br, Mr;
+            if (P.mode == 1) {
+              bl = (double)sL0 * sci * inv_s2; Ml = (double)sL1 * sci * inv_s2;
+              br = (double)sR0 * sci * inv_s2; Mr = (double)sR1 * sci * inv_s2;
+            } else {
+              bl = (double)s0[P.l] * sci * inv_s2; Ml = (double)s1of(P.l) * sci * inv_s2;
+              br = (double)s0[P.r] * sci * inv_s2; Mr = (double)s1of(P.r) * sci * inv_s2;
+            }
+            // lanes 0..2 evaluate the three log marginal likelihoods at one call site: birth (l, r, l+r),
+            // death (l+r, l, r), in the order the ratio adds them
+            const int which = P.mode == 1 ? lane : (lane == 0 ? 2 : lane - 1);
+            const double hb = which == 0 ? bl : (which == 1 ? br : bl + br);
+            const double hM = which == 0 ? Ml : (which == 1 ? Mr : Ml + Mr);
+            double hv = 0.0;
+            if (lane < 3) hv = lh(hb, hM, t2);
+            const double h0 = __shfl_sync(0xffffffffu, hv, 0), h1 = __shfl_sync(0xffffffffu, hv, 1),
+                         h2 = __shfl_sync(0xffffffffu, hv, 2);
+            double lalpha = (P.mode == 1) ? P.logpr + h0 + h1 - h2 : P.logpr + h0 - h1 - h2;
+            if (lalpha > 0) lalpha = 0;
+            accept = P.lu < lalpha;
           }
-        } else if (accept && P.mode == 2) {
-          nmode = 2;
-          used &= ~((1ull << P.l) | (1ull << P.r));
-          leafm = (leafm & ~((1ull << P.l) | (1ull << P.r))) | (1ull << P.nx);
+          if (sep && lane == 0) ctl.accept = accept ? 1 : 0;
         }
-        // this thread's slot: new leaf value (DRMU) and apply delta
-        const unsigned long long lm0 = mk.used & mk.leaf, lm1 = used & leafm;
-        const float old = thj[s];
-        float nw = old;
-        if ((lm1 >> s) & 1ull) {
-          long long S0s, S1s;
-          if (nmode == 1 && s == L) { S0s = sL0; S1s = sL1; }
-          else if (nmode == 1 && s == R) { S0s = sR0; S1s = sR1; }
-          else if (nmode == 2 && s == P.nx) { S0s = s0[P.l] + s0[P.r]; S1s = s1of(P.l) + s1of(P.r); }
-          else { S0s = s0[s]; S1s = ((lm0 >> s) & 1ull) ? s1of(s) : 0ll; }
-          const double b = (double)S0s * sci * inv_s2, M = (double)S1s * sci * inv_s2;
-          const int zi = __popcll(P.cand & ((1ull << s) - 1ull));
-          const double z = zi < ZMAX ? S.zall[j * ZMAX + zi] : S.z[s];
-          nw = (float)(M / (a_prior + b) + z / sqrt(a_prior + b));
-          thj[s] = nw;
+        // slots a birth would take (lowest free slots), decided before the outcome is known
+        int Lc = -1, Rc = -1;
+        if (P.mode == 1) { Lc = first_free(mk.used, -1); Rc = Lc >= 0 ? first_free(mk.used, Lc) : -1; }
+        const unsigned long long lm0 = mk.used & mk.leaf;
+        float nws = 0.0f;   // this slot's leaf value in the outcome where it is a leaf
+        if (s < NODES) {
+          bool has = true;
+          long long S0s = 0, S1s = 0;
+          if ((lm0 >> s) & 1ull) { S0s = s0[s]; S1s = s1of(s); }
+          else if (eval && P.mode == 1 && Lc >= 0 && Rc >= 0 && s == Lc) { S0s = sL0; S1s = sL1; }
+          else if (eval && P.mode == 1 && Lc >= 0 && Rc >= 0 && s == Rc) { S0s = sR0; S1s = sR1; }
+          else if (eval && P.mode == 2 && s == P.nx) { S0s = s0[P.l] + s0[P.r]; S1s = s1of(P.l) + s1of(P.r); }
+          else has = false;
+          if (has) {
+            const double b = (double)S0s * sci * inv_s2, M = (double)S1s * sci * inv_s2;
+            const int zi = __popcll(P.cand & ((1ull << s) - 1ull));
+            const double z = zi < ZMAX ? S.zall[j * ZMAX + zi] : S.z[s];
+            nws = (float)(M / (a_prior + b) + z / sqrt(a_prior + b));
+          }
         }
-        // leaf values of slots that stop being leaves do not change, so the reads below see old values
-        if (!(nmode == 2 && (s == P.l || s == P.r))) S.D[s] = __fsub_rn(nw, old);
-        if (nmode == 2 && s == P.nx) { S.D[P.l] = __fsub_rn(nw, thj[P.l]); S.D[P.r] = __fsub_rn(nw, thj[P.r]); }
-        if (nmode == 1 && s == L) ctl.DL = __fsub_rn(nw, thj[P.nx]);
-        if (nmode == 1 && s == R) ctl.DR = __fsub_rn(nw, thj[P.nx]);
-        if (s == 0) {
-          if (cap) ctl.caps++;
-          if (nmode == 1) ctl.births++;
-          if (nmode == 2) ctl.deaths++;
-          ctl.pmode = nmode; ctl.pnx = P.nx; ctl.pv = P.v; ctl.pc = P.c; ctl.pL = L; ctl.pR = R;
-          ctl.pl = P.l; ctl.pr = P.r; ctl.sL0 = sL0; ctl.sR0 = sR0; ctl.nL = nL; ctl.nR = nR;
-          ctl.used = used; ctl.leaf = leafm;
+        if (sep) {
+          asm volatile("bar.sync 1, 96;" ::: "memory");   // warps 0-2: the decision is published
+          accept = ctl.accept != 0;
         }
-        // the next tree's table; its accumulators start at zero
-        if (j + 1 < m) build_tc_slot(S, j + 1, s);
-        S.ovb[(cur ^ 1) * NODES + s] = 0ull;
+        if (s < NODES) {
+          int nmode = 0, L = 0, R = 0;
+          bool cap = false;
+          unsigned long long used = mk.used, leafm = mk.leaf;
+          if (accept && P.mode == 1) {
+            L = Lc; R = Rc;
+            if (L < 0 || R < 0) { cap = true; L = R = 0; }
+            else {
+              nmode = 1;
+              used |= (1ull << L) | (1ull << R);
+              leafm = (leafm & ~(1ull << P.nx)) | (1ull << L) | (1ull << R);
+            }
+          } else if (accept && P.mode == 2) {
+            nmode = 2;
+            used &= ~((1ull << P.l) | (1ull << P.r));
+            leafm = (leafm & ~((1ull << P.l) | (1ull << P.r))) | (1ull << P.nx);
+          }
+          // this thread's slot: new leaf value (DRMU) and apply delta
+          const unsigned long long lm1 = used & leafm;
+          const float old = thj[s];
+          float nw = old;
+          if ((lm1 >> s) & 1ull) {
+            nw = nws;
+            thj[s] = nw;
+          }
+          // leaf values of slots that stop being leaves do not change, so the reads below see old values
+          if (!(nmode == 2 && (s == P.l || s == P.r))) S.D[s] = __fsub_rn(nw, old);
+          if (nmode == 2 && s == P.nx) { S.D[P.l] = __fsub_rn(nw, thj[P.l]); S.D[P.r] = __fsub_rn(nw, thj[P.r]); }
+          if (nmode == 1 && s == L) ctl.DL = __fsub_rn(nw, thj[P.nx]);
+          if (nmode == 1 && s == R) ctl.DR = __fsub_rn(nw, thj[P.nx]);
+          if (s == 0) {
+            if (cap) ctl.caps++;
+            if (nmode == 1) ctl.births++;
+            if (nmode == 2) ctl.deaths++;
+            ctl.pmode = nmode; ctl.pnx = P.nx; ctl.pv = P.v; ctl.pc = P.c; ctl.pL = L; ctl.pR = R;
+            ctl.pl = P.l; ctl.pr = P.r; ctl.sL0 = sL0; ctl.sR0 = sR0; ctl.nL = nL; ctl.nR = nR;
+            ctl.used = used; ctl.leaf = leafm;
+          }
+          // the next tree's table; its accumulators start at zero
+          if (j + 1 < m) build_tc_slot(S, j + 1, s);
+          S.ovb[(cur ^ 1) * NODES + s] = 0ull;
+        }
       }
       __syncthreads();
     }
