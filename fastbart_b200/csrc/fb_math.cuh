@@ -47,7 +47,10 @@ __device__ __forceinline__ double u52d(uint32_t hi, uint32_t lo) {
   return ((double)k + 0.5) * 0x1p-52;
 }
 
-__device__ __noinline__ double fb_log(double x) {
+__device__ __forceinline__ double fb_log_inl(double x);
+__device__ __noinline__ double fb_log(double x) { return fb_log_inl(x); }
+// the same logarithm, inlined where its latency is on the critical path (the MH likelihoods)
+__device__ __forceinline__ double fb_log_inl(double x) {
   if (x != x) return x;
   if (x <= 0.0) return x == 0.0 ? -__longlong_as_double(0x7FF0000000000000LL) : __longlong_as_double(0x7FF8000000000000LL);
   if (__double_as_longlong(x) == 0x7FF0000000000000LL) return x;

@@ -300,7 +300,7 @@ __device__ __forceinline__ int count_goodvars_warp(const DTree* t, int x, const 
 }
 __device__ __noinline__ double lh(double b, double M, double t2) {   // src/bart_kernel.cpp:278
   const double k = b * t2 + 1.0;
-  return -0.5 * fbm::fb_log(k) + 0.5 * M * M * t2 / k;
+  return -0.5 * fbm::fb_log_inl(k) + 0.5 * M * M * t2 / k;   // inlined log: its division overlaps the one here
 }
 
 // ------------------------------------------------------------------------------------------------ learned proposal
@@ -1015,6 +1015,10 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
             nws = (float)(M / (a_prior + b) + z / sqrt(a_prior + b));
           }
         }
+        if (s < NODES) {   // the next tree's table (its accumulators start at zero) does not depend on this decision
+          if (j + 1 < m) build_tc_slot(S, j + 1, s);
+          S.ovb[(cur ^ 1) * NODES + s] = 0ull;
+        }
         if (sep) {
           asm volatile("bar.sync 1, 96;" ::: "memory");   // warps 0-2: the decision is published
           accept = ctl.accept != 0;
@@ -1057,9 +1061,6 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
             ctl.pl = P.l; ctl.pr = P.r; ctl.sL0 = sL0; ctl.sR0 = sR0; ctl.nL = nL; ctl.nR = nR;
             ctl.used = used; ctl.leaf = leafm;
           }
-          // the next tree's table; its accumulators start at zero
-          if (j + 1 < m) build_tc_slot(S, j + 1, s);
-          S.ovb[(cur ^ 1) * NODES + s] = 0ull;
         }
       }
       __syncthreads();
