@@ -250,7 +250,7 @@ def bench_ours(args):
     import fastbart_b200 as F
     from fastbart_b200 import diagnostics
 
-    b = F.Batch(chains, NSKIP, NDPOST, threads=args.threads, device=local)
+    b = F.Batch(chains, NSKIP, NDPOST, threads=args.threads, device=local, cluster=args.cluster)
     info = b.launch_info()
     stream = torch.cuda.current_stream()
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -330,7 +330,7 @@ def bench_ours(args):
         arr = (_lib.Chain * len(pin_chains))(*[api._as_chain(c, keep) for c in pin_chains])
         outs_p = [api._alloc_out(c, NSKIP, NDPOST, True, alloc=pinned) for c in pin_chains]
         oarr = (_lib.ChainOut * len(outs_p))(*[s_ for _, s_ in outs_p])
-        opt = _lib.Options(NSKIP, NDPOST, args.threads, 0, local)
+        opt = _lib.Options(NSKIP, NDPOST, args.threads, 0, local, args.cluster)
         h2d = sum(np.asarray(c["q"]).nbytes + 8 * len(c["y"]) + 4 * len(c["y"]) + len(c["y"]) for c in chains)
         h2d += len(chains) * 1024
         d2h = sum(8 * S + 8 * len(c["y"]) * (1 + NDPOST) + 8 * NDPOST * NTREE * 64 for c in chains)
@@ -612,6 +612,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--cluster", type=int, default=0, help="CTAs per chain (0: automatic, 1: no clusters)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
