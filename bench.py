@@ -250,6 +250,10 @@ def bench_ours(args):
     import fastbart_b200 as F
     from fastbart_b200 import diagnostics
 
+    tuned = None
+    if args.autotune:   # outside the timed region
+        tuned = F.autotune(chains, NSKIP, NDPOST, trial_sweeps=3, device=local)
+        args.threads, args.cluster = tuned["threads"], tuned["cluster"]
     b = F.Batch(chains, NSKIP, NDPOST, threads=args.threads, device=local, cluster=args.cluster)
     info = b.launch_info()
     stream = torch.cuda.current_stream()
@@ -363,7 +367,8 @@ def bench_ours(args):
                 "config": {"workload": WORKLOAD_NAME, "chains_per_gpu": len(chains), "ntree": NTREE,
                            "nskip": NSKIP, "ndpost": NDPOST, "n_range": N_RANGE, "p_range": P_RANGE,
                            "l2": "flushed (512 MiB write) before every timed step", "threads": info["threads"],
-                           "grid": info["grid"], "smem_bytes": info["smem"], "ctas_per_chain": info["cluster"]},
+                           "grid": info["grid"], "smem_bytes": info["smem"], "ctas_per_chain": info["cluster"],
+                           "shape": "autotuned" if tuned else "rules"},
                 "e2e": e2e, "gpu_launches": args.steps * info["launches"], "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "ess_per_s": ess_line, "r_f_vs_reference_chain0": r_f, "wall_s": wall}
         print(json.dumps(line), flush=True)
@@ -613,6 +618,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per chain (0: automatic, 1: no clusters)")
+    ap.add_argument("--autotune", action="store_true", help="time candidate launch shapes first (fb_autotune)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

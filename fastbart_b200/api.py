@@ -78,6 +78,18 @@ def fit_batch(chains: Sequence[dict], nskip: int, ndpost: int, threads: int = 0,
     return [_collect(o, oarr[k]) for k, (o, _) in enumerate(outs)]
 
 
+def autotune(chains: Sequence[dict], nskip: int, ndpost: int, trial_sweeps: int = 3, device: int = 0) -> dict:
+    """Fastest launch shape for these chains (fb_autotune): {"threads", "cluster", "trial_ms"}, to pass to Batch /
+    fit_batch."""
+    keep: list = []
+    arr = (_lib.Chain * len(chains))(*[_as_chain(c, keep) for c in chains])
+    opt = _options(nskip, ndpost, 0, 0, device, 0)
+    best = _lib.Options()
+    ms = C.c_double()
+    check(_lib.lib().fb_autotune(arr, len(chains), C.byref(opt), int(trial_sweeps), C.byref(best), C.byref(ms)))
+    return dict(threads=best.threads, cluster=best.cluster, trial_ms=ms.value)
+
+
 class Batch:
     """Staged batch: inputs uploaded once; run() repeats the full MCMC on the device; download() copies outputs."""
 

@@ -276,6 +276,47 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
   return FB_OK;
 }
 
+fb_status fb_autotune(const fb_chain* chains, int nchains, const fb_options* opt, int trial_sweeps, fb_options* best,
+                      double* best_ms) {
+  if (!chains || nchains < 1 || !opt || !best) return fail(FB_ERR_ARG, "chains, nchains >= 1, opt and best are required");
+  if (trial_sweeps < 2) return fail(FB_ERR_ARG, "trial_sweeps must be >= 2");
+  int ndev = 0, nsm = 148;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  CK(cudaSetDevice(opt->device));
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
+  std::vector<int> clusters{1};
+  for (int c = 2; c <= 8; c++)
+    if ((long long)nchains * c <= nsm) clusters.push_back(c);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double bestt = 1e300;
+  fb_options keep = *opt;
+  for (int T : {256, 384, 512}) {
+    for (int c : clusters) {
+      fb_options o = *opt;
+      o.nskip = trial_sweeps - 1; o.ndpost = 1; o.threads = T; o.cluster = c; o.sweeps_per_launch = 0;
+      fb_batch* b = nullptr;
+      if (fb_batch_create(chains, nchains, &o, &b) != FB_OK) continue;   // shape not possible here
+      // only shapes whose clusters are all resident at once (a second wave is never the fastest)
+      if (b->cluster != c || (c > 1 && b->grid < nchains * c)) { fb_batch_destroy(b); continue; }
+      float ms = 0.0f;
+      const bool ok = fb_batch_run(b, nullptr) == FB_OK && cudaEventRecord(e0) == cudaSuccess &&
+                      fb_batch_run(b, nullptr) == FB_OK && cudaEventRecord(e1) == cudaSuccess &&
+                      cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+      fb_batch_destroy(b);
+      if (!ok) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(FB_ERR_CUDA, "trial run failed"); }
+      if (ms < bestt) { bestt = ms; keep = *opt; keep.threads = T; keep.cluster = c; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (bestt == 1e300) return fail(FB_ERR_CUDA, "no launch shape could be created");
+  *best = keep;
+  if (best_ms) *best_ms = bestt;
+  return FB_OK;
+}
+
 fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
   if (!b) return fail(FB_ERR_ARG, "batch is NULL");
   CK(cudaSetDevice(b->device));

@@ -166,3 +166,13 @@ def test_statistical_agreement_with_reference(orc):
     sr = np.mean([r["sigma"][800:].mean() for r in rs])
     assert corr >= 0.98 and corr >= seed_spread - 0.003, (corr, seed_spread)
     assert abs(sg / sr - 1) < 0.02, (sg, sr)
+
+
+def test_autotune_picks_a_shape_with_identical_results():
+    chains = [W.fwbart_friedman(n=3000, p=6, seed=51 + k, ntree=20, nskip=8, ndpost=4) for k in range(3)]
+    best = F.autotune(chains, 8, 4, trial_sweeps=2)
+    assert best["threads"] in (256, 384, 512) and 1 <= best["cluster"] <= 8 and best["trial_ms"] > 0
+    tuned = fit_batch(chains, 8, 4, threads=best["threads"], cluster=best["cluster"])
+    plain = fit_batch(chains, 8, 4, cluster=1)
+    for a, b in zip(tuned, plain):
+        _compare(a, b)
