@@ -20,7 +20,7 @@ EXPORTS = ["fb_last_error", "fb_version", "fb_fit_batch", "fb_batch_create", "fb
            "fb_varcount", "fb_compile_trees", "fb_compiled_info", "fb_compiled_arrays", "fb_compiled_free",
            "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass",
            "fb_batch_set_proposal", "fb_batch_collect", "fb_batch_training_data", "fb_train_proposal",
-           "fb_mlp_loss_grad", "fb_autotune"]
+           "fb_mlp_loss_grad", "fb_autotune", "fb_cut_codes"]
 
 MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
 
@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         L.fb_predict_draw_static.argtypes = [vp, vp, i, i, i, d, vp]
         L.fb_debug_tree_pass.argtypes = [C.POINTER(PassState), vp]
         L.fb_batch_set_proposal.argtypes = [vp, C.POINTER(ProposalModel)]
+        L.fb_cut_codes.argtypes = [vp, i, i, vp, vp, i, vp]
         L.fb_autotune.argtypes = [C.POINTER(Chain), i, C.POINTER(Options), i, C.POINTER(Options), C.POINTER(d)]
         L.fb_batch_collect.argtypes = [vp, i]
         L.fb_batch_training_data.argtypes = [vp, vp, vp, vp, i, C.POINTER(i)]

@@ -209,6 +209,22 @@ def mlp_loss_grad(model: dict, x, y, mask, device: int = 0) -> tuple[float, dict
     return loss.value, g
 
 
+def cut_codes(x, cutpoints: Sequence[np.ndarray], device: int = 0) -> np.ndarray:
+    """Cutpoint codes on the device (fb_cut_codes): q [p][n] uint8 with x < cutpoints[v][c] <=> q <= c."""
+    X = np.asarray(x, dtype=np.float64)
+    if X.ndim == 1:
+        X = X[:, None]
+    n, p = X.shape
+    cols = [np.ascontiguousarray(X[:, j]) for j in range(p)]
+    cps = [np.ascontiguousarray(c, dtype=np.float64) for c in cutpoints]
+    cp = (C.c_void_p * max(1, p))(*[c.ctypes.data for c in cols])
+    kp = (C.c_void_p * max(1, p))(*[c.ctypes.data for c in cps])
+    nc = np.array([c.size for c in cps], dtype=np.int32)
+    q = np.zeros((p, n), dtype=np.uint8)
+    check(_lib.lib().fb_cut_codes(cp, p, n, kp, ptr(nc), int(device), ptr(q)))
+    return q
+
+
 # ------------------------------------------------------------------------------------------------ tree text
 def trees_text(trees: np.ndarray, p: int) -> str:
     t = np.ascontiguousarray(trees, dtype=np.uint64)

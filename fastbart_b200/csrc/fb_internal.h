@@ -152,6 +152,8 @@ int mlp_grad_launch(const MlpParams& P, const float* X, const int* Y, const unsi
 int mlp_adam_launch(float* p, float* m1, float* m2, const float* g, float inv_batch, float lr, int step,
                     const MlpParams& P, void* stream);
 
+// cutpoint codes of p columns of n values (x [p][n], cutpoints cuts[cutoff[v] .. cutoff[v + 1]), q [p][n])
+int launch_cut_codes(const double* x, int n, int p, const double* cuts, const int* cutoff, uint8_t* q, void* stream);
 // fixed device scratch of the allocation-free predict call: n * (ncol + 1) doubles at most (8 MiB per device)
 constexpr size_t PREDICT_SCRATCH_DOUBLES = size_t(1) << 20;
 // 0: *ptr = the scratch's address on `device` (the current device); -1: CUDA error; -2: device ordinal not tracked

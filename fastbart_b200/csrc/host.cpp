@@ -1033,6 +1033,42 @@ fb_status fb_mlp_loss_grad(const fb_proposal_model* model, const float* x, const
   return FB_OK;
 }
 
+fb_status fb_cut_codes(const double* const* cols, int ncol, int n, const double* const* cutpoints, const int* ncut,
+                       int device, uint8_t* q) {
+  if (ncol < 0 || n < 0) return fail(FB_ERR_ARG, "ncol and n must be >= 0");
+  if (ncol == 0 || n == 0) return FB_OK;
+  if (!cols || !cutpoints || !ncut || !q) return fail(FB_ERR_ARG, "cols, cutpoints, ncut and q are required");
+  std::vector<int> off(ncol + 1, 0);
+  for (int v = 0; v < ncol; v++) {
+    if (ncut[v] < 0 || ncut[v] > 255) return fail(FB_ERR_LIMIT, "predictor %d has %d cutpoints (0..255 allowed)", v, ncut[v]);
+    if (ncut[v] > 0 && !cutpoints[v]) return fail(FB_ERR_ARG, "cutpoints of predictor %d are missing", v);
+    for (int k = 1; k < ncut[v]; k++)
+      if (!(cutpoints[v][k - 1] < cutpoints[v][k])) return fail(FB_ERR_ARG, "cutpoints of predictor %d are not increasing", v);
+    off[v + 1] = off[v] + ncut[v];
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  CK(cudaSetDevice(device));
+  MlpJob job;
+  double *dx = nullptr, *dc = nullptr;
+  int* doff = nullptr;
+  uint8_t* dq = nullptr;
+  const size_t N = (size_t)ncol * n;
+  if (!job.alloc(&dx, N) || !job.alloc(&dc, (size_t)std::max(off[ncol], 1)) || !job.alloc(&doff, off.size()) ||
+      !job.alloc(&dq, N))
+    return fail(FB_ERR_CUDA, "out of device memory");
+  for (int v = 0; v < ncol; v++) {
+    if (!cols[v]) return fail(FB_ERR_ARG, "column %d is missing", v);
+    CK(cudaMemcpy(dx + (size_t)v * n, cols[v], sizeof(double) * n, cudaMemcpyHostToDevice));
+    if (ncut[v] > 0) CK(cudaMemcpy(dc + off[v], cutpoints[v], sizeof(double) * ncut[v], cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(doff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+  if (launch_cut_codes(dx, n, ncol, dc, doff, dq, nullptr) != 0)
+    return fail(FB_ERR_CUDA, "cut-code launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  CK(cudaMemcpy(q, dq, N, cudaMemcpyDeviceToHost));
+  return FB_OK;
+}
+
 // ------------------------------------------------------------------------------------------------ diagnostics
 fb_status fb_debug_tree_pass(const fb_pass_state* s, int64_t* out) {
   if (!s || !out || !s->r || !s->w || !s->tho || !s->thn || !s->thc) return fail(FB_ERR_ARG, "missing argument");

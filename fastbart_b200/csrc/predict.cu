@@ -233,6 +233,31 @@ int launch_predict(const DForest& f, const double* x, int n, int ld, int draw0, 
   return 0;
 }
 
+// Cutpoint codes (the findInterval step of R/fwbart.R:19): q[v][i] = number of cutpoints of v that are <= x[v][i]
+// (binary search; NaN gives 0), so that x < cut[v][c] <=> q <= c.  One thread per value, columns along grid y.
+__global__ void cut_codes_kernel(const double* __restrict__ x, int n, const double* __restrict__ cuts,
+                                 const int* __restrict__ cutoff, uint8_t* __restrict__ q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = blockIdx.y;
+  if (i >= n) return;
+  const double xv = x[(long long)v * n + i];
+  const double* cv = cuts + cutoff[v];
+  int lo = 0, hi = cutoff[v + 1] - cutoff[v];
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(cv + mid) <= xv) lo = mid + 1;
+    else hi = mid;
+  }
+  q[(long long)v * n + i] = (uint8_t)lo;
+}
+
+int launch_cut_codes(const double* x, int n, int p, const double* cuts, const int* cutoff, uint8_t* q, void* stream) {
+  if (n <= 0 || p <= 0) return 0;
+  cut_codes_kernel<<<dim3((n + 255) / 256, p), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(x, n, cuts, cutoff,
+                                                                                               q);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 // Fixed device scratch of fb_predict_draw_static: the newdata columns and the result are staged here instead of in
 // device memory allocated per call.  It belongs to the library's module, so every device that loads the library
 // holds it until the process exits.  Nothing in it needs to start at zero: each call copies in all the columns it

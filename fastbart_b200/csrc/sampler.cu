@@ -1238,7 +1238,7 @@ size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_sme
 
 int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster) {
   // the learned-proposal kernels need the same shared memory; residency is the same for both
-  const KernelFn k = kernel_for(0, cluster > 1, true);
+  const KernelFn k = kernel_for(gmax, cluster > 1, true);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
@@ -1264,10 +1264,8 @@ int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
                    void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  // learned-proposal kernels stream the leaf words (no per-thread word registers): their model calls keep the
-  // register-held variants from fitting in 128 registers without spilling in the pass
   const bool lp = (b.mw1 != nullptr && b.mix > 0.0) || b.train_cap > 0;
-  const KernelFn k = kernel_for(lp ? 0 : gmax, cluster > 1, lp);
+  const KernelFn k = kernel_for(gmax, cluster > 1, lp);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
   if (cudaMemsetAsync(b.queue, 0, sizeof(int), s) != cudaSuccess) return -1;
   if (cluster <= 1) {

@@ -204,6 +204,12 @@ fb_status fb_predict_draws_device(const fb_compiled* ct, const double* x_dev, in
 fb_status fb_predict_draw_static(const fb_compiled* ct, const double* const* cols, int ncol, int n, int draw,
                                  double mu, double* out);
 
+/* Cutpoint codes on the device, the findInterval step of R/fwbart.R:19 and R/fpbart.R:13: q[v][i] = number of
+ * cutpoints of predictor v that are <= cols[v][i] (so x < cutpoints[v][c] <=> q <= c; NaN gives 0).  cutpoints[v]
+ * has ncut[v] (0..255) strictly increasing values; q is [ncol][n] bytes (host). */
+fb_status fb_cut_codes(const double* const* cols, int ncol, int n, const double* const* cutpoints, const int* ncut,
+                       int device, uint8_t* q);
+
 /* ------------------------------------------------------------------------------------------------ diagnostics */
 
 /* One fused per-tree data pass on explicit state (the pass of src/bart_kernel.cpp:131-213), run by the same device

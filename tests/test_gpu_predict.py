@@ -85,3 +85,18 @@ def test_bulk_predict_bit_exact_all_evaluators(orc, p, n, ndraws, dup):
         o = orc.predict_draw(ref, [x[:, v] for v in range(p)], d + 1, 0.25)
         assert np.array_equal(got[d], o), d
         assert np.array_equal(F.predict_draw(ct, x, d + 1), o)
+
+
+def test_cut_codes_match_find_interval():
+    """Device cut codes equal numpy searchsorted(side='right') (R's findInterval), ties and NaN included."""
+    rng = np.random.default_rng(5)
+    x, _ = W.hazard_data(10007, 8)
+    x[::97, 2] = np.nan
+    d = F.prep.model_matrix(x, numcut=100)
+    x[::13, 0] = d.xi[0][rng.integers(0, d.xi[0].size, x[::13, 0].size)]   # values exactly on a cutpoint
+    q = F.cut_codes(x[:, d.rm_const - 1], d.xi)
+    for v in range(q.shape[0]):
+        col = x[:, d.rm_const[v] - 1]
+        ref = np.searchsorted(d.xi[v], col, side="right")
+        ref[np.isnan(col)] = 0
+        assert np.array_equal(q[v], ref.astype(np.uint8)), v
