@@ -91,8 +91,8 @@ def test_cut_codes_match_find_interval():
     """Device cut codes equal numpy searchsorted(side='right') (R's findInterval), ties and NaN included."""
     rng = np.random.default_rng(5)
     x, _ = W.hazard_data(10007, 8)
-    x[::97, 2] = np.nan
     d = F.prep.model_matrix(x, numcut=100)
+    x[::97, 2] = np.nan
     x[::13, 0] = d.xi[0][rng.integers(0, d.xi[0].size, x[::13, 0].size)]   # values exactly on a cutpoint
     q = F.cut_codes(x[:, d.rm_const - 1], d.xi)
     for v in range(q.shape[0]):
