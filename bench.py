@@ -9,6 +9,8 @@ from the initial state, producing all outputs (sigma draws, yhat.train draws, po
   python bench.py [--gpus N --steps K --warmup W]          this implementation (one rank per GPU under torchrun)
   python bench.py --impl reference [--steps K --warmup W]   the reference sampler (bart_fit_cpu, built from source
                                                             into oracle/_ref) on the host cores, one chain per core
+  --workload sparse | predict | learned                     the other measured configurations: 16 chains of n 65,536
+                                                            on clusters; bulk predict_draw; learned vs plain proposal
 
 Timing: W untimed warm-up steps; K timed steps, each preceded (outside its event pair) by a write of 512 MiB to flush
 L2; CUDA events on the launching stream; max over ranks.  Multi-GPU: every rank runs its own 96-chain batch (different
@@ -51,7 +53,7 @@ N_RANGE, P_RANGE = [3091, 4573], [15, 19]
 def set_workload(name: str):
     """'titer96' (the benchmark), 'small' (6 chains, one per shape, 40 sweeps: the profiling case) or 'sparse'
     (16 chains, n 65,536, p 32, numcut 255, Friedman-5 signal on 5 of 32 predictors: the large-n configuration, run
-    on thread-block clusters of 8 CTAs per chain)."""
+    on thread-block clusters; the automatic choice is 6 CTAs per chain)."""
     global NSKIP, NDPOST, WORKLOAD_NAME, workload, METRIC, FULL_REF, N_RANGE, P_RANGE
     if name == "sparse":
         WORKLOAD_NAME, FULL_REF, N_RANGE, P_RANGE = "friedman_sparse_16x65536", False, [65536, 65536], [32, 32]
@@ -501,18 +503,33 @@ def bench_predict(args):
             "frac": alg / per_s / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
             "algorithmic_bytes": alg,
             "node_steps_note": "x read once, every output written once, each draw's packed nodes and leaf values read"}
-    # end to end through the reference-facing call (one draw per call, host columns in, host result out)
+    # end to end with host buffers: every step copies x (column-major, pinned) to the device, evaluates all draws
+    # (fb_predict_draws_device) and copies every result back to pinned host memory
     e2e = None
     if not args.no_e2e:
-        ed = 3
-        F.predict_draw(ct, xh, 1)
+        xhp = torch.empty((PRED_P, PRED_ROWS), dtype=torch.float64, pin_memory=True)
+        xhp.copy_(torch.from_numpy(np.ascontiguousarray(xh.T)))
+        outh = torch.empty((PRED_DRAWS, PRED_ROWS), dtype=torch.float64, pin_memory=True)
+        xe = torch.empty_like(xd)
+
+        def e2e_step():
+            xe.copy_(xhp, non_blocking=True)
+            F.predict_draws_device(ct, xe.data_ptr(), PRED_P, PRED_ROWS, PRED_ROWS, 1, PRED_DRAWS, out.data_ptr(),
+                                   PRED_ROWS, stream.cuda_stream)
+            outh.copy_(out, non_blocking=True)
+        e2e_step()
+        torch.cuda.synchronize()
+        ed = 2
         t1 = time.perf_counter()
-        for d in range(ed):
-            F.predict_draw(ct, xh, 2 + d)
+        for _ in range(ed):
+            e2e_step()
+        torch.cuda.synchronize()
         e2e_s = shard.max_over_ranks((time.perf_counter() - t1) / ed, device="cuda")
-        e2e = {"value": PRED_ROWS * world / e2e_s, "unit": PRED_UNIT, "h2d_bytes_per_step": PRED_P * PRED_ROWS * 8,
-               "d2h_bytes_per_step": PRED_ROWS * 8, "steps": ed, "ms_per_step": 1000 * e2e_s,
-               "api": "fb_predict_draw (one draw per call: host columns copied in, result copied out)"}
+        assert np.array_equal(outh[0, :2000].numpy(), chk), "host copy of the bulk result disagrees"
+        e2e = {"value": PRED_DRAWS * PRED_ROWS * world / e2e_s, "unit": PRED_UNIT,
+               "h2d_bytes_per_step": PRED_P * PRED_ROWS * 8, "d2h_bytes_per_step": PRED_DRAWS * PRED_ROWS * 8,
+               "steps": ed, "ms_per_step": 1000 * e2e_s,
+               "api": "fb_predict_draws_device with pinned host x copied in and all 1,000 x 1 M results copied out"}
     if rank == 0:
         line = {"metric": PRED_METRIC, "value": value, "unit": PRED_UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
