@@ -81,6 +81,8 @@ struct DBufs {
   const uint16_t* mw2; const float* mb2;   // [MLP_H][MLP_H], [MLP_H]
   const uint16_t* mw3; const float* mb3;   // [MLP_OUT][MLP_H], [MLP_OUT]
   double mix;                              // probability of the model component
+  // the model's per-tree choices of the current sweep (model_pass_kernel), or null: birth variable, correction
+  const int* mvar; const double* mcorr;
   // accepted births as training examples (train_cap 0: off)
   float* feat;                             // [trees][MLP_IN] features of each tree's birth proposal
   unsigned* feat_valid;                    // [trees] valid-variable mask of that proposal
@@ -96,6 +98,8 @@ size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_sme
 int sampler_gmax(int threads, int n_pad_max);
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
                    void* stream);
+// learned-proposal pre-pass of sweep it (one CTA per chain): fills b.mvar / b.mcorr
+int launch_model_pass(const DBufs& b, int it, void* stream);
 // CTAs that can be resident at once (a multiple of cluster), 0 when none
 int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster);
 

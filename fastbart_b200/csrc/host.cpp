@@ -99,6 +99,8 @@ struct fb_batch {
   long long rows = 0, qbytes = 0, leafbytes = 0, ntrees = 0, nsig = 0, nyhat = 0, ntout = 0;
   cudaStream_t stream = nullptr;
   void* model_mem = nullptr;   // learned proposal weights (owned; also listed in allocs)
+  int* mvar = nullptr;         // learned proposal: per-tree choices of the current sweep (model pre-pass)
+  double* mcorr = nullptr;
   int cluster = 1;             // CTAs per chain
   int slice_rows = 0;          // rows of one CTA's slice (shared-memory capacity)
   int collect_cap = 0;         // allocated capacity of the training-example buffers
@@ -268,6 +270,20 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
   const int S = b->nskip + b->ndpost;
   if (b->d.train_cap > 0 && cudaMemsetAsync(b->d.train_count, 0, sizeof(int), b->stream) != cudaSuccess)
     return fail(FB_ERR_CUDA, "cannot reset the training-example counter");
+  if (b->d.mw1 && b->d.mix > 0.0 && b->d.train_cap == 0) {
+    // learned proposal: per sweep, the model's pre-pass, then the plain sampler kernel reading its choices
+    DBufs ds = b->d;
+    ds.mvar = b->mvar; ds.mcorr = b->mcorr;
+    DBufs dk = ds;
+    dk.mw1 = nullptr; dk.mix = 0.0;   // selects the sampler variant without in-kernel model calls
+    for (int it = 0; it < S; it++) {
+      if (launch_model_pass(ds, it, stream) != 0)
+        return fail(FB_ERR_CUDA, "model pre-pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+      if (launch_sampler(dk, it, it + 1, b->threads, b->grid, b->smem, b->gmax, b->cluster, stream) != 0)
+        return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    return FB_OK;
+  }
   for (int it0 = 0; it0 < S; it0 += b->spl) {
     const int it1 = std::min(S, it0 + b->spl);
     if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, b->gmax, b->cluster, stream) != 0)
@@ -343,6 +359,13 @@ fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
   CK(cudaMemcpy(b2, model->b2, 4 * MLP_H, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b3, model->b3, 4 * MLP_OUT, cudaMemcpyHostToDevice));
   b->d.mw1 = w1; b->d.mw2 = w2; b->d.mw3 = w3; b->d.mb1 = b1; b->d.mb2 = b2; b->d.mb3 = b3; b->d.mix = model->mix;
+  if (!b->mvar) {
+    if (cudaMalloc(&b->mvar, sizeof(int) * (size_t)b->ntrees) != cudaSuccess) return fail(FB_ERR_CUDA, "out of device memory");
+    b->allocs.push_back(b->mvar);
+    if (cudaMalloc(&b->mcorr, sizeof(double) * (size_t)b->ntrees) != cudaSuccess)
+      return fail(FB_ERR_CUDA, "out of device memory");
+    b->allocs.push_back(b->mcorr);
+  }
   return FB_OK;
 }
 

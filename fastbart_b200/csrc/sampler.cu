@@ -474,6 +474,9 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
         v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
         if (feat) *fvalid = node_features(t, nx, cnt[nx], -1, C, feat);
       }
+    } else if (B.mvar) {   // the learned model's choice, computed for this sweep by model_pass_kernel
+      v = B.mvar[C.off_tree + j];
+      corr = B.mcorr[C.off_tree + j];
     } else {
       v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
     }
@@ -496,7 +499,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
       }
       const double Pbotx = (double)1 / ngood;
       pr = (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
-      if (model) pr = pr * corr;
+      if (model || (!LP && B.mvar)) pr = pr * corr;
       P.mode = 1; P.nx = (uint8_t)nx; P.v = (uint8_t)v; P.c = (uint8_t)c;
     }
   } else if (nnogs > 0) {
@@ -510,6 +513,8 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
     pr = ((1 - PGny) * PBy * Pboty) / (PGny * (1 - PGlx) * (1 - PGrx) * PDx * Pnogx);
     if constexpr (LP) {
       if (model) pr = pr * model_death_corr(t, nx, cnt[l] + cnt[r], C, B);   // the reverse birth
+    } else {
+      if (B.mvar) pr = pr * B.mcorr[C.off_tree + j];
     }
     P.mode = 2; P.nx = (uint8_t)nx; P.l = (uint8_t)l; P.r = (uint8_t)r;
   }
@@ -529,6 +534,65 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
   }
   P.cand = cand;
   return P;
+}
+
+// Learned-proposal pre-pass of sweep it, launched before the sweep's sampler launch: for every tree of every chain
+// (one CTA per chain, one thread per tree), the same node choice as propose() makes, then the model's birth variable
+// and proposal-ratio correction, or a death's reverse-birth correction, into B.mvar / B.mcorr.  Keeping the model
+// out of the sampler kernel keeps its calls from costing the sampler registers.  Reads the trees as the previous
+// launch left them (the first CTA's copy in cluster mode: every copy is identical between sweeps), or root-only
+// trees for sweep 0.
+__global__ void __launch_bounds__(256) model_pass_kernel(DBufs B, int it) {
+  const DChain& C = B.chains[blockIdx.x];
+  const int CS = B.cluster > 1 ? B.cluster : 1;
+  const DTree* trees = B.trees + C.off_tree * CS;
+  const long long* s0g = B.s0 + C.off_tree * CS * LST;
+  // sweep 0 starts from root-only trees, which the sampler launch itself initialises: stand in for them here
+  DTree root;
+  int root_cnt[NODES];
+  if (it == 0) {
+    uint8_t* rb = reinterpret_cast<uint8_t*>(&root);
+    for (int k = 0; k < (int)sizeof(DTree); k++) rb[k] = 0;
+    root.ngv[0] = (uint8_t)C.root_ngv;
+    root.used = 1ull; root.leaf = 1ull;
+    for (int k = 0; k < NODES; k++) root_cnt[k] = 0;
+    root_cnt[0] = C.n;
+  }
+  for (int j = threadIdx.x; j < C.m; j += blockDim.x) {
+    const DTree* t = it == 0 ? &root : trees + j;
+    const int* cnt = it == 0 ? root_cnt : reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES);
+    const unsigned long long used = t->used, leafm = t->leaf;
+    unsigned long long goodm = 0, nogm = 0;
+    for (unsigned long long um = used; um; um &= um - 1ull) {
+      const int s = __ffsll((long long)um) - 1;
+      if ((leafm >> s) & 1ull) {
+        const int g = t->ngv[s] == 255 ? count_goodvars(t, s, C.numcut, C.p) : t->ngv[s];
+        if (g > 0) goodm |= 1ull << s;
+      } else if (((leafm >> t->l[s]) & 1ull) && ((leafm >> t->r[s]) & 1ull)) {
+        nogm |= 1ull << s;
+      }
+    }
+    const int ngood = __popcll(goodm), nnogs = __popcll(nogm);
+    const double PBx = ngood == 0 ? 0 : (used == 1ull ? 1 : 0.5);
+    const fbm::U4 x = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP, C.seed);
+    const double ub = fbm::u32d(x.x), un = fbm::u32d(x.y), uv = fbm::u32d(x.z);
+    int v = 0;
+    double corr = 1.0;
+    if (ub < PBx) {
+      const int nx = select_kth(goodm, (int)(un * ngood));
+      v = model_birth_var(t, nx, cnt[nx], C, B, j, it, uv, &corr, nullptr, nullptr);
+    } else if (nnogs > 0) {
+      const int nx = select_kth(nogm, (int)(un * nnogs));
+      corr = model_death_corr(t, nx, cnt[t->l[nx]] + cnt[t->r[nx]], C, B);
+    }
+    const_cast<int*>(B.mvar)[C.off_tree + j] = v;
+    const_cast<double*>(B.mcorr)[C.off_tree + j] = corr;
+  }
+}
+
+int launch_model_pass(const DBufs& b, int it, void* stream) {
+  model_pass_kernel<<<b.nchains, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(b, it);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 // ------------------------------------------------------------------------------------------------ shared layout
