@@ -76,13 +76,12 @@ struct DBufs {
   int n_pad_max;                   // rows of one CTA's slice (shared-memory capacity)
   int rows_in_smem;
   int cluster;                     // CTAs per chain (a thread-block cluster when > 1)
-  // learned split-variable proposal (null mw1: BART's uniform proposal)
-  const uint16_t* mw1; const float* mb1;   // [MLP_H][MLP_IN] bf16, [MLP_H]
-  const uint16_t* mw2; const float* mb2;   // [MLP_H][MLP_H], [MLP_H]
-  const uint16_t* mw3; const float* mb3;   // [MLP_OUT][MLP_H], [MLP_OUT]
-  double mix;                              // probability of the model component
-  // the model's per-tree choices of the current sweep (model_pass_kernel), or null: birth variable, correction
-  const int* mvar; const double* mcorr;
+  // learned split-variable proposal (null mvar: BART's uniform proposal): the model's weight image (see MIMG_*),
+  // staged in shared memory behind the sampler's own layout when model_smem is set, else read from global memory
+  const uint32_t* mimg;
+  int model_smem;
+  double mix;                              // probability of the model component, in (0, 1]
+  int* mvar; double* mcorr;                // [trees] the model's choices of the current sweep: variable, correction
   // accepted births as training examples (train_cap 0: off)
   float* feat;                             // [trees][MLP_IN] features of each tree's birth proposal
   unsigned* feat_valid;                    // [trees] valid-variable mask of that proposal
@@ -94,12 +93,12 @@ struct DBufs {
 };
 
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster);
+// whether the sampler stages the proposal model's weights in its pass bins (no extra shared memory needed)
+bool sampler_bins_hold_model(int threads);
 // groups of 4 rows per row thread held in registers (1, 2, 4, 8), or 0 when the rows stream from L2 in the pass
 int sampler_gmax(int threads, int n_pad_max);
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
                    void* stream);
-// learned-proposal pre-pass of sweep it (one CTA per chain): fills b.mvar / b.mcorr
-int launch_model_pass(const DBufs& b, int it, void* stream);
 // CTAs that can be resident at once (a multiple of cluster), 0 when none
 int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster);
 
@@ -144,6 +143,12 @@ struct DForest {
 // Learned-proposal training (mlp.cu).  Flat FP32 parameter vector: w1 [H][IN], b1 [H], w2 [H][H], b2 [H],
 // w3 [OUT][H], b3 [OUT]; the forward pass reads BF16 copies of the weights.
 constexpr int MLP_NPARAM = MLP_H * MLP_IN + MLP_H + MLP_H * MLP_H + MLP_H + MLP_OUT * MLP_H + MLP_OUT;
+// The sampler's image of a proposal model (32-bit words): BF16 weight pairs row by row, rows padded to an odd
+// number of words so that the lanes of a warp reading one row each hit distinct shared-memory banks, then the
+// FP32 biases.  W1 rows [MLP_H][MIMG_W1S], W2 rows [MLP_H][MIMG_W2S], W3 rows [MLP_OUT][MIMG_W2S], b1, b2, b3.
+constexpr int MIMG_W1S = MLP_IN / 2, MIMG_W2S = MLP_H / 2 + 1;
+constexpr int MIMG_W2 = MLP_H * MIMG_W1S, MIMG_W3 = MIMG_W2 + MLP_H * MIMG_W2S, MIMG_B = MIMG_W3 + MLP_OUT * MIMG_W2S;
+constexpr int MIMG_WORDS = (MIMG_B + 2 * MLP_H + MLP_OUT + 3) / 4 * 4;   // a multiple of 16 bytes
 struct MlpParams {
   uint16_t* w1; uint16_t* w2; uint16_t* w3;   // BF16 weights (device)
   const float* b1; const float* b2; const float* b3;

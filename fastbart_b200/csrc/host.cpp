@@ -99,7 +99,8 @@ struct fb_batch {
   long long rows = 0, qbytes = 0, leafbytes = 0, ntrees = 0, nsig = 0, nyhat = 0, ntout = 0;
   cudaStream_t stream = nullptr;
   void* model_mem = nullptr;   // learned proposal weights (owned; also listed in allocs)
-  int* mvar = nullptr;         // learned proposal: per-tree choices of the current sweep (model pre-pass)
+  int* mvar = nullptr;         // learned proposal: per-tree choices of the current sweep (owned)
+  size_t smem_model = 0;       // the sampler's shared memory with the proposal model's weight image
   double* mcorr = nullptr;
   int cluster = 1;             // CTAs per chain
   int slice_rows = 0;          // rows of one CTA's slice (shared-memory capacity)
@@ -270,23 +271,10 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
   const int S = b->nskip + b->ndpost;
   if (b->d.train_cap > 0 && cudaMemsetAsync(b->d.train_count, 0, sizeof(int), b->stream) != cudaSuccess)
     return fail(FB_ERR_CUDA, "cannot reset the training-example counter");
-  if (b->d.mw1 && b->d.mix > 0.0 && b->d.train_cap == 0) {
-    // learned proposal: per sweep, the model's pre-pass, then the plain sampler kernel reading its choices
-    DBufs ds = b->d;
-    ds.mvar = b->mvar; ds.mcorr = b->mcorr;
-    DBufs dk = ds;
-    dk.mw1 = nullptr; dk.mix = 0.0;   // selects the sampler variant without in-kernel model calls
-    for (int it = 0; it < S; it++) {
-      if (launch_model_pass(ds, it, stream) != 0)
-        return fail(FB_ERR_CUDA, "model pre-pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-      if (launch_sampler(dk, it, it + 1, b->threads, b->grid, b->smem, b->gmax, b->cluster, stream) != 0)
-        return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-    }
-    return FB_OK;
-  }
   for (int it0 = 0; it0 < S; it0 += b->spl) {
     const int it1 = std::min(S, it0 + b->spl);
-    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->smem, b->gmax, b->cluster, stream) != 0)
+    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->d.mvar ? b->smem_model : b->smem, b->gmax, b->cluster,
+                       stream) != 0)
       return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   return FB_OK;
@@ -337,28 +325,28 @@ fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
   if (!b) return fail(FB_ERR_ARG, "batch is NULL");
   CK(cudaSetDevice(b->device));
   if (!model || model->mix <= 0.0) {
-    b->d.mw1 = nullptr; b->d.mix = 0.0;
+    b->d.mvar = nullptr; b->d.mcorr = nullptr; b->d.mix = 0.0;
     return FB_OK;
   }
   if (!model->w1 || !model->b1 || !model->w2 || !model->b2 || !model->w3 || !model->b3)
     return fail(FB_ERR_ARG, "every weight and bias array of the model is required");
   if (!(model->mix <= 1.0)) return fail(FB_ERR_ARG, "mix must be in (0, 1]");
-  const size_t n1 = (size_t)MLP_H * MLP_IN, n2 = (size_t)MLP_H * MLP_H, n3 = (size_t)MLP_OUT * MLP_H;
+  // the sampler's weight image (MIMG_* in fb_internal.h): BF16 pairs row by row, padded rows, then the biases
+  std::vector<uint32_t> img(MIMG_WORDS, 0u);
+  auto pair = [](const uint16_t* row, int kk) { return (uint32_t)row[2 * kk] | ((uint32_t)row[2 * kk + 1] << 16); };
+  for (int o = 0; o < MLP_H; o++)
+    for (int kk = 0; kk < MLP_IN / 2; kk++) img[o * MIMG_W1S + kk] = pair(model->w1 + o * MLP_IN, kk);
+  for (int o = 0; o < MLP_H; o++)
+    for (int kk = 0; kk < MLP_H / 2; kk++) img[MIMG_W2 + o * MIMG_W2S + kk] = pair(model->w2 + o * MLP_H, kk);
+  for (int o = 0; o < MLP_OUT; o++)
+    for (int kk = 0; kk < MLP_H / 2; kk++) img[MIMG_W3 + o * MIMG_W2S + kk] = pair(model->w3 + o * MLP_H, kk);
+  std::memcpy(img.data() + MIMG_B, model->b1, 4 * MLP_H);
+  std::memcpy(img.data() + MIMG_B + MLP_H, model->b2, 4 * MLP_H);
+  std::memcpy(img.data() + MIMG_B + 2 * MLP_H, model->b3, 4 * MLP_OUT);
   if (!b->model_mem) {
-    if (cudaMalloc(&b->model_mem, 2 * (n1 + n2 + n3) + 4 * (2 * MLP_H + MLP_OUT)) != cudaSuccess)
-      return fail(FB_ERR_CUDA, "out of device memory");
+    if (cudaMalloc(&b->model_mem, 4 * img.size()) != cudaSuccess) return fail(FB_ERR_CUDA, "out of device memory");
     b->allocs.push_back(b->model_mem);
   }
-  unsigned char* m = static_cast<unsigned char*>(b->model_mem);
-  uint16_t* w1 = reinterpret_cast<uint16_t*>(m); uint16_t* w2 = w1 + n1; uint16_t* w3 = w2 + n2;
-  float* b1 = reinterpret_cast<float*>(w3 + n3); float* b2 = b1 + MLP_H; float* b3 = b2 + MLP_H;
-  CK(cudaMemcpy(w1, model->w1, 2 * n1, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(w2, model->w2, 2 * n2, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(w3, model->w3, 2 * n3, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b1, model->b1, 4 * MLP_H, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b2, model->b2, 4 * MLP_H, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b3, model->b3, 4 * MLP_OUT, cudaMemcpyHostToDevice));
-  b->d.mw1 = w1; b->d.mw2 = w2; b->d.mw3 = w3; b->d.mb1 = b1; b->d.mb2 = b2; b->d.mb3 = b3; b->d.mix = model->mix;
   if (!b->mvar) {
     if (cudaMalloc(&b->mvar, sizeof(int) * (size_t)b->ntrees) != cudaSuccess) return fail(FB_ERR_CUDA, "out of device memory");
     b->allocs.push_back(b->mvar);
@@ -366,6 +354,18 @@ fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
       return fail(FB_ERR_CUDA, "out of device memory");
     b->allocs.push_back(b->mcorr);
   }
+  CK(cudaMemcpy(b->model_mem, img.data(), 4 * img.size(), cudaMemcpyHostToDevice));
+  b->d.mimg = static_cast<const uint32_t*>(b->model_mem);
+  // the sampler stages the image in its pass bins when they are large enough (wide CTAs); otherwise behind its
+  // shared memory when that keeps every CTA of the launch resident, else it reads the image from global memory
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device) != cudaSuccess) optin = 0;
+  const size_t with = (b->smem + 15) / 16 * 16 + 4 * (size_t)MIMG_WORDS;
+  b->d.model_smem = !sampler_bins_hold_model(b->threads) && with <= (size_t)optin &&
+                    sampler_max_grid(b->threads, with, b->device, b->gmax, b->cluster) >= b->grid;
+  b->smem_model = b->d.model_smem ? with : b->smem;
+  b->d.mix = model->mix;
+  b->d.mvar = b->mvar; b->d.mcorr = b->mcorr;
   return FB_OK;
 }
 

@@ -48,6 +48,11 @@ constexpr int TOT = 16;       // CTA totals per tree: [0, NBS) leaf sums, NBS.. 
 constexpr int NSPLIT = 3;     // split partials per row thread: sum fx(w), sum fx(w*R), count of the left child
 constexpr int LST = LEAF_STAT_WORDS;
 constexpr int ZMAX = 16;      // leaf-mu normals drawn ahead per tree (candidate slots beyond are drawn in the step)
+constexpr int MODE_PLAIN = 0, MODE_MODEL = 1, MODE_COLLECT = 2;   // sampler kernel variants (see sampler_kernel)
+// the pass bins of a CTA of `threads` can hold the proposal model's weight image at sweep start
+__host__ __device__ inline bool bins_hold_model(int threads) {
+  return (size_t)(NBS + NSPLIT) * (size_t)(threads - 32) * 8 >= (size_t)MIMG_WORDS * 4;
+}
 
 struct Prop {                 // proposal of one tree for the current sweep
   double logpr, lu;
@@ -288,16 +293,6 @@ __device__ int count_goodvars(const DTree* t, int x, const int* nc, int p) {   /
   }
   return g;
 }
-// goodvar count of node x, lanes of one warp over the predictors (p <= 32)
-__device__ __forceinline__ int count_goodvars_warp(const DTree* t, int x, const int* nc, int p, int lane) {
-  bool good = false;
-  if (lane < p) {
-    int L, U;
-    node_range(t, x, lane, nc[lane], L, U);
-    good = U >= L;
-  }
-  return __popc(__ballot_sync(0xffffffffu, good));
-}
 __device__ __noinline__ double lh(double b, double M, double t2) {   // src/bart_kernel.cpp:278
   const double k = b * t2 + 1.0;
   return -0.5 * fbm::fb_log_inl(k) + 0.5 * M * M * t2 / k;   // inlined log: its division overlaps the one here
@@ -337,108 +332,257 @@ __device__ __noinline__ unsigned node_features(const DTree* t, int nx, int cnt, 
   return valid;
 }
 
-__device__ __forceinline__ float bf16f(uint16_t h) { return __uint_as_float((unsigned)h << 16); }
+// ---- the learned model's phase at sweep start: one warp per tree, up to MP_NB trees of a warp at once
+// A tree held across a warp's registers: lane i holds bytes [16 i, 16 i + 16) of the DTree, and a field is read by a
+// warp-uniform shuffle.  The proposal's tree walks then cost shuffles instead of dependent global loads.
+namespace wt {
+constexpr int L = 0, R = NODES, PAR = 2 * NODES, V = 3 * NODES, C = 4 * NODES, D = 5 * NODES, NGV = 6 * NODES;
+constexpr int USED = 7 * NODES, LEAF = 7 * NODES + 8, UNITS = (int)(sizeof(DTree) / 16);
+static_assert(sizeof(DTree) % 16 == 0 && UNITS <= 32, "a tree fits one 16-byte unit per lane");
+__device__ __forceinline__ uint4 load(const DTree* t, int lane) {
+  return lane < UNITS ? reinterpret_cast<const uint4*>(t)[lane] : make_uint4(0u, 0u, 0u, 0u);
+}
+__device__ __forceinline__ uint32_t word(const uint4& q, int off) {   // the 32-bit word at byte offset off (uniform)
+  const int c = (off >> 2) & 3;
+  const uint32_t w = c == 0 ? q.x : c == 1 ? q.y : c == 2 ? q.z : q.w;
+  return __shfl_sync(0xffffffffu, w, off >> 4);
+}
+__device__ __forceinline__ int byte(const uint4& q, int field, int s) {
+  const int off = field + s;
+  return (int)((word(q, off & ~3) >> (8 * (off & 3))) & 0xffu);
+}
+__device__ __forceinline__ unsigned long long mask(const uint4& q, int off) {
+  return (unsigned long long)word(q, off) | ((unsigned long long)word(q, off + 4) << 32);
+}
+// node_range (src/bart_kernel.cpp:238-251) of node x for predictor v with nc cutpoints; the walk is warp-uniform
+__device__ __forceinline__ void node_range(const uint4& q, int x, int v, int nc, int& L, int& U) {
+  L = 0; U = nc - 1;
+  int node = x;
+  for (int s = 0; s < MAXDEPTH; s++) {
+    if (node == 0) break;
+    const int pa = byte(q, PAR, node);
+    const int vp = byte(q, V, pa), lp = byte(q, wt::L, pa), cp = byte(q, wt::C, pa);
+    if (vp == v) {
+      if (lp == node) { if (cp - 1 < U) U = cp - 1; }
+      else { if (cp + 1 > L) L = cp + 1; }
+    }
+    node = pa;
+  }
+}
+}  // namespace wt
 
-// MLP forward (FP32, no fused multiply-add, fixed order) and masked softmax in FP64: q[v] for valid v, else 0.
-// Four outputs of a dense layer at once (four independent accumulators share each input load); each output is the
-// sequential sum bias + w[0] x[0] + w[1] x[1] + ... in FP32 without fused multiply-add, as the oracle computes it.
-// Weight rows are read as pairs of BF16 values (rows start on 4-byte boundaries: NIN is even).
-template <int NIN>
-__device__ __forceinline__ void dense4(const uint16_t* W, const float* bias, const float* x, int h, float (&a)[4]) {
-  const uint32_t* w[4];
+constexpr int MP_NB = 1;   // trees of one warp evaluated together (each weight load serves all of them)
+
+// node_features with lane v on predictor v, from a warp-held tree: lane v returns x[2 + v], x[34 + v], x[66 + v] in
+// xa, xb, xc and every lane x[0], x[1]; returns the valid mask
+__device__ __forceinline__ unsigned node_features_wt(const uint4& q, int nx, int cnt, int exclude, const DChain& C,
+                                                     int lane, float& x0, float& x1, float& xa, float& xb, float& xc) {
+  x0 = __fdiv_rn((float)wt::byte(q, wt::D, nx), 8.0f);
+  x1 = __fdiv_rn((float)(31 - __clz(cnt + 1)), 16.0f);
+  int use = 0;
+  const unsigned long long inner = wt::mask(q, wt::USED) & ~wt::mask(q, wt::LEAF);
+  for (unsigned long long im = inner; im; im &= im - 1ull) {
+    const int sl = __ffsll((long long)im) - 1;
+    if (sl != exclude && wt::byte(q, wt::V, sl) == lane) use++;
+  }
+  xa = __fdiv_rn((float)(use < 8 ? use : 8), 8.0f);
+  const int nc = lane < C.p ? C.numcut[lane] : 0;
+  int L, U;
+  wt::node_range(q, nx, lane, nc, L, U);
+  const bool ok = nc > 0 && U >= L;
+  xb = ok ? __fdiv_rn((float)(U - L + 1), (float)nc) : 0.0f;
+  xc = ok ? __fdiv_rn((float)L, (float)nc) : 0.0f;
+  return __ballot_sync(0xffffffffu, ok);
+}
+
+// The model at NB nodes, evaluated by one warp from the weight image W (shared or global memory).  Lane o computes
+// hidden outputs o and o + 32, then logit o, of every node; each output is the sequential sum bias + w[0] x[0] +
+// w[1] x[1] + ... in FP32 without fused multiply-add.  The masked softmax is in FP64 (max over the valid logits, 0
+// when none; exp of the differences; their sum in predictor order).  q[b] = q_lane of node b (0 when invalid).
+__device__ __forceinline__ float feat_k(int k, float x0, float x1, float xa, float xb, float xc) {
+  return k == 0 ? x0 : k == 1 ? x1 : __shfl_sync(0xffffffffu, k < 34 ? xa : k < 66 ? xb : xc, (k - 2) & 31);
+}
+__device__ __forceinline__ float acc2(float a, uint32_t pw, float xlo, float xhi) {
+  a = __fadd_rn(a, __fmul_rn(__uint_as_float(pw << 16), xlo));
+  return __fadd_rn(a, __fmul_rn(__uint_as_float(pw & 0xFFFF0000u), xhi));
+}
+template <int NB>
+__device__ __forceinline__ void model_q_batch(const uint32_t* W, const float (&x0)[NB], const float (&x1)[NB],
+                                              const float (&xa)[NB], const float (&xb)[NB], const float (&xc)[NB],
+                                              const unsigned (&valid)[NB], int lane, double (&q)[NB]) {
+  const float* bias = reinterpret_cast<const float*>(W + MIMG_B);
+  float a0[NB], a1[NB], h1a[NB], h1b[NB];
+  const uint32_t* r0 = W + lane * MIMG_W1S;
+  const uint32_t* r1 = W + (lane + 32) * MIMG_W1S;
 #pragma unroll
-  for (int u = 0; u < 4; u++) { a[u] = __ldg(bias + h + u); w[u] = reinterpret_cast<const uint32_t*>(W + (h + u) * NIN); }
-#pragma unroll 8
-  for (int kk = 0; kk < NIN / 2; kk++) {
-    const float xa = x[2 * kk], xb = x[2 * kk + 1];
+  for (int b = 0; b < NB; b++) { a0[b] = bias[lane]; a1[b] = bias[lane + 32]; }
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const uint32_t pw = __ldg(w[u] + kk);
-      a[u] = __fadd_rn(a[u], __fmul_rn(__uint_as_float(pw << 16), xa));
-      a[u] = __fadd_rn(a[u], __fmul_rn(__uint_as_float(pw & 0xFFFF0000u), xb));
+  for (int kk = 0; kk < MIMG_W1S; kk++) {
+    const uint32_t p0 = r0[kk], p1 = r1[kk];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const float xl = feat_k(2 * kk, x0[b], x1[b], xa[b], xb[b], xc[b]);
+      const float xh = feat_k(2 * kk + 1, x0[b], x1[b], xa[b], xb[b], xc[b]);
+      a0[b] = acc2(a0[b], p0, xl, xh);
+      a1[b] = acc2(a1[b], p1, xl, xh);
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    h1a[b] = a0[b] > 0.0f ? a0[b] : 0.0f; h1b[b] = a1[b] > 0.0f ? a1[b] : 0.0f;
+    a0[b] = bias[MLP_H + lane]; a1[b] = bias[MLP_H + lane + 32];
+  }
+  r0 = W + MIMG_W2 + lane * MIMG_W2S;
+  r1 = W + MIMG_W2 + (lane + 32) * MIMG_W2S;
+#pragma unroll
+  for (int kk = 0; kk < MLP_H / 2; kk++) {
+    const uint32_t p0 = r0[kk], p1 = r1[kk];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const float hl = __shfl_sync(0xffffffffu, kk < 16 ? h1a[b] : h1b[b], (2 * kk) & 31);
+      const float hh = __shfl_sync(0xffffffffu, kk < 16 ? h1a[b] : h1b[b], (2 * kk + 1) & 31);
+      a0[b] = acc2(a0[b], p0, hl, hh);
+      a1[b] = acc2(a1[b], p1, hl, hh);
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    h1a[b] = a0[b] > 0.0f ? a0[b] : 0.0f; h1b[b] = a1[b] > 0.0f ? a1[b] : 0.0f;   // now the second hidden layer
+    a0[b] = bias[2 * MLP_H + lane];
+  }
+  r0 = W + MIMG_W3 + lane * MIMG_W2S;
+#pragma unroll
+  for (int kk = 0; kk < MLP_H / 2; kk++) {
+    const uint32_t p0 = r0[kk];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const float hl = __shfl_sync(0xffffffffu, kk < 16 ? h1a[b] : h1b[b], (2 * kk) & 31);
+      const float hh = __shfl_sync(0xffffffffu, kk < 16 ? h1a[b] : h1b[b], (2 * kk + 1) & 31);
+      a0[b] = acc2(a0[b], p0, hl, hh);
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    const double z = (double)a0[b];
+    const bool vl = (valid[b] >> lane) & 1u;
+    double zmax = vl ? z : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, zmax, o);
+      zmax = other > zmax ? other : zmax;
+    }
+    if (!valid[b]) zmax = 0.0;
+    const double e = vl ? fbm::fb_exp(z - zmax) : 0.0;
+    double sum = 0.0;
+#pragma unroll
+    for (int v = 0; v < MLP_OUT; v++) sum = sum + __shfl_sync(0xffffffffu, e, v);
+    q[b] = sum > 0.0 ? e / sum : 0.0;
+  }
+}
+
+// probability that the mixture proposes valid predictor v: mix * q_v + (1 - mix) / p
+__device__ __forceinline__ double mix_prob(double mix, double qv, int p) {
+  return mix * qv + (1.0 - mix) * (1.0 / (double)p);
+}
+
+// The learned model's part of every proposal of sweep it, at sweep start (trees j = crank, crank + CS, ... of the
+// chain are this CTA's share; a warp takes every (CS * warps)-th of them, MP_NB at a time): the same node choice as
+// propose() makes from the trees at sweep start, then for a birth the model's variable (with probability mix from
+// the masked softmax, else uniformly, as BART) and the proposal-ratio correction (1/p) / (mix q_v + (1 - mix)/p); for
+// a death the correction of the reverse birth, the model evaluated at the collapsed node with the node's own split
+// left out of the use counts.  Results go to B.mvar / B.mcorr, which propose() reads after a barrier.
+__device__ __forceinline__ void model_phase(const DBufs& B, const DChain& C, const DTree* trees, const long long* s0g,
+                                            const uint32_t* W, int it, int crank, int CS) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
+  const int step = CS * NW;
+  for (int j0 = crank + CS * warp; j0 < C.m; j0 += MP_NB * step) {   // warp-uniform loop
+    float x0[MP_NB], x1[MP_NB], xa[MP_NB], xb[MP_NB], xc[MP_NB];
+    unsigned valid[MP_NB];
+    int kind[MP_NB], vdeath[MP_NB];
+    double uvb[MP_NB];
+#pragma unroll
+    for (int b = 0; b < MP_NB; b++) {
+      const int j = j0 + b * step;
+      x0[b] = x1[b] = xa[b] = xb[b] = xc[b] = 0.0f;
+      valid[b] = 0u; kind[b] = 0; vdeath[b] = 0; uvb[b] = 0.0;
+      if (j >= C.m) continue;
+      const uint4 q = wt::load(trees + j, lane);
+      const int* cnt = reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES);
+      const unsigned long long used = wt::mask(q, wt::USED), leafm = wt::mask(q, wt::LEAF);
+      unsigned long long goodm = 0, nogm = 0;
+      for (unsigned long long um = used; um; um &= um - 1ull) {
+        const int s = __ffsll((long long)um) - 1;
+        if ((leafm >> s) & 1ull) {
+          int g = wt::byte(q, wt::NGV, s);
+          if (g == 255) {
+            const int nc = lane < C.p ? C.numcut[lane] : 0;
+            int L, U;
+            wt::node_range(q, s, lane, nc, L, U);
+            g = __popc(__ballot_sync(0xffffffffu, lane < C.p && U >= L));
+          }
+          if (g > 0) goodm |= 1ull << s;
+        } else if (((leafm >> wt::byte(q, wt::L, s)) & 1ull) && ((leafm >> wt::byte(q, wt::R, s)) & 1ull)) {
+          nogm |= 1ull << s;
+        }
+      }
+      const int ngood = __popcll(goodm), nnogs = __popcll(nogm);
+      const double PBx = ngood == 0 ? 0 : (used == 1ull ? 1 : 0.5);
+      const fbm::U4 xr = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP, C.seed);
+      const double ub = fbm::u32d(xr.x), un = fbm::u32d(xr.y);
+      uvb[b] = fbm::u32d(xr.z);
+      if (ub < PBx) {
+        const int nx = select_kth(goodm, (int)(un * ngood));
+        kind[b] = 1;
+        valid[b] = node_features_wt(q, nx, cnt[nx], -1, C, lane, x0[b], x1[b], xa[b], xb[b], xc[b]);
+      } else if (nnogs > 0) {
+        const int nx = select_kth(nogm, (int)(un * nnogs));
+        kind[b] = 2;
+        vdeath[b] = wt::byte(q, wt::V, nx);
+        const int lr = cnt[wt::byte(q, wt::L, nx)] + cnt[wt::byte(q, wt::R, nx)];
+        valid[b] = node_features_wt(q, nx, lr, nx, C, lane, x0[b], x1[b], xa[b], xb[b], xc[b]);
+      }
+    }
+    double qb[MP_NB];
+    model_q_batch<MP_NB>(W, x0, x1, xa, xb, xc, valid, lane, qb);
+#pragma unroll
+    for (int b = 0; b < MP_NB; b++) {
+      const int j = j0 + b * step;
+      if (j >= C.m) continue;
+      int v = 0;
+      double corr = 1.0;
+      if (kind[b] == 1) {
+        const fbm::U4 y2 = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP2, C.seed);
+        const double umix = fbm::u32d(y2.x), uvm = fbm::u32d(y2.y);
+        if (umix < B.mix && valid[b]) {   // the first valid k whose cumulative q exceeds uvm, else the last valid
+          double cum = 0.0;
+          int last = 0;
+          v = -1;
+#pragma unroll
+          for (int k = 0; k < MLP_OUT; k++) {
+            const double qk = __shfl_sync(0xffffffffu, qb[b], k);
+            if ((valid[b] >> k) & 1u) { cum = cum + qk; last = k; if (v < 0 && uvm < cum) v = k; }
+          }
+          if (v < 0) v = last;
+        } else {
+          v = (int)(uvb[b] * C.p); if (v >= C.p) v = C.p - 1;
+        }
+        const double qv = __shfl_sync(0xffffffffu, qb[b], v);
+        corr = ((valid[b] >> v) & 1u) ? (1.0 / (double)C.p) / mix_prob(B.mix, qv, C.p) : 1.0;
+      } else if (kind[b] == 2) {
+        const double qv = __shfl_sync(0xffffffffu, qb[b], vdeath[b]);
+        corr = mix_prob(B.mix, qv, C.p) * (double)C.p;
+      }
+      if (lane == 0) { B.mvar[C.off_tree + j] = v; B.mcorr[C.off_tree + j] = corr; }
     }
   }
 }
 
-__device__ __noinline__ void model_probs(const DBufs& B, const float* x, unsigned valid, double* q) {
-  float h1[MLP_H], h2[MLP_H], z[MLP_OUT];
-  for (int h = 0; h < MLP_H; h += 4) {
-    float a[4];
-    dense4<MLP_IN>(B.mw1, B.mb1, x, h, a);
-#pragma unroll
-    for (int u = 0; u < 4; u++) h1[h + u] = a[u] > 0.0f ? a[u] : 0.0f;
-  }
-  for (int h = 0; h < MLP_H; h += 4) {
-    float a[4];
-    dense4<MLP_H>(B.mw2, B.mb2, h1, h, a);
-#pragma unroll
-    for (int u = 0; u < 4; u++) h2[h + u] = a[u] > 0.0f ? a[u] : 0.0f;
-  }
-  for (int o = 0; o < MLP_OUT; o += 4) {
-    float a[4];
-    dense4<MLP_H>(B.mw3, B.mb3, h2, o, a);
-#pragma unroll
-    for (int u = 0; u < 4; u++) z[o + u] = a[u];
-  }
-  double zmax = 0.0;
-  bool any = false;
-  for (int v = 0; v < MLP_OUT; v++)
-    if ((valid >> v) & 1u) { if (!any || (double)z[v] > zmax) zmax = (double)z[v]; any = true; }
-  double S = 0.0;
-  for (int v = 0; v < MLP_OUT; v++) {
-    q[v] = ((valid >> v) & 1u) ? fbm::fb_exp((double)z[v] - zmax) : 0.0;
-    S = S + q[v];
-  }
-  for (int v = 0; v < MLP_OUT; v++) q[v] = S > 0.0 ? q[v] / S : 0.0;
-}
-
-// probability that the mixture proposes valid predictor v: mix * q[v] + (1 - mix) / p
-__device__ __forceinline__ double mix_prob(double mix, const double* q, int v, int p) {
-  return mix * q[v] + (1.0 - mix) * (1.0 / (double)p);
-}
-
 // Proposal of tree j at sweep it (src/bart_kernel.cpp:413-464); also resolves unknown goodvar counts of leaves.
-// With a learned model (B.mw1), the birth variable comes from the model's masked softmax with probability B.mix
-// (else uniformly, as BART), and pr carries the proposal-probability correction of the birth, or of the reverse birth
-// of a death, so the chain keeps BART's target.  cnt: the tree's per-slot row counts.  When training examples are
-// collected, the birth node's features go to feat / *fvalid.
-// Birth variable from the learned model's mixture (see propose); *corr receives the proposal-ratio correction of the
-// drawn variable, feat / *fvalid the node's features when they are collected.
-__device__ __noinline__ int model_birth_var(const DTree* t, int nx, int cnt_nx, const DChain& C, const DBufs& B, int j,
-                                            int it, double uv, double* corr, float* feat, unsigned* fvalid) {
-  float xf[MLP_IN];
-  double q[MLP_OUT];
-  const unsigned valid = node_features(t, nx, cnt_nx, -1, C, xf);
-  model_probs(B, xf, valid, q);
-  const fbm::U4 y2 = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP2, C.seed);
-  const double umix = fbm::u32d(y2.x), uvm = fbm::u32d(y2.y);
-  int v;
-  if (umix < B.mix && valid) {
-    double cum = 0.0;
-    int last = 0;
-    v = -1;
-    for (int k = 0; k < MLP_OUT; k++)
-      if ((valid >> k) & 1u) { cum = cum + q[k]; last = k; if (v < 0 && uvm < cum) v = k; }
-    if (v < 0) v = last;
-  } else {
-    v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
-  }
-  *corr = ((valid >> v) & 1u) ? (1.0 / (double)C.p) / mix_prob(B.mix, q, v, C.p) : 1.0;
-  if (feat) { for (int k = 0; k < MLP_IN; k++) feat[k] = xf[k]; *fvalid = valid; }
-  return v;
-}
-
-// Proposal-ratio correction of a death of nx: the model's probability of the reverse birth (nx's split, in the tree
-// without it) over BART's.
-__device__ __noinline__ double model_death_corr(const DTree* t, int nx, int cnt_lr, const DChain& C, const DBufs& B) {
-  float xf[MLP_IN];
-  double q[MLP_OUT];
-  const unsigned valid = node_features(t, nx, cnt_lr, nx, C, xf);
-  model_probs(B, xf, valid, q);
-  return mix_prob(B.mix, q, (int)t->v[nx], C.p) * (double)C.p;
-}
-
-template <bool LP>
+// With a learned model (B.mvar), the birth variable and the proposal-probability correction of the birth, or of the
+// reverse birth of a death, come from model_phase, and pr carries the correction, so the chain keeps BART's target.
+// cnt: the tree's per-slot row counts.  When training examples are collected, the birth node's features go to
+// feat / *fvalid.
+template <bool LP, bool MP>
 __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cnt, int j, int it, Masks& mk,
                         float* feat, unsigned* fvalid) {
   const double pb = 0.5;
@@ -459,7 +603,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
   const double PBx = ngood == 0 ? 0 : (single ? 1 : pb);
   const fbm::U4 x = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP, C.seed);
   const double ub = fbm::u32d(x.x), un = fbm::u32d(x.y), uv = fbm::u32d(x.z), uc = fbm::u32d(x.w);
-  const bool model = LP && B.mw1 != nullptr && B.mix > 0.0;
+  const bool model = MP && B.mvar != nullptr;
   Prop P;
   P.mode = 0; P.nx = 0; P.v = 0; P.c = 0; P.l = 0; P.r = 0; P.pad0 = P.pad1 = 0; P.logpr = 0; P.lu = 0;
   double pr = 0;
@@ -467,18 +611,10 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
     const int nx = select_kth(goodm, (int)(un * ngood));
     int v;
     double corr = 1.0;
+    if (model) { v = B.mvar[C.off_tree + j]; corr = B.mcorr[C.off_tree + j]; }
+    else { v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1; }
     if constexpr (LP) {
-      if (model) {
-        v = model_birth_var(t, nx, cnt[nx], C, B, j, it, uv, &corr, feat, fvalid);
-      } else {
-        v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
-        if (feat) *fvalid = node_features(t, nx, cnt[nx], -1, C, feat);
-      }
-    } else if (B.mvar) {   // the learned model's choice, computed for this sweep by model_pass_kernel
-      v = B.mvar[C.off_tree + j];
-      corr = B.mcorr[C.off_tree + j];
-    } else {
-      v = (int)(uv * C.p); if (v >= C.p) v = C.p - 1;
+      if (feat) *fvalid = node_features(t, nx, cnt[nx], -1, C, feat);
     }
     int bL, bU;
     node_range(t, nx, v, C.numcut[v], bL, bU);
@@ -499,7 +635,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
       }
       const double Pbotx = (double)1 / ngood;
       pr = (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
-      if (model || (!LP && B.mvar)) pr = pr * corr;
+      if (model) pr = pr * corr;
       P.mode = 1; P.nx = (uint8_t)nx; P.v = (uint8_t)v; P.c = (uint8_t)c;
     }
   } else if (nnogs > 0) {
@@ -511,11 +647,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
     const int ng2 = ngood - (t->ngv[l] > 0) - (t->ngv[r] > 0) + 1;
     const double Pboty = (double)1 / ng2, PDx = 1 - PBx, Pnogx = (double)1 / nnogs;
     pr = ((1 - PGny) * PBy * Pboty) / (PGny * (1 - PGlx) * (1 - PGrx) * PDx * Pnogx);
-    if constexpr (LP) {
-      if (model) pr = pr * model_death_corr(t, nx, cnt[l] + cnt[r], C, B);   // the reverse birth
-    } else {
-      if (B.mvar) pr = pr * B.mcorr[C.off_tree + j];
-    }
+    if (model) pr = pr * B.mcorr[C.off_tree + j];   // the reverse birth
     P.mode = 2; P.nx = (uint8_t)nx; P.l = (uint8_t)l; P.r = (uint8_t)r;
   }
   if (P.mode) {
@@ -534,65 +666,6 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
   }
   P.cand = cand;
   return P;
-}
-
-// Learned-proposal pre-pass of sweep it, launched before the sweep's sampler launch: for every tree of every chain
-// (one CTA per chain, one thread per tree), the same node choice as propose() makes, then the model's birth variable
-// and proposal-ratio correction, or a death's reverse-birth correction, into B.mvar / B.mcorr.  Keeping the model
-// out of the sampler kernel keeps its calls from costing the sampler registers.  Reads the trees as the previous
-// launch left them (the first CTA's copy in cluster mode: every copy is identical between sweeps), or root-only
-// trees for sweep 0.
-__global__ void __launch_bounds__(256) model_pass_kernel(DBufs B, int it) {
-  const DChain& C = B.chains[blockIdx.x];
-  const int CS = B.cluster > 1 ? B.cluster : 1;
-  const DTree* trees = B.trees + C.off_tree * CS;
-  const long long* s0g = B.s0 + C.off_tree * CS * LST;
-  // sweep 0 starts from root-only trees, which the sampler launch itself initialises: stand in for them here
-  DTree root;
-  int root_cnt[NODES];
-  if (it == 0) {
-    uint8_t* rb = reinterpret_cast<uint8_t*>(&root);
-    for (int k = 0; k < (int)sizeof(DTree); k++) rb[k] = 0;
-    root.ngv[0] = (uint8_t)C.root_ngv;
-    root.used = 1ull; root.leaf = 1ull;
-    for (int k = 0; k < NODES; k++) root_cnt[k] = 0;
-    root_cnt[0] = C.n;
-  }
-  for (int j = threadIdx.x; j < C.m; j += blockDim.x) {
-    const DTree* t = it == 0 ? &root : trees + j;
-    const int* cnt = it == 0 ? root_cnt : reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES);
-    const unsigned long long used = t->used, leafm = t->leaf;
-    unsigned long long goodm = 0, nogm = 0;
-    for (unsigned long long um = used; um; um &= um - 1ull) {
-      const int s = __ffsll((long long)um) - 1;
-      if ((leafm >> s) & 1ull) {
-        const int g = t->ngv[s] == 255 ? count_goodvars(t, s, C.numcut, C.p) : t->ngv[s];
-        if (g > 0) goodm |= 1ull << s;
-      } else if (((leafm >> t->l[s]) & 1ull) && ((leafm >> t->r[s]) & 1ull)) {
-        nogm |= 1ull << s;
-      }
-    }
-    const int ngood = __popcll(goodm), nnogs = __popcll(nogm);
-    const double PBx = ngood == 0 ? 0 : (used == 1ull ? 1 : 0.5);
-    const fbm::U4 x = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP, C.seed);
-    const double ub = fbm::u32d(x.x), un = fbm::u32d(x.y), uv = fbm::u32d(x.z);
-    int v = 0;
-    double corr = 1.0;
-    if (ub < PBx) {
-      const int nx = select_kth(goodm, (int)(un * ngood));
-      v = model_birth_var(t, nx, cnt[nx], C, B, j, it, uv, &corr, nullptr, nullptr);
-    } else if (nnogs > 0) {
-      const int nx = select_kth(nogm, (int)(un * nnogs));
-      corr = model_death_corr(t, nx, cnt[t->l[nx]] + cnt[t->r[nx]], C, B);
-    }
-    const_cast<int*>(B.mvar)[C.off_tree + j] = v;
-    const_cast<double*>(B.mcorr)[C.off_tree + j] = corr;
-  }
-}
-
-int launch_model_pass(const DBufs& b, int it, void* stream) {
-  model_pass_kernel<<<b.nchains, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(b, it);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 // ------------------------------------------------------------------------------------------------ shared layout
@@ -617,6 +690,7 @@ struct Smem {
   long long* xch;               // [2][4] per-CTA values exchanged across the cluster (rss, latent-z caps, sum w)
   long long* xtot;              // [2][cluster][TOT] every CTA's pass totals, pushed by their owners
   unsigned long long* xovb;     // [2][cluster][64]
+  uint32_t* mimg;               // [MIMG_WORDS] the proposal model's weight image, behind the layout (B.model_smem)
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -676,6 +750,8 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.xch = reinterpret_cast<long long*>(base + off[18]);
   S.xtot = reinterpret_cast<long long*>(base + off[19]);
   S.xovb = reinterpret_cast<unsigned long long*>(base + off[20]);
+  S.mimg = reinterpret_cast<uint32_t*>(base + align_up(smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off),
+                                                       16));
   return S;
 }
 
@@ -764,14 +840,14 @@ __device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTre
 namespace cg = cooperative_groups;
 
 // Proposals of every tree of sweep it (one thread per tree) with the leaf-mu normals drawn ahead.
-template <bool LP>
+template <bool LP, bool MP>
 __device__ __forceinline__ void proposals_body(const Smem& S, const DBufs& B, const DChain& C, DTree* trees,
                                                const long long* s0g, int it, bool lead) {
   const int m = C.m;
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
     Masks mk;
     float* featj = (LP && B.train_cap > 0 && lead) ? B.feat + (C.off_tree + j) * MLP_IN : nullptr;
-    const Prop P = propose<LP>(trees + j, C, B, reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES), j, it,
+    const Prop P = propose<LP, MP>(trees + j, C, B, reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES), j, it,
                                mk, featj, B.feat_valid + (C.off_tree + j));
     S.prop[j] = P;
     S.masks[j] = mk;
@@ -782,11 +858,11 @@ __device__ __forceinline__ void proposals_body(const Smem& S, const DBufs& B, co
     }
   }
 }
-// Out of line for the learned-proposal kernels: the model's calls then save only this function's few live
-// registers, not the chain loop's.
-__device__ __noinline__ void proposals_model(const Smem& S, const DBufs& B, const DChain& C, DTree* trees,
+// Out of line for the collecting kernels: the feature calls then save only this function's few live registers, not
+// the chain loop's.
+__device__ __noinline__ void proposals_collect(const Smem& S, const DBufs& B, const DChain& C, DTree* trees,
                                              const long long* s0g, int it, bool lead) {
-  proposals_body<true>(S, B, C, trees, s0g, it, lead);
+  proposals_body<true, true>(S, B, C, trees, s0g, it, lead);
 }
 
 // Cluster exchange of the pass totals (buffer cur), push style: every CTA stores its totals into slot [crank] of every
@@ -829,8 +905,9 @@ __device__ __forceinline__ long long cluster_value(const Smem& S, int k, int CS)
 // Metropolis-Hastings, leaf draws and sigma come out bit-identical in every CTA, each on its own copy of the trees);
 // only the exact integer pass totals and the end-of-sweep rss cross the cluster, through distributed shared memory,
 // once per tree step.  Integer sums do not depend on order, so the results equal the one-CTA run bit for bit.
-template <int G, bool CL, bool LP>
+template <int G, bool CL, int MODE>
 __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& S) {
+  constexpr bool LP = MODE == MODE_COLLECT, MP = MODE != MODE_PLAIN;
   const DChain& C = B.chains[ci];
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const int RT = T - 32;
@@ -931,9 +1008,29 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
 
   for (int it = it0; it < it1; it++) {
     const double inv_s2 = 1.0 / (ctl.sigma * ctl.sigma);
+    // ---------------------------------------------------------------- learned model, one warp per tree
+    if (MP && B.mvar) {
+      // the weights in shared memory: in the pass bins, free at sweep start when they are large enough (the leaf
+      // rows, which the pass accumulates into, are zeroed again afterwards), else behind the layout, else global
+      const bool in_bins = bins_hold_model(T);
+      const uint32_t* W = B.model_smem ? S.mimg : B.mimg;
+      if (in_bins) {
+        for (int k = tid; k < MIMG_WORDS / 4; k += T)
+          reinterpret_cast<uint4*>(S.bins)[k] = __ldg(reinterpret_cast<const uint4*>(B.mimg) + k);
+        __syncthreads();
+        W = reinterpret_cast<const uint32_t*>(S.bins);
+      }
+      model_phase(B, C, trees, s0g, W, it, crank, CS);
+      if (in_bins) {
+        __syncthreads();
+        for (int k = tid; k < NBS * RT; k += T) S.bins[k] = 0;
+      }
+      if constexpr (CL) { __threadfence(); cg::this_cluster().sync(); }   // every CTA's share, in global memory
+      else __syncthreads();
+    }
     // ---------------------------------------------------------------- proposals, one thread per tree
-    if constexpr (LP) proposals_model(S, B, C, trees, s0g, it, lead);
-    else proposals_body<false>(S, B, C, trees, s0g, it, lead);
+    if constexpr (LP) proposals_collect(S, B, C, trees, s0g, it, lead);
+    else proposals_body<false, MP>(S, B, C, trees, s0g, it, lead);
     for (int k = tid; k < 2 * TOT; k += T) S.tot[k] = 0;
     for (int k = tid; k < 2 * NODES; k += T) S.ovb[k] = 0ull;
     __syncthreads();
@@ -1252,15 +1349,23 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   if (CL) cg::this_cluster().sync();   // no CTA reuses or leaves its shared memory while others read it
 }
 
-// G: groups of 4 rows held in registers per row thread (0: streamed); CL: a cluster of CTAs per chain; LP: learned
-// proposal or training-example collection compiled in (kept out of the plain kernels, where its calls would spill).
-template <int G, bool CL, bool LP>
+// G: groups of 4 rows held in registers per row thread (0: streamed); CL: a cluster of CTAs per chain; MODE: plain,
+// with the learned proposal's model phase, or with training-example collection (and the model phase).  Each feature
+// lives in its own variant: compiled into the plain kernels, its code would cost them registers.
+template <int G, bool CL, int MODE>
 __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it0, int it1) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem, B.cluster);
+  if constexpr (MODE != MODE_PLAIN) {   // the proposal model's weights, once per launch
+    if (B.mvar && B.model_smem && !bins_hold_model(blockDim.x)) {
+      for (int k = threadIdx.x; k < MIMG_WORDS / 4; k += blockDim.x)
+        reinterpret_cast<uint4*>(S.mimg)[k] = __ldg(reinterpret_cast<const uint4*>(B.mimg) + k);
+      __syncthreads();
+    }
+  }
   if constexpr (CL) {   // one chain per cluster at a time, in the host's order; every CTA of a cluster agrees
     const int ncl = gridDim.x / B.cluster, cid = blockIdx.x / B.cluster;
-    for (int qi = cid; qi < B.nchains; qi += ncl) run_chain<G, CL, LP>(B, B.order[qi], it0, it1, S);
+    for (int qi = cid; qi < B.nchains; qi += ncl) run_chain<G, CL, MODE>(B, B.order[qi], it0, it1, S);
   } else {
     for (;;) {
       if (threadIdx.x == 0) S.ctl->chain = atomicAdd(B.queue, 1);
@@ -1268,25 +1373,28 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it
       const int qi = S.ctl->chain;
       __syncthreads();
       if (qi >= B.nchains) break;
-      run_chain<G, CL, LP>(B, B.order[qi], it0, it1, S);
+      run_chain<G, CL, MODE>(B, B.order[qi], it0, it1, S);
     }
   }
 }
 
 using KernelFn = void (*)(DBufs, int, int);
-template <bool CL, bool LP>
+template <bool CL, int MODE>
 static KernelFn kernel_g(int gmax) {
   switch (gmax) {
-    case 1: return sampler_kernel<1, CL, LP>;
-    case 2: return sampler_kernel<2, CL, LP>;
-    case 4: return sampler_kernel<4, CL, LP>;
-    case 8: return sampler_kernel<8, CL, LP>;
-    default: return sampler_kernel<0, CL, LP>;
+    case 1: return sampler_kernel<1, CL, MODE>;
+    case 2: return sampler_kernel<2, CL, MODE>;
+    case 4: return sampler_kernel<4, CL, MODE>;
+    case 8: return sampler_kernel<8, CL, MODE>;
+    default: return sampler_kernel<0, CL, MODE>;
   }
 }
-static KernelFn kernel_for(int gmax, bool cluster, bool lp) {
-  if (cluster) return lp ? kernel_g<true, true>(gmax) : kernel_g<true, false>(gmax);
-  return lp ? kernel_g<false, true>(gmax) : kernel_g<false, false>(gmax);
+static KernelFn kernel_for(int gmax, bool cluster, int mode) {
+  if (cluster)
+    return mode == MODE_COLLECT ? kernel_g<true, MODE_COLLECT>(gmax)
+         : mode == MODE_MODEL ? kernel_g<true, MODE_MODEL>(gmax) : kernel_g<true, MODE_PLAIN>(gmax);
+  return mode == MODE_COLLECT ? kernel_g<false, MODE_COLLECT>(gmax)
+       : mode == MODE_MODEL ? kernel_g<false, MODE_MODEL>(gmax) : kernel_g<false, MODE_PLAIN>(gmax);
 }
 
 int sampler_gmax(int threads, int n_pad_max) {
@@ -1295,14 +1403,16 @@ int sampler_gmax(int threads, int n_pad_max) {
   return g <= 1 ? 1 : g <= 2 ? 2 : g <= 4 ? 4 : g <= 8 ? 8 : 0;
 }
 
+bool sampler_bins_hold_model(int threads) { return bins_hold_model(threads); }
+
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster) {
   size_t off[NOFF];
   return smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off);
 }
 
 int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster) {
-  // the learned-proposal kernels need the same shared memory; residency is the same for both
-  const KernelFn k = kernel_for(gmax, cluster > 1, true);
+  // every variant needs the same shared memory; residency is the same for all
+  const KernelFn k = kernel_for(gmax, cluster > 1, MODE_COLLECT);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
@@ -1328,8 +1438,8 @@ int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
                    void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const bool lp = (b.mw1 != nullptr && b.mix > 0.0) || b.train_cap > 0;
-  const KernelFn k = kernel_for(gmax, cluster > 1, lp);
+  const int mode = b.train_cap > 0 ? MODE_COLLECT : b.mvar ? MODE_MODEL : MODE_PLAIN;
+  const KernelFn k = kernel_for(gmax, cluster > 1, mode);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
   if (cudaMemsetAsync(b.queue, 0, sizeof(int), s) != cudaSuccess) return -1;
   if (cluster <= 1) {

@@ -24,8 +24,8 @@ def random_model(seed, scale=0.3, mix=0.5):
                 w3=_bf16(rng.normal(0, scale, (32, 64))), b3=rng.normal(0, 0.5, 32).astype(np.float32), mix=mix)
 
 
-def _run(ch, nskip, ndpost, model=None, collect=0, cluster=0):
-    b = F.Batch([ch], nskip, ndpost, cluster=cluster)
+def _run(ch, nskip, ndpost, model=None, collect=0, cluster=0, threads=0):
+    b = F.Batch([ch], nskip, ndpost, cluster=cluster, threads=threads)
     if model is not None:
         b.set_proposal(model)
     if collect:
@@ -49,16 +49,28 @@ def test_collected_examples_bit_exact(orc, cluster):
     assert np.array_equal(x.view(np.uint32), ref["train_x"].view(np.uint32))
 
 
-@pytest.mark.parametrize("mix,cluster", [(0.5, 1), (1.0, 1), (0.5, 2)])
-def test_model_chain_bit_exact(orc, mix, cluster):
+# threads 512: the weights staged in the pass bins; 256: behind the shared layout; cluster 2: split over two CTAs
+@pytest.mark.parametrize("mix,cluster,threads", [(0.5, 1, 0), (1.0, 1, 0), (0.5, 2, 0), (0.5, 1, 256)])
+def test_model_chain_bit_exact(orc, mix, cluster, threads):
     ch = W.fwbart_friedman(n=400, p=12, seed=8, ntree=20, nskip=30, ndpost=10)
     model = random_model(3, mix=mix)
-    out, _ = _run(ch, 30, 10, model=model, cluster=cluster)
+    out, _ = _run(ch, 30, 10, model=model, cluster=cluster, threads=threads)
     ref = orc.fit(ch, orc.MODE_DEV, model=model)
     for k, r in (("sigma", "sigma"), ("yhat_mean", "fmean"), ("trees", "trees"), ("moves", "moves")):
         assert np.array_equal(np.asarray(out[k]), np.asarray(ref[r])), k
     plain = orc.fit(ch, orc.MODE_DEV)
     assert not np.array_equal(plain["trees"], ref["trees"])   # the model does change the proposals
+
+
+def test_model_chain_collecting_examples_bit_exact(orc):
+    # a learned chain that also collects its accepted births (the collecting kernel variant runs the model too)
+    ch = W.fwbart_friedman(n=400, p=12, seed=9, ntree=20, nskip=30, ndpost=10)
+    model = random_model(5, mix=0.5)
+    out, (x, y, m, cnt) = _run(ch, 30, 10, model=model, collect=20000)
+    ref = orc.fit(ch, orc.MODE_DEV, model=model, train_cap=20000)
+    assert np.array_equal(out["sigma"], ref["sigma"]) and np.array_equal(out["trees"], ref["trees"])
+    assert cnt == len(ref["train_y"]) and np.array_equal(y, ref["train_y"]) and np.array_equal(m, ref["train_mask"])
+    assert np.array_equal(x.view(np.uint32), ref["train_x"].view(np.uint32))
 
 
 def test_training_gradients_match_oracle(orc):
