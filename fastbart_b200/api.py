@@ -16,7 +16,8 @@ from scipy import stats
 from . import _lib, prep, workloads
 from ._lib import NODES, FastbartError, check, ptr
 
-__all__ = ["fwbart", "fpbart", "compile_trees", "predict_draw", "fit_batch", "Batch", "trees_text", "varcount",
+__all__ = ["fwbart", "fpbart", "compile_trees", "predict_draw", "fit_batch", "Batch", "trees_text", "trees_text_gpu",
+           "varcount",
            "FastbartError"]
 
 
@@ -120,6 +121,14 @@ class Batch:
         oarr = (_lib.ChainOut * len(outs))(*[s for _, s in outs])
         check(_lib.lib().fb_batch_download(self._h, oarr))
         return [_collect(o, oarr[k]) for k, (o, _) in enumerate(outs)]
+
+    def trees_text(self, chain: int) -> str:
+        """BART tree text of one chain's kept draws, assembled on the device from its trees there."""
+        L, ln = _lib.lib(), C.c_size_t()
+        check(L.fb_batch_trees_text(self._h, chain, None, 0, C.byref(ln)))
+        buf = C.create_string_buffer(ln.value + 1)
+        check(L.fb_batch_trees_text(self._h, chain, buf, ln.value + 1, C.byref(ln)))
+        return buf.raw[:ln.value].decode()
 
     def set_proposal(self, model: dict | None):
         """Learned split-variable proposal for the next runs (see `train_proposal`); None restores BART's."""
@@ -236,6 +245,17 @@ def trees_text(trees: np.ndarray, p: int) -> str:
     return buf.raw[:ln].decode()
 
 
+def trees_text_gpu(trees: np.ndarray, p: int, device: int = 0) -> str:
+    """`trees_text` assembled on the device (the same bytes), for host arrays of packed draws."""
+    t = np.ascontiguousarray(trees, dtype=np.uint64)
+    nd, m = t.shape[0], t.shape[1]
+    L, ln = _lib.lib(), C.c_size_t()
+    check(L.fb_trees_text_gpu(ptr(t), nd, m, p, device, None, 0, C.byref(ln)))
+    buf = C.create_string_buffer(ln.value + 1)
+    check(L.fb_trees_text_gpu(ptr(t), nd, m, p, device, buf, ln.value + 1, C.byref(ln)))
+    return buf.raw[:ln.value].decode()
+
+
 def varcount(trees: np.ndarray, p: int) -> np.ndarray:
     t = np.ascontiguousarray(trees, dtype=np.uint64)
     out = np.zeros((t.shape[0], p), dtype=np.int32)
@@ -281,7 +301,7 @@ def fwbart(x_train, y_train, x_test=None, sparse=False, xinfo=None, usequants=Fa
     return BartFit("wbart", sigma=o["sigma"], **{"yhat.train.mean": o["yhat_mean"] + fm,
                                                 "yhat.train": o["yhat"] + fm},
                    varcount=varcount(o["trees"], p), varprob=np.full((ndpost, p), 1.0 / p),
-                   treedraws=dict(cutpoints=xi, trees=trees_text(o["trees"], p)), mu=fm, moves=o["moves"],
+                   treedraws=dict(cutpoints=xi, trees=trees_text_gpu(o["trees"], p, device)), mu=fm, moves=o["moves"],
                    **{"rm.const": d.rm_const, "varcount.mean": varcount(o["trees"], p).mean(axis=0),
                       "varprob.mean": np.full(p, 1.0 / p)}, colnames=names)
 
@@ -308,7 +328,8 @@ def fpbart(x_train, y_train, x_test=None, sparse=False, xinfo=None, usequants=Fa
     vc = varcount(o["trees"], p)
     return BartFit("pbart", **{"yhat.train": yh, "prob.train": prob, "prob.train.mean": prob.mean(axis=0)},
                    varcount=vc, varprob=np.full((ndpost, p), 1.0 / p),
-                   treedraws=dict(cutpoints={nm: d.xi[v] for v, nm in enumerate(names)}, trees=trees_text(o["trees"], p)),
+                   treedraws=dict(cutpoints={nm: d.xi[v] for v, nm in enumerate(names)},
+                                  trees=trees_text_gpu(o["trees"], p, device)),
                    binaryOffset=off, moves=o["moves"],
                    **{"rm.const": d.rm_const, "varcount.mean": vc.mean(axis=0), "varprob.mean": np.full(p, 1.0 / p)},
                    colnames=names)

@@ -93,6 +93,10 @@ struct DBufs {
 };
 
 size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster);
+// Tree text (without its header) of ntrees consecutive device trees: *total receives its length; with d_out
+// non-null, *d_out is allocated (cudaMalloc, caller frees) and receives the text.  0 on success.
+int trees_text_device(const uint64_t* d_trees, long long ntrees, char** d_out, unsigned long long* total,
+                      void* stream);
 // whether the sampler stages the proposal model's weights in its pass bins (no extra shared memory needed)
 bool sampler_bins_hold_model(int threads);
 // groups of 4 rows per row thread held in registers (1, 2, 4, 8), or 0 when the rows stream from L2 in the pass

@@ -512,6 +512,58 @@ size_t fb_trees_text(const uint64_t* trees, int ndpost, int ntree, int p, char* 
   return s.size();
 }
 
+}  // extern "C"
+
+// Header plus the device-assembled text of ndpost x ntree device trees into buf (the fb_trees_text contract).
+static fb_status text_from_device(const uint64_t* d_trees, int ndpost, int ntree, int p, char* buf, size_t cap,
+                                  size_t* len) {
+  char head[64];
+  const int hl = std::snprintf(head, sizeof head, "%d %d %d\n", ndpost, ntree, p);
+  unsigned long long body = 0;
+  char* d_text = nullptr;
+  const bool want = buf && cap > 0;
+  if (trees_text_device(d_trees, (long long)ndpost * ntree, want ? &d_text : nullptr, &body, nullptr) != 0)
+    return fail(FB_ERR_CUDA, "tree text kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
+  const size_t total = (size_t)hl + (size_t)body;
+  if (len) *len = total;
+  if (!want) return FB_OK;
+  const size_t c = std::min(cap - 1, total);
+  std::memcpy(buf, head, std::min(c, (size_t)hl));
+  fb_status st = FB_OK;
+  if (c > (size_t)hl && cudaMemcpy(buf + hl, d_text, c - (size_t)hl, cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = fail(FB_ERR_CUDA, "cannot copy the tree text");
+  buf[c] = 0;
+  cudaFree(d_text);
+  return st;
+}
+
+extern "C" {
+
+fb_status fb_trees_text_gpu(const uint64_t* trees, int ndpost, int ntree, int p, int device, char* buf, size_t cap,
+                            size_t* len) {
+  if (!trees || ndpost < 0 || ntree < 0) return fail(FB_ERR_ARG, "trees, ndpost >= 0 and ntree >= 0 are required");
+  CK(cudaSetDevice(device));
+  const size_t words = (size_t)ndpost * ntree * NODES;
+  uint64_t* d = nullptr;
+  if (cudaMalloc(&d, sizeof(uint64_t) * (words > 0 ? words : 1)) != cudaSuccess) return fail(FB_ERR_CUDA, "out of device memory");
+  fb_status st = FB_OK;
+  if (words > 0 && cudaMemcpy(d, trees, sizeof(uint64_t) * words, cudaMemcpyHostToDevice) != cudaSuccess)
+    st = fail(FB_ERR_CUDA, "cannot copy the trees to the device");
+  if (st == FB_OK) st = text_from_device(d, ndpost, ntree, p, buf, cap, len);
+  cudaFree(d);
+  return st;
+}
+
+fb_status fb_batch_trees_text(fb_batch* b, int chain, char* buf, size_t cap, size_t* len) {
+  if (!b) return fail(FB_ERR_ARG, "batch is NULL");
+  if (chain < 0 || chain >= b->nchains) return fail(FB_ERR_RANGE, "chain %d is outside 0..%d", chain, b->nchains - 1);
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const DChain& D = b->hch[chain];
+  return text_from_device(reinterpret_cast<const uint64_t*>(b->d.trees_out + D.off_tout), b->ndpost, D.m, D.p, buf,
+                          cap, len);
+}
+
 fb_status fb_varcount(const uint64_t* trees, int ndpost, int ntree, int p, int* varcount) {
   if (!trees || !varcount) return fail(FB_ERR_ARG, "trees and varcount are required");
   std::memset(varcount, 0, sizeof(int) * (size_t)ndpost * p);
@@ -556,7 +608,15 @@ fb_status fb_fbart(const int* q, int n, int p, const double* y, const double* wt
   fb_chain_out out;
   std::memset(&out, 0, sizeof out);
   out.sigma = sigma; out.yhat_mean = yhat_train_mean; out.yhat = yh.data(); out.trees = tr.data();
-  fb_status s = fb_fit_batch(&c, 1, &o, &out);
+  fb_batch* b = nullptr;
+  fb_status s = fb_batch_create(&c, 1, &o, &b);
+  if (s != FB_OK) return s;
+  s = fb_batch_run(b, nullptr);
+  if (s == FB_OK) s = fb_batch_sync(b);
+  if (s == FB_OK) s = fb_batch_download(b, &out);
+  size_t len = 0;
+  if (s == FB_OK) s = fb_batch_trees_text(b, 0, trees_text, text_cap, &len);   // assembled on the device
+  fb_batch_destroy(b);
   if (s != FB_OK) return s;
   if (yhat_train)
     for (int dr = 0; dr < ndpost; dr++)
@@ -567,7 +627,6 @@ fb_status fb_fbart(const int* q, int n, int p, const double* y, const double* wt
     for (int dr = 0; dr < ndpost; dr++)
       for (int v = 0; v < p; v++) varcount[(size_t)dr + (size_t)v * ndpost] = vc[(size_t)dr * p + v];
   }
-  const size_t len = fb_trees_text(tr.data(), ndpost, ntree, p, trees_text, text_cap);
   if (text_len) *text_len = len;
   if (moves) { moves[0] = out.moves[0]; moves[1] = out.moves[1]; moves[2] = out.moves[2]; }
   return FB_OK;

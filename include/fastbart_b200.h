@@ -165,6 +165,14 @@ fb_status fb_fbart(const int* q, int n, int p, const double* y, const double* wt
  * count and pre-order "id v c theta" lines (root id 1, children 2id / 2id+1, 10 significant digits).  Writes at most
  * cap bytes (NUL-terminated when cap > 0) and returns the full length. */
 size_t fb_trees_text(const uint64_t* trees, int ndpost, int ntree, int p, char* buf, size_t cap);
+/* The same text assembled on the device (one thread per tree), byte for byte what fb_trees_text writes: trees are
+ * host arrays copied to `device`.  *len receives the full length; buf (cap bytes, NUL-terminated when cap > 0) may be
+ * NULL to size it.  Replaces the host loop of src/glue.cpp:29-57 (F1: device-side output assembly). */
+fb_status fb_trees_text_gpu(const uint64_t* trees, int ndpost, int ntree, int p, int device, char* buf, size_t cap,
+                            size_t* len);
+/* Tree text of chain `chain` of a batch from its kept draws in device memory (after fb_batch_sync), as
+ * fb_trees_text would write it from the downloaded trees; only the text crosses to the host. */
+fb_status fb_batch_trees_text(fb_batch* b, int chain, char* buf, size_t cap, size_t* len);
 /* varcount[dr][v] = number of internal nodes splitting on v in draw dr (src/glue.cpp:49). */
 fb_status fb_varcount(const uint64_t* trees, int ndpost, int ntree, int p, int* varcount);
 
