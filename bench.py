@@ -9,8 +9,9 @@ from the initial state, producing all outputs (sigma draws, yhat.train draws, po
   python bench.py [--gpus N --steps K --warmup W]          this implementation (one rank per GPU under torchrun)
   python bench.py --impl reference [--steps K --warmup W]   the reference sampler (bart_fit_cpu, built from source
                                                             into oracle/_ref) on the host cores, one chain per core
-  --workload sparse | predict | learned                     the other measured configurations: 16 chains of n 65,536
-                                                            on clusters; bulk predict_draw; learned vs plain proposal
+  --workload sparse | predict | learned | text              the other measured configurations: 16 chains of n 65,536
+                                                            on clusters; bulk predict_draw; learned vs plain proposal;
+                                                            tree text of the fitted 96-chain batch
 
 Timing: W untimed warm-up steps; K timed steps, each preceded (outside its event pair) by a write of 512 MiB to flush
 L2; CUDA events on the launching stream; max over ranks.  Multi-GPU: every rank runs its own 96-chain batch (different
@@ -545,6 +546,60 @@ def bench_predict(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------ tree text
+TXT_METRIC = "BART tree text of the 96 fitted titer chains, assembled on the device and delivered as host strings"
+
+
+def bench_text(args):
+    """The output-assembly step after a fit: BART tree text (src/glue.cpp:29-57 format) of every chain of the fitted
+    96-chain titer batch (100 draws x 200 trees each), assembled on the device from the kept trees there
+    (fb_batch_trees_text) and returned as host strings.  The fit itself is not timed.  Baseline: the host C++ writer
+    (fb_trees_text, snprintf) on downloaded trees, one thread, on a sample of 8 chains."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+    import fastbart_b200 as F
+    from fastbart_b200 import workloads as W
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    chains = W.titer_bootstrap(reps=16, seed=0, nskip=NSKIP, ndpost=NDPOST, ntree=NTREE)
+    b = F.Batch(chains, NSKIP, NDPOST)
+    b.run()
+    b.sync()
+
+    def step():
+        return [b.trees_text(k) for k in range(len(chains))]
+    for _ in range(args.warmup):
+        texts = step()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        texts = step()
+    sec = (time.perf_counter() - t) / args.steps
+    clk = clocks.stop()
+    mb = sum(len(x) for x in texts) / 1e6
+    outs = b.download()
+    cpu = None
+    if not args.no_cpu_baseline:
+        t = time.perf_counter()
+        host = [F.trees_text(o["trees"], c["q"].shape[0]) for o, c in zip(outs[:8], chains[:8])]
+        hs = time.perf_counter() - t
+        assert host == texts[:8], "device and host tree text differ"
+        cpu = {"value": sum(len(x) for x in host) / 1e6 / hs, "unit": "MB/s", "cores": 1, "kind": "port",
+               "sample": "host C++ writer (snprintf) on the downloaded trees of the first 8 chains"}
+    b.close()
+    line = {"metric": TXT_METRIC, "value": mb / sec, "unit": "MB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * sec, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 trees -> text", "data": "synthetic",
+            "config": {"workload": "tree_text_titer96", "chains": len(chains), "ndpost": NDPOST, "ntree": NTREE,
+                       "text_mb": mb},
+            "e2e": {"value": mb / sec, "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(mb * 1e6),
+                    "note": "the timed step is already end to end: device trees in, host strings out"},
+            "gpu_launches": 7 * len(chains) * args.steps, "roofline": None, "cpu_baseline": cpu, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------------------------------------ learned proposal
 LRN_N, LRN_P, LRN_CHAINS, LRN_TRAIN = 65_536, 32, 16, 200_000
 LRN_METRIC = "ESS/s of sigma and f, learned vs plain proposal (16 fwbart chains, n 65,536, p 32, 27 noise predictors)"
@@ -639,7 +694,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="titer96", choices=["titer96", "small", "sparse", "predict", "learned"])
+    ap.add_argument("--workload", default="titer96",
+                    choices=["titer96", "small", "sparse", "predict", "learned", "text"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -647,6 +703,8 @@ def main():
         return bench_predict(args)
     if args.workload == "learned":
         return bench_learned(args)
+    if args.workload == "text":
+        return bench_text(args)
     set_workload(args.workload)
     if args.impl == "reference":
         return bench_reference(args)
