@@ -99,7 +99,7 @@ int trees_text_device(const uint64_t* d_trees, long long ntrees, char** d_out, u
                       void* stream);
 // whether the sampler stages the proposal model's weights in its pass bins (no extra shared memory needed)
 bool sampler_bins_hold_model(int threads);
-// groups of 4 rows per row thread held in registers (1, 2, 4, 8), or 0 when the rows stream from L2 in the pass
+// groups of 4 rows per row thread held in registers (1, 2, 3, 4, 6, 8), or 0 when the rows stream from L2 in the pass
 int sampler_gmax(int threads, int n_pad_max);
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
                    void* stream);

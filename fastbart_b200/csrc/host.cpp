@@ -183,12 +183,13 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt->device) != cudaSuccess) optin = 232448;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
   // CTAs per chain: a cluster splits each chain's rows over CS SMs when SMs would otherwise idle (or as requested)
-  // Automatic choice (measured on B200): the largest cluster of 4..8 CTAs whose clusters are all resident at once,
-  // one per chain, when there are SMs to spare and at least 512 rows per CTA; otherwise one CTA per chain.
+  // Automatic choice (measured on B200): the largest cluster of 4..16 CTAs whose clusters are all resident at once,
+  // one per chain, when there are SMs to spare and at least 512 rows per CTA; otherwise one CTA per chain.  (Sizes
+  // above 8 are non-portable; B200 keeps up to 15 clusters of 7..9 CTAs, 7 of 12..16, resident.)
   std::vector<int> tries;
-  if (opt->cluster > 0) tries.push_back(std::min(opt->cluster, 8));
+  if (opt->cluster > 0) tries.push_back(std::min(opt->cluster, 16));
   else {
-    for (int c = 8; c >= 4; c--)
+    for (int c = 16; c >= 4; c--)
       if ((long long)nchains * c <= nsm && n_pad_max / c >= 512) tries.push_back(c);
   }
   tries.push_back(1);
@@ -289,7 +290,7 @@ fb_status fb_autotune(const fb_chain* chains, int nchains, const fb_options* opt
   CK(cudaSetDevice(opt->device));
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
   std::vector<int> clusters{1};
-  for (int c = 2; c <= 8; c++)
+  for (int c = 2; c <= 16; c++)
     if ((long long)nchains * c <= nsm) clusters.push_back(c);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));

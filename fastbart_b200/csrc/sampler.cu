@@ -1384,7 +1384,9 @@ static KernelFn kernel_g(int gmax) {
   switch (gmax) {
     case 1: return sampler_kernel<1, CL, MODE>;
     case 2: return sampler_kernel<2, CL, MODE>;
+    case 3: return sampler_kernel<3, CL, MODE>;
     case 4: return sampler_kernel<4, CL, MODE>;
+    case 6: return sampler_kernel<6, CL, MODE>;
     case 8: return sampler_kernel<8, CL, MODE>;
     default: return sampler_kernel<0, CL, MODE>;
   }
@@ -1400,7 +1402,7 @@ static KernelFn kernel_for(int gmax, bool cluster, int mode) {
 int sampler_gmax(int threads, int n_pad_max) {
   const int RT = threads - 32;
   const int g = (n_pad_max / 4 + RT - 1) / RT;
-  return g <= 1 ? 1 : g <= 2 ? 2 : g <= 4 ? 4 : g <= 8 ? 8 : 0;
+  return g <= 1 ? 1 : g <= 2 ? 2 : g <= 3 ? 3 : g <= 4 ? 4 : g <= 6 ? 6 : g <= 8 ? 8 : 0;
 }
 
 bool sampler_bins_hold_model(int threads) { return bins_hold_model(threads); }
@@ -1414,6 +1416,11 @@ int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster
   // every variant needs the same shared memory; residency is the same for all
   const KernelFn k = kernel_for(gmax, cluster > 1, MODE_COLLECT);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  // clusters of 9..16 CTAs are beyond the portable size: allowed per kernel
+  if (cluster > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
   if (cluster <= 1) {
@@ -1441,6 +1448,8 @@ int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size
   const int mode = b.train_cap > 0 ? MODE_COLLECT : b.mvar ? MODE_MODEL : MODE_PLAIN;
   const KernelFn k = kernel_for(gmax, cluster > 1, mode);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+  if (cluster > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return -1;
   if (cudaMemsetAsync(b.queue, 0, sizeof(int), s) != cudaSuccess) return -1;
   if (cluster <= 1) {
     k<<<grid, threads, smem, s>>>(b, it0, it1);

@@ -67,7 +67,8 @@ typedef struct fb_options {
   int sweeps_per_launch;    /* 0 = the whole MCMC in one launch; k > 0 = launches of k sweeps */
   int device;               /* CUDA device ordinal */
   int cluster;              /* CTAs per chain (a thread-block cluster sharing the rows): 0 = automatic, 1 = one CTA,
-                               2..8 = that many when they can be resident; results are identical for every value */
+                               2..16 = that many when they can be resident (above 8: non-portable cluster sizes);
+                               results are identical for every value */
 } fb_options;
 
 /* Caller-owned host outputs of one chain; a NULL pointer skips that copy. */
@@ -98,7 +99,7 @@ fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, i
                                int* cluster);
 void fb_batch_destroy(fb_batch* b);
 /* Autotuner of the launch shape: runs trial_sweeps sweeps of the given chains for every candidate shape (threads per
- * CTA 256, 384, 512 x CTAs per chain 1..8 whose clusters are all resident at once), timed with CUDA events, and writes
+ * CTA 256, 384, 512 x CTAs per chain 1..16 whose clusters are all resident at once), timed with CUDA events, and writes
  * to *best a copy of *opt with the fastest threads and cluster (and its trial time to *best_ms when non-NULL).
  * No counterpart in the reference, whose GPU prototype takes the block size on its command line
  * (gpu/bart_batch.cu:302-308). */
