@@ -20,7 +20,8 @@ EXPORTS = ["fb_last_error", "fb_version", "fb_fit_batch", "fb_batch_create", "fb
            "fb_varcount", "fb_compile_trees", "fb_compiled_info", "fb_compiled_arrays", "fb_compiled_free",
            "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass",
            "fb_batch_set_proposal", "fb_batch_collect", "fb_batch_training_data", "fb_train_proposal",
-           "fb_mlp_loss_grad", "fb_autotune", "fb_cut_codes", "fb_trees_text_gpu", "fb_batch_trees_text"]
+           "fb_mlp_loss_grad", "fb_autotune", "fb_cut_codes", "fb_trees_text_gpu", "fb_batch_trees_text",
+           "fb_release_cached_memory"]
 
 MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
 
@@ -103,6 +104,7 @@ def lib() -> C.CDLL:
         L.fb_varcount.argtypes = [vp, i, i, i, vp]
         L.fb_trees_text_gpu.argtypes = [vp, i, i, i, i, C.c_char_p, sz, C.POINTER(sz)]
         L.fb_batch_trees_text.argtypes = [vp, i, C.c_char_p, sz, C.POINTER(sz)]
+        L.fb_release_cached_memory.argtypes = [i]
         L.fb_compile_trees.argtypes = [C.c_char_p, sz, vp, vp, i, i, C.POINTER(vp)]
         L.fb_compiled_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.fb_compiled_arrays.argtypes = [vp, vp, vp, vp, vp, vp]

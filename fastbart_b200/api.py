@@ -17,7 +17,7 @@ from . import _lib, prep, workloads
 from ._lib import NODES, FastbartError, check, ptr
 
 __all__ = ["fwbart", "fpbart", "compile_trees", "predict_draw", "fit_batch", "Batch", "trees_text", "trees_text_gpu",
-           "varcount",
+           "varcount", "release_cached_memory",
            "FastbartError"]
 
 
@@ -243,6 +243,11 @@ def trees_text(trees: np.ndarray, p: int) -> str:
     buf = C.create_string_buffer(ln + 1)
     L.fb_trees_text(ptr(t), nd, m, p, buf, ln + 1)
     return buf.raw[:ln].decode()
+
+
+def release_cached_memory(device: int = 0):
+    """Returns the device memory kept by finished batches (for the next batch) to the driver."""
+    check(_lib.lib().fb_release_cached_memory(device))
 
 
 def trees_text_gpu(trees: np.ndarray, p: int, device: int = 0) -> str:

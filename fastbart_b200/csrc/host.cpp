@@ -7,8 +7,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -78,12 +80,43 @@ fb_status check_chain(const fb_chain& c, int k) {
   return FB_OK;
 }
 
-template <class T>
-fb_status dalloc(T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) count = 1;
-  CK(cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T)));
-  return FB_OK;
+// Device memory of batches comes from one pool per device that keeps what is freed (release threshold unlimited):
+// a fit's arrays (1.5 GB for 96 titer chains) are then reused by the next fit instead of being unmapped by cudaFree
+// and mapped again, which took 0.5-0.7 s per fit.  fb_release_cached_memory() returns the cache to the device.
+std::mutex g_pool_mu;
+std::unordered_map<int, cudaMemPool_t> g_pools;
+
+cudaMemPool_t batch_pool(int device) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(device);
+  if (it != g_pools.end()) return it->second;
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof props);
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  g_pools[device] = pool;
+  return pool;
+}
+
+// bytes from the batch pool, ordered on the legacy stream (the caller synchronises it before other streams use them);
+// when the device is full, the pool's cache is trimmed and the allocation tried once more
+void* pool_alloc(size_t bytes, int device) {
+  cudaMemPool_t pool = batch_pool(device);
+  if (!pool) return nullptr;
+  void* p = nullptr;
+  if (bytes == 0) bytes = 1;
+  if (cudaMallocFromPoolAsync(&p, bytes, pool, 0) == cudaSuccess) return p;
+  cudaGetLastError();
+  cudaStreamSynchronize(0);
+  cudaMemPoolTrimTo(pool, 0);
+  if (cudaMallocFromPoolAsync(&p, bytes, pool, 0) == cudaSuccess) return p;
+  cudaGetLastError();
+  return nullptr;
 }
 
 }  // namespace
@@ -105,11 +138,20 @@ struct fb_batch {
   int cluster = 1;             // CTAs per chain
   int slice_rows = 0;          // rows of one CTA's slice (shared-memory capacity)
   int collect_cap = 0;         // allocated capacity of the training-example buffers
+  // n elements of T from the batch pool, owned by the batch; null when the device is full
+  template <class T>
+  T* alloc(size_t n) {
+    void* p = pool_alloc(n * sizeof(T), device);
+    if (p) allocs.push_back(p);
+    return static_cast<T*>(p);
+  }
   ~fb_batch() {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(device);
-    for (void* p : allocs) cudaFree(p);
+    cudaDeviceSynchronize();   // runs may be in flight on a caller's stream (cudaFree used to wait for them too)
+    for (void* p : allocs) cudaFreeAsync(p, 0);
+    cudaStreamSynchronize(0);
     cudaSetDevice(cur);
   }
 };
@@ -216,9 +258,9 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   // device arrays
   DBufs& d = b->d;
   auto A = [&](auto** p, size_t cnt) -> fb_status {
-    fb_status s = dalloc(p, cnt);
-    if (s == FB_OK) b->allocs.push_back((void*)*p);
-    return s;
+    using T = std::remove_pointer_t<std::remove_pointer_t<decltype(p)>>;
+    *p = b->alloc<T>(cnt);
+    return *p ? FB_OK : fail(FB_ERR_CUDA, "out of device memory (%zu elements)", cnt);
   };
   DChain* dch; DState* dst; uint8_t* dq; double* dyin; double* dyw; float* dw; int8_t* dyb; float* drs; float* dws;
   uint8_t* dleaf;
@@ -233,6 +275,7 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
     delete b;
     return s;
   }
+  CK(cudaStreamSynchronize(0));   // the pool allocations are complete before any stream of the caller uses them
   // inputs, padded rows are zero
   std::vector<uint8_t> hq((size_t)b->qbytes, 0);
   std::vector<double> hy((size_t)b->rows, 0.0);
@@ -344,17 +387,13 @@ fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
   std::memcpy(img.data() + MIMG_B, model->b1, 4 * MLP_H);
   std::memcpy(img.data() + MIMG_B + MLP_H, model->b2, 4 * MLP_H);
   std::memcpy(img.data() + MIMG_B + 2 * MLP_H, model->b3, 4 * MLP_OUT);
-  if (!b->model_mem) {
-    if (cudaMalloc(&b->model_mem, 4 * img.size()) != cudaSuccess) return fail(FB_ERR_CUDA, "out of device memory");
-    b->allocs.push_back(b->model_mem);
-  }
+  if (!b->model_mem && !(b->model_mem = b->alloc<uint32_t>(img.size()))) return fail(FB_ERR_CUDA, "out of device memory");
   if (!b->mvar) {
-    if (cudaMalloc(&b->mvar, sizeof(int) * (size_t)b->ntrees) != cudaSuccess) return fail(FB_ERR_CUDA, "out of device memory");
-    b->allocs.push_back(b->mvar);
-    if (cudaMalloc(&b->mcorr, sizeof(double) * (size_t)b->ntrees) != cudaSuccess)
-      return fail(FB_ERR_CUDA, "out of device memory");
-    b->allocs.push_back(b->mcorr);
+    b->mvar = b->alloc<int>((size_t)b->ntrees);
+    b->mcorr = b->alloc<double>((size_t)b->ntrees);
+    if (!b->mvar || !b->mcorr) { b->mvar = nullptr; return fail(FB_ERR_CUDA, "out of device memory"); }
   }
+  CK(cudaStreamSynchronize(0));
   CK(cudaMemcpy(b->model_mem, img.data(), 4 * img.size(), cudaMemcpyHostToDevice));
   b->d.mimg = static_cast<const uint32_t*>(b->model_mem);
   // the sampler stages the image in its pass bins when they are large enough (wide CTAs); otherwise behind its
@@ -375,16 +414,14 @@ fb_status fb_batch_collect(fb_batch* b, int capacity) {
   if (capacity < 0) return fail(FB_ERR_ARG, "capacity must be >= 0");
   CK(cudaSetDevice(b->device));
   if (capacity > b->collect_cap) {
-    void *feat = nullptr, *fv = nullptr, *tx = nullptr, *ty = nullptr, *tm = nullptr, *tc = nullptr;
-    if (cudaMalloc(&feat, sizeof(float) * MLP_IN * (size_t)b->ntrees) != cudaSuccess ||
-        cudaMalloc(&fv, sizeof(unsigned) * (size_t)b->ntrees) != cudaSuccess ||
-        cudaMalloc(&tx, sizeof(float) * MLP_IN * (size_t)capacity) != cudaSuccess ||
-        cudaMalloc(&ty, sizeof(int) * (size_t)capacity) != cudaSuccess ||
-        cudaMalloc(&tm, sizeof(unsigned) * (size_t)capacity) != cudaSuccess || cudaMalloc(&tc, sizeof(int)) != cudaSuccess) {
-      cudaFree(feat); cudaFree(fv); cudaFree(tx); cudaFree(ty); cudaFree(tm); cudaFree(tc);
-      return fail(FB_ERR_CUDA, "out of device memory");
-    }
-    for (void* q : {feat, fv, tx, ty, tm, tc}) b->allocs.push_back(q);
+    float* feat = b->alloc<float>((size_t)MLP_IN * b->ntrees);
+    unsigned* fv = b->alloc<unsigned>((size_t)b->ntrees);
+    float* tx = b->alloc<float>((size_t)MLP_IN * capacity);
+    int* ty = b->alloc<int>((size_t)capacity);
+    unsigned* tm = b->alloc<unsigned>((size_t)capacity);
+    int* tc = b->alloc<int>(1);
+    if (!feat || !fv || !tx || !ty || !tm || !tc) return fail(FB_ERR_CUDA, "out of device memory");
+    CK(cudaStreamSynchronize(0));
     b->d.feat = static_cast<float*>(feat); b->d.feat_valid = static_cast<unsigned*>(fv);
     b->d.train_x = static_cast<float*>(tx); b->d.train_y = static_cast<int*>(ty);
     b->d.train_mask = static_cast<unsigned*>(tm); b->d.train_count = static_cast<int*>(tc);
@@ -459,6 +496,20 @@ fb_status fb_batch_download(fb_batch* b, fb_chain_out* outs) {
 }
 
 void fb_batch_destroy(fb_batch* b) { delete b; }
+
+fb_status fb_release_cached_memory(int device) {
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pools.find(device);
+    if (it == g_pools.end()) return FB_OK;
+    pool = it->second;
+  }
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(0));
+  CK(cudaMemPoolTrimTo(pool, 0));
+  return FB_OK;
+}
 
 fb_status fb_fit_batch(const fb_chain* chains, int nchains, const fb_options* opt, fb_chain_out* outs) {
   fb_batch* b = nullptr;

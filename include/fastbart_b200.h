@@ -93,6 +93,9 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
 fb_status fb_batch_run(fb_batch* b, void* cuda_stream);        /* enqueues on cuda_stream (NULL: default stream) */
 fb_status fb_batch_sync(fb_batch* b);
 fb_status fb_batch_download(fb_batch* b, fb_chain_out* outs);
+/* Batches take device memory from a per-device pool that keeps freed blocks for the next batch (no unmapping and
+ * remapping between fits); this returns the kept blocks of `device` to the driver.  No counterpart in the reference. */
+fb_status fb_release_cached_memory(int device);
 /* number of sampler kernel launches per fb_batch_run, the dynamic shared memory / threads / grid of each, and the
  * CTAs per chain (thread-block cluster size; 1 without clusters).  Outputs may be NULL. */
 fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes,
