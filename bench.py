@@ -9,9 +9,10 @@ from the initial state, producing all outputs (sigma draws, yhat.train draws, po
   python bench.py [--gpus N --steps K --warmup W]          this implementation (one rank per GPU under torchrun)
   python bench.py --impl reference [--steps K --warmup W]   the reference sampler (bart_fit_cpu, built from source
                                                             into oracle/_ref) on the host cores, one chain per core
-  --workload sparse | predict | learned | text              the other measured configurations: 16 chains of n 65,536
-                                                            on clusters; bulk predict_draw; learned vs plain proposal;
-                                                            tree text of the fitted 96-chain batch
+  --workload sparse | probit | predict | learned | text     the other measured configurations: 16 chains of n 65,536
+                                                            on clusters; one fpbart chain (n 24,576, p 3) and the
+                                                            predict_draw of its draws; bulk predict_draw; learned vs
+                                                            plain proposal; tree text of the fitted 96-chain batch
 
 Timing: W untimed warm-up steps; K timed steps, each preceded (outside its event pair) by a write of 512 MiB to flush
 L2; CUDA events on the launching stream; max over ranks.  Multi-GPU: every rank runs its own 96-chain batch (different
@@ -55,7 +56,16 @@ def set_workload(name: str):
     """'titer96' (the benchmark), 'small' (6 chains, one per shape, 40 sweeps: the profiling case) or 'sparse'
     (16 chains, n 65,536, p 32, numcut 255, Friedman-5 signal on 5 of 32 predictors: the large-n configuration, run
     on thread-block clusters; the automatic choice is 6 CTAs per chain)."""
-    global NSKIP, NDPOST, WORKLOAD_NAME, workload, METRIC, FULL_REF, N_RANGE, P_RANGE
+    global NSKIP, NDPOST, NTREE, WORKLOAD_NAME, workload, METRIC, FULL_REF, N_RANGE, P_RANGE
+    if name == "probit":
+        NTREE = 50
+        WORKLOAD_NAME, FULL_REF, N_RANGE, P_RANGE = "fpbart_hazard_24576", False, [24576, 24576], [3, 3]
+        METRIC = "chain-sweeps/s (fpbart, n 24,576 person-weeks, p 3, ntree 50; then predict_draw of its 100 draws)"
+
+        def probit(rank: int = 0, reps: int = 0, nskip=None, ndpost=None):
+            from fastbart_b200 import workloads as W
+            return [W.fpbart_hazard(n=24576, seed=rank, ntree=NTREE, nskip=NSKIP, ndpost=NDPOST)]
+        workload = probit
     if name == "sparse":
         WORKLOAD_NAME, FULL_REF, N_RANGE, P_RANGE = "friedman_sparse_16x65536", False, [65536, 65536], [32, 32]
         METRIC = "chain-sweeps/s (16 fwbart chains, n 65,536, p 32)"
@@ -74,6 +84,33 @@ def set_workload(name: str):
         def small(rank: int = 0, reps: int = 1, nskip=None, ndpost=None):
             return base(rank, 1, NSKIP, NDPOST)
         workload = small
+
+
+def predict_fresh_rows(F, ch, out, stream, device):
+    """The probit configuration's second half: compile_trees of the fit's 100 kept draws, then predict_draw of every
+    draw on a fresh 24,576-row table from the same distribution (FP64), timed with CUDA events on the device
+    (fb_predict_draws_device, x and results resident), after one untimed call."""
+    import torch
+    from fastbart_b200 import workloads as W
+    x, _ = W.hazard_data(24576, 999)
+    ct = F.CompiledTrees(F.trees_text_gpu(out["trees"], x.shape[1], device), ch["xi"], mu=ch["offset"], device=device)
+    n, p = x.shape
+    xd = torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda")
+    od = torch.empty((NDPOST, n), dtype=torch.float64, device="cuda")
+    F.predict_draws_device(ct, xd.data_ptr(), p, n, n, 1, NDPOST, od.data_ptr(), n, stream.cuda_stream)
+    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    a.record(stream)
+    for _ in range(reps):
+        F.predict_draws_device(ct, xd.data_ptr(), p, n, n, 1, NDPOST, od.data_ptr(), n, stream.cuda_stream)
+    c.record(stream)
+    torch.cuda.synchronize()
+    sec = a.elapsed_time(c) / 1000.0 / reps
+    chk = F.predict_draw(ct, x, NDPOST)   # the single-draw entry point agrees with the bulk one
+    assert np.array_equal(chk, od[NDPOST - 1].cpu().numpy()), "bulk and single-draw predict disagree"
+    return {"row_draws_per_s": NDPOST * n / sec, "ms_per_call": 1000 * sec, "draws": NDPOST, "rows": n,
+            "ntree": ch["ntree"], "hbm_gbs": (n * p * 8 + NDPOST * n * 8) / sec / 1e9,
+            "note": "all 100 draws on fresh rows in one fb_predict_draws_device call; x read once, results written once"}
 
 
 # ------------------------------------------------------------------------------------------------ CPU reference
@@ -239,7 +276,9 @@ def bench_ours(args):
         pool.map(_warm_worker, range(ncores), chunksize=1)
         v, kind, wall = run_cpu_sample(pool, chains, ncores, sweeps)
         cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": kind,
-               "sample": f"{ncores} of the {len(chains)} chains, one per core, {sweeps} sweeps each ({wall:.1f} s wall)"}
+               "sample": (f"{ncores} of the {len(chains)} chains" if len(chains) >= ncores else
+                          f"{ncores} copies of the workload's {len(chains)} chain(s)")
+               + f", one per core, {sweeps} sweeps each ({wall:.1f} s wall)"}
         if FULL_REF:
             full_ref = pool.apply_async(_full_ref_chain, (chains[0],))   # agreement check of chain 0, full length
 
@@ -299,6 +338,11 @@ def bench_ours(args):
     per_step_s = tot_ms / 1000.0 / args.steps
     ess_line = {"sigma_per_s": sum(ess_s) * world / per_step_s, "f_median_per_s": sum(ess_f) * world / per_step_s,
                 "sigma_mean_ess": float(np.mean(ess_s)), "f_median_ess": float(np.mean(ess_f)), "kept": NDPOST}
+    if WORKLOAD_NAME.startswith("fpbart"):   # probit: sigma is fixed at 1
+        ess_line["sigma_per_s"] = ess_line["sigma_mean_ess"] = None
+    predict = None
+    if WORKLOAD_NAME.startswith("fpbart"):
+        predict = predict_fresh_rows(F, chains[0], outs[0], stream, local)
     b.close()
 
     # roofline of the sampler kernel (one launch per step)
@@ -340,7 +384,7 @@ def bench_ours(args):
         opt = _lib.Options(NSKIP, NDPOST, args.threads, 0, local, args.cluster)
         h2d = sum(np.asarray(c["q"]).nbytes + 8 * len(c["y"]) + 4 * len(c["y"]) + len(c["y"]) for c in chains)
         h2d += len(chains) * 1024
-        d2h = sum(8 * S + 8 * len(c["y"]) * (1 + NDPOST) + 8 * NDPOST * NTREE * 64 for c in chains)
+        d2h = sum(8 * S + 8 * len(c["y"]) * (1 + NDPOST) + 8 * NDPOST * c["ntree"] * 64 for c in chains)
         times = []
         for k in range(args.e2e_steps + 1):
             torch.cuda.synchronize()
@@ -374,6 +418,8 @@ def bench_ours(args):
                            "shape": "autotuned" if tuned else "rules"},
                 "e2e": e2e, "gpu_launches": args.steps * info["launches"], "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "ess_per_s": ess_line, "r_f_vs_reference_chain0": r_f, "wall_s": wall}
+        if predict is not None:
+            line["predict_draw"] = predict
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -708,7 +754,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="titer96",
-                    choices=["titer96", "small", "sparse", "predict", "learned", "text"])
+                    choices=["titer96", "small", "sparse", "probit", "predict", "learned", "text"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
