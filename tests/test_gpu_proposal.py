@@ -130,3 +130,24 @@ def test_learned_chain_targets_the_same_posterior(orc):
     mp, ml = np.mean(fp, axis=0), np.mean(fl, axis=0)
     assert np.corrcoef(mp, ml)[0, 1] > 0.995
     assert abs(np.mean(sl) / np.mean(sp) - 1) < 0.02
+
+
+@pytest.mark.parametrize("cluster", [1, 3])
+def test_mixed_batch_with_model_bit_exact(orc, cluster):
+    """The mixed configuration at test size: fwbart and fpbart chains of uneven n, p and ntree in one launch, all with
+    the learned proposal; every chain equals its own oracle run bit for bit."""
+    chains = [W.fwbart_friedman(n=900, p=8, seed=61, ntree=25, nskip=15, ndpost=6),
+              W.fpbart_hazard(n=1500, seed=62, ntree=10, nskip=15, ndpost=6),
+              W.fwbart_friedman(n=2300, p=14, seed=63, ntree=18, nskip=15, ndpost=6),
+              W.fpbart_hazard(n=700, seed=64, ntree=7, nskip=15, ndpost=6)]
+    model = random_model(21, mix=0.7)
+    b = F.Batch(chains, 15, 6, cluster=cluster)
+    b.set_proposal(model)
+    b.run()
+    b.sync()
+    outs = b.download()
+    b.close()
+    for ch, o in zip(chains, outs):
+        ref = orc.fit(ch, orc.MODE_DEV, model=model)
+        for k, r in (("sigma", "sigma"), ("yhat_mean", "fmean"), ("trees", "trees"), ("moves", "moves")):
+            assert np.array_equal(np.asarray(o[k]), np.asarray(ref[r])), k
