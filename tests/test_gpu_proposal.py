@@ -151,3 +151,20 @@ def test_mixed_batch_with_model_bit_exact(orc, cluster):
         ref = orc.fit(ch, orc.MODE_DEV, model=model)
         for k, r in (("sigma", "sigma"), ("yhat_mean", "fmean"), ("trees", "trees"), ("moves", "moves")):
             assert np.array_equal(np.asarray(o[k]), np.asarray(ref[r])), k
+
+
+def test_clearing_the_model_restores_bart_proposals(orc):
+    # one batch: a learned run, then the model cleared (the plain kernel variant again), then the model set again
+    ch = W.fwbart_friedman(n=600, p=10, seed=71, ntree=15, nskip=20, ndpost=5)
+    model = random_model(8, mix=0.6)
+    b = F.Batch([ch], 20, 5)
+    runs = []
+    for mdl in (model, None, model):
+        b.set_proposal(mdl)
+        b.run()
+        b.sync()
+        runs.append(b.download()[0])
+    b.close()
+    learned, plain = orc.fit(ch, orc.MODE_DEV, model=model), orc.fit(ch, orc.MODE_DEV)
+    assert np.array_equal(runs[0]["trees"], learned["trees"]) and np.array_equal(runs[2]["trees"], learned["trees"])
+    assert np.array_equal(runs[1]["trees"], plain["trees"]) and np.array_equal(runs[1]["sigma"], plain["sigma"])
