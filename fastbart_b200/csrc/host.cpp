@@ -103,6 +103,16 @@ cudaMemPool_t batch_pool(int device) {
   return pool;
 }
 
+// Narrowest CTA (whole warps, 256..512 threads) whose row threads hold a slice of `groups` 4-row groups in as few
+// groups each as a 512-thread CTA does: the pass's longest thread is unchanged, while the barriers and the bin
+// reductions span fewer warps.  Measured on B200: the titer chains (1,144 groups) run 3.6% faster on 416 threads.
+int fitted_threads(int groups) {
+  const int g = (groups + 479) / 480;   // groups per row thread at 512 threads
+  if (g > 8) return 512;                 // rows streamed from L2: widest
+  const int rt = ((groups + g - 1) / g + 31) / 32 * 32;
+  return std::max(256, std::min(512, rt + 32));
+}
+
 // bytes from the batch pool, ordered on the legacy stream (the caller synchronises it before other streams use them);
 // when the device is full, the pool's cache is trimmed and the allocation tried once more
 void* pool_alloc(size_t bytes, int device) {
@@ -216,10 +226,12 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
 
   // launch shape
   int T = opt->threads;
+  bool fit_width = false;   // automatic width for one chain (or cluster) per SM: fitted to the slice below
   if (T == 0) {
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt->device);
-    T = nchains <= nsm ? 512 : 256;   // one chain per SM: widest CTA; more chains than SMs: two CTAs per SM
+    T = nchains <= nsm ? 512 : 256;   // one chain per SM: wide CTA; more chains than SMs: two CTAs per SM
+    fit_width = nchains <= nsm;
   }
   int optin = 0, nsm = 148;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt->device) != cudaSuccess) optin = 232448;
@@ -237,9 +249,11 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   tries.push_back(1);
   int CS = 1, rows_in_smem = 1, gmax = 0, maxgrid = 0;
   size_t smem = 0;
+  const int T_req = T;
   for (size_t ti = 0; ti < tries.size(); ti++) {
     CS = tries[ti];
     const int cap = 4 * ((n_pad_max / 4 + CS - 1) / CS);   // rows of one CTA's slice
+    T = fit_width ? fitted_threads(cap / 4) : T_req;
     rows_in_smem = 1;
     smem = sampler_smem_bytes(T, m_max, cap, 1, CS);
     if (smem > (size_t)optin) { rows_in_smem = 0; smem = sampler_smem_bytes(T, m_max, cap, 0, CS); }
@@ -340,7 +354,7 @@ fb_status fb_autotune(const fb_chain* chains, int nchains, const fb_options* opt
   CK(cudaEventCreate(&e1));
   double bestt = 1e300;
   fb_options keep = *opt;
-  for (int T : {256, 384, 512}) {
+  for (int T : {256, 384, 416, 448, 512}) {
     for (int c : clusters) {
       fb_options o = *opt;
       o.nskip = trial_sweeps - 1; o.ndpost = 1; o.threads = T; o.cluster = c; o.sweeps_per_launch = 0;

@@ -171,7 +171,7 @@ def test_statistical_agreement_with_reference(orc):
 def test_autotune_picks_a_shape_with_identical_results():
     chains = [W.fwbart_friedman(n=3000, p=6, seed=51 + k, ntree=20, nskip=8, ndpost=4) for k in range(3)]
     best = F.autotune(chains, 8, 4, trial_sweeps=2)
-    assert best["threads"] in (256, 384, 512) and 1 <= best["cluster"] <= 16 and best["trial_ms"] > 0
+    assert best["threads"] in (256, 384, 416, 448, 512) and 1 <= best["cluster"] <= 16 and best["trial_ms"] > 0
     tuned = fit_batch(chains, 8, 4, threads=best["threads"], cluster=best["cluster"])
     plain = fit_batch(chains, 8, 4, cluster=1)
     for a, b in zip(tuned, plain):
