@@ -102,8 +102,9 @@ fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, i
                                int* cluster);
 void fb_batch_destroy(fb_batch* b);
 /* Autotuner of the launch shape: runs trial_sweeps sweeps of the given chains for every candidate shape (threads per
- * CTA 256, 384, 416, 448, 512 x CTAs per chain 1..16 whose clusters are all resident at once), timed with CUDA events, and writes
- * to *best a copy of *opt with the fastest threads and cluster (and its trial time to *best_ms when non-NULL).
+ * CTA 256, 384, 416, 448, 512 x CTAs per chain 1..16 whose clusters are all resident at once), timed with CUDA
+ * events, and writes to *best a copy of *opt with the fastest threads and cluster (and its trial time to *best_ms
+ * when non-NULL).
  * No counterpart in the reference, whose GPU prototype takes the block size on its command line
  * (gpu/bart_batch.cu:302-308). */
 fb_status fb_autotune(const fb_chain* chains, int nchains, const fb_options* opt, int trial_sweeps, fb_options* best,
