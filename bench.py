@@ -77,6 +77,14 @@ def set_workload(name: str):
                 c["seed"] = 100 + 16 * rank + k
             return out
         workload = sparse
+    if name == "single":
+        WORKLOAD_NAME, FULL_REF, N_RANGE, P_RANGE = "friedman_single_4096x16", True, [4096, 4096], [16, 16]
+        METRIC = "chain-sweeps/s (one fwbart chain, n 4,096, p 16, ntree 200)"
+
+        def single(rank: int = 0, reps: int = 0, nskip=None, ndpost=None):
+            from fastbart_b200 import workloads as W
+            return [W.fwbart_friedman(n=4096, p=16, seed=rank, ntree=NTREE, nskip=NSKIP, ndpost=NDPOST)]
+        workload = single
     if name == "small":
         NSKIP, NDPOST, WORKLOAD_NAME = 30, 10, "titer_small_6x40"
         base = workload
@@ -136,10 +144,10 @@ def _warm_worker(_):
 
 
 def _full_ref_chain(ch):
+    """One full-length chain of the reference sampler: (posterior mean of f, mean sigma over the kept draws)."""
     from oracle import oracle as O
-    if O.ref_available():
-        return O.ref_fit(ch)["fmean"]
-    return O.fit(ch, O.MODE_REF)["fmean"]
+    r = O.ref_fit(ch) if O.ref_available() else O.fit(ch, O.MODE_REF)
+    return r["fmean"], float(np.mean(r["sigma"][int(ch["nskip"]):]))
 
 
 def cpu_sample_plan(ncores: int):
@@ -147,12 +155,95 @@ def cpu_sample_plan(ncores: int):
     return sweeps
 
 
+def stratified(chains, k: int):
+    """The k-th chain of a sample spread over the workload's shapes: chains are grouped by (n, p) in order of first
+    appearance, and the sample takes one chain of each group in turn."""
+    groups: dict = {}
+    for c in chains:
+        groups.setdefault(np.asarray(c["q"]).shape, []).append(c)
+    g = list(groups.values())
+    grp = g[k % len(g)]
+    return grp[(k // len(g)) % len(grp)]
+
+
+def sample_chains(chains, ncores: int) -> list:
+    """ncores chains spread over the workload: one per shape in turn (stratified), or, when there are more shapes than
+    cores, every (shapes / ncores)-th shape."""
+    nshape = len({np.asarray(c["q"]).shape for c in chains})
+    if nshape <= ncores:
+        return [stratified(chains, k) for k in range(ncores)]
+    return [chains[(k * len(chains)) // ncores] for k in range(ncores)]
+
+
 def run_cpu_sample(pool, chains, ncores, sweeps):
-    tasks = [(chains[k % len(chains)], sweeps) for k in range(ncores)]
+    picked = sample_chains(chains, ncores)
+    tasks = [(c, sweeps) for c in picked]
     t = time.perf_counter()
     res = pool.map(_ref_worker, tasks)
     wall = time.perf_counter() - t
     return ncores * sweeps / wall, res[0][1], wall
+
+
+def cpu_sample_text(chains, ncores, sweeps):
+    picked = sample_chains(chains, ncores)
+    shapes = sorted({np.asarray(c["q"]).shape[::-1] for c in picked})
+    mean_n = float(np.mean([np.asarray(c["q"]).shape[1] for c in picked]))
+    listed = f" {[list(x) for x in shapes]} (n, p)" if len(shapes) <= 8 else ""
+    return (f"{ncores} chains (one per core) spread over {len(shapes)} of the workload's shapes{listed}, mean n "
+            f"{mean_n:.0f}, {sweeps} sweeps each")
+
+
+def config_of(chains):
+    """The workload description shared by both arms (launch details of this implementation go to "launch")."""
+    return {"workload": WORKLOAD_NAME, "chains_per_gpu": len(chains), "ntree": NTREE, "nskip": NSKIP,
+            "ndpost": NDPOST, "n_range": N_RANGE, "p_range": P_RANGE,
+            "l2": "inputs resident; the GPU arm flushes L2 (512 MiB write) before every timed step"}
+
+
+def agreement_plan(chains):
+    """One chain of each shape (its first bootstrap resample) for the agreement check against the reference: the
+    batch's own chain and a second seed on the GPU, two seeds of the reference sampler on the CPU."""
+    seen, picks = set(), []
+    for k, c in enumerate(chains):
+        sh = np.asarray(c["q"]).shape
+        if sh not in seen:
+            seen.add(sh)
+            picks.append(k)
+    refs = []
+    for k in picks:
+        for s in (0, 1):
+            d = dict(chains[k])
+            d["seed"] = 700_001 + 2 * k + s
+            d["nskip"], d["ndpost"] = NSKIP, NDPOST
+            refs.append(d)
+    return picks, refs
+
+
+def agreement(picks, gpu_main, gpu_second, ref_results):
+    """Posterior-mean f correlation and sigma ratio against the reference, per shape: single chains (the batch's chain
+    vs one reference seed), the reference's own seed-to-seed correlation, and both seeds pooled on each side."""
+    corr = lambda a, b: float(np.corrcoef(a, b)[0, 1])
+    per = []
+    for i, k in enumerate(picks):
+        (fa, sa), (fb, sb) = ref_results[2 * i], ref_results[2 * i + 1]
+        g1, g2 = gpu_main[k], gpu_second[i]
+        sg = 0.5 * (np.mean(g1["sigma"][NSKIP:]) + np.mean(g2["sigma"][NSKIP:]))
+        per.append({"n": int(len(fa)), "r_f": corr(g1["yhat_mean"], fa), "ref_seed_spread": corr(fa, fb),
+                    "r_f_pooled": corr(g1["yhat_mean"] + g2["yhat_mean"], fa + fb),
+                    "sigma_ratio": float(sg / (0.5 * (sa + sb))), "ref_sigma_seed_ratio": float(max(sa, sb) / min(sa, sb))})
+    col = lambda key: [x[key] for x in per]
+    return {"shapes": len(per), "r_f_min": min(col("r_f")), "r_f_median": float(np.median(col("r_f"))),
+            "ref_seed_spread_min": min(col("ref_seed_spread")),
+            "ref_seed_spread_median": float(np.median(col("ref_seed_spread"))),
+            "r_f_pooled_min": min(col("r_f_pooled")), "r_f_pooled_median": float(np.median(col("r_f_pooled"))),
+            "sigma_ratio_min": min(col("sigma_ratio")), "sigma_ratio_max": max(col("sigma_ratio")),
+            "ref_sigma_seed_ratio_max": max(col("ref_sigma_seed_ratio")),
+            "per_shape": per,
+            "what": "one chain per shape; r_f = corr(posterior-mean f) of this sampler's chain and one reference "
+                    "chain (full length); ref_seed_spread = the same between two reference seeds; pooled = two "
+                    "seeds on each side; sigma_ratio = mean sigma over the kept draws, two seeds each; ref_sigma_seed_ratio = "
+                    "the larger over the smaller mean sigma of the two reference seeds (bootstrap resamples hold "
+                    "duplicated rows, and chains settle at sigma levels a few percent apart)"}
 
 
 # ------------------------------------------------------------------------------------------------ clocks
@@ -244,12 +335,11 @@ def bench_reference(args):
             vals.append(v); walls.append(wall)
     tot = sum(walls)
     value = ncores * sweeps * args.steps / tot
-    sample = f"{ncores} chains of the {len(chains)} (one per core), {sweeps} sweeps each, per step"
+    sample = cpu_sample_text(chains, ncores, sweeps) + ", per step"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "chains": 96, "ntree": NTREE, "nskip": NSKIP,
-                       "ndpost": NDPOST},
+            "config": config_of(chains),
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -276,11 +366,10 @@ def bench_ours(args):
         pool.map(_warm_worker, range(ncores), chunksize=1)
         v, kind, wall = run_cpu_sample(pool, chains, ncores, sweeps)
         cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": kind,
-               "sample": (f"{ncores} of the {len(chains)} chains" if len(chains) >= ncores else
-                          f"{ncores} copies of the workload's {len(chains)} chain(s)")
-               + f", one per core, {sweeps} sweeps each ({wall:.1f} s wall)"}
-        if FULL_REF:
-            full_ref = pool.apply_async(_full_ref_chain, (chains[0],))   # agreement check of chain 0, full length
+               "sample": cpu_sample_text(chains, ncores, sweeps) + f" ({wall:.1f} s wall)"}
+        if FULL_REF:   # agreement with the reference, full-length chains, while the GPU runs
+            picks, ref_chains = agreement_plan(chains)
+            full_ref = pool.map_async(_full_ref_chain, ref_chains)
 
     import torch
     import torch.distributed as dist
@@ -399,10 +488,39 @@ def bench_ours(args):
                "d2h_bytes_per_step": int(d2h), "steps": len(times), "ms_per_step": 1000 * e2e_s,
                "api": "fb_fit_batch (host buffers; allocation, H2D, MCMC, D2H of sigma/yhat/yhat_mean/trees)"}
 
+    # the plain one-chain-per-launch form of the same chains: one chain of each shape, each alone in its launch
+    # (automatic shape for one chain), outside the timed region
+    per_launch = None
+    if rank == 0 and world == 1 and FULL_REF and not args.no_single:
+        picks1 = agreement_plan(chains)[0]
+        secs = []
+        for k in picks1:
+            b1 = F.Batch([chains[k]], NSKIP, NDPOST, device=local)
+            b1.run(stream.cuda_stream)
+            a1, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a1.record(stream)
+            b1.run(stream.cuda_stream)
+            c1.record(stream)
+            torch.cuda.synchronize()
+            secs.append(a1.elapsed_time(c1) / 1000.0)
+            info1 = b1.launch_info()
+            b1.close()
+        rate = len(picks1) * S / sum(secs)
+        per_launch = {"chain_sweeps_per_s": rate, "chains_timed": len(picks1), "batched_over_per_launch": value / rate,
+                      "shape": f"{info1['threads']} threads x {info1['cluster']} CTA(s) per chain (automatic)",
+                      "what": "one chain of each shape per launch, device-timed: the plain one-chain-per-launch form"}
+
     r_f = None
     if full_ref is not None:
-        fm = full_ref.get(timeout=600)
-        r_f = float(np.corrcoef(outs[0]["yhat_mean"], fm)[0, 1])
+        ref_res = full_ref.get(timeout=900)
+        picks, ref_chains = agreement_plan(chains)
+        second = []
+        for k in picks:   # a second GPU seed of the same chain (outside the timed region)
+            d = dict(chains[k])
+            d["seed"] = int(d["seed"]) + 1_000_003
+            second.append(d)
+        gs2 = F.fit_batch(second, NSKIP, NDPOST, device=local, trees=False)
+        r_f = agreement(picks, outs, gs2, ref_res)
         pool.close()
     if pool is not None:
         pool.terminate()
@@ -411,13 +529,12 @@ def bench_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64-fixed+f32+f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD_NAME, "chains_per_gpu": len(chains), "ntree": NTREE,
-                           "nskip": NSKIP, "ndpost": NDPOST, "n_range": N_RANGE, "p_range": P_RANGE,
-                           "l2": "flushed (512 MiB write) before every timed step", "threads": info["threads"],
-                           "grid": info["grid"], "smem_bytes": info["smem"], "ctas_per_chain": info["cluster"],
-                           "shape": "autotuned" if tuned else "rules"},
+                "config": config_of(chains),
+                "launch": {"threads": info["threads"], "grid": info["grid"], "smem_bytes": info["smem"],
+                           "ctas_per_chain": info["cluster"], "shape": "autotuned" if tuned else "rules"},
                 "e2e": e2e, "gpu_launches": args.steps * info["launches"], "roofline": roof, "cpu_baseline": cpu,
-                "clocks": clk, "ess_per_s": ess_line, "r_f_vs_reference_chain0": r_f, "wall_s": wall}
+                "clocks": clk, "ess_per_s": ess_line, "agreement_with_reference": r_f,
+                "one_chain_per_launch": per_launch, "wall_s": wall}
         if predict is not None:
             line["predict_draw"] = predict
         print(json.dumps(line), flush=True)
@@ -741,6 +858,206 @@ def bench_learned(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------ mixed batch
+MIX_METRIC = ("chain-sweeps/s (256 mixed chains in one launch: 128 fwbart n 2,000-65,536 p 8-32 ntree 200, "
+              "128 fpbart n 4,096-24,576 ntree 50), then predict_draw of 1,000 draws x 200 trees on 1,000,000 rows")
+MIX_PRED_ROWS, MIX_P = 1_000_000, 32
+
+
+def _dev_oracle_fit(ch):
+    from oracle import oracle as O
+    o = O.fit(ch, O.MODE_DEV)
+    return {k: np.asarray(o[k]) for k in ("sigma", "fmean", "trees", "moves")}
+
+
+def _mix_newdata(rows: int, seed: int = 31):
+    """Fresh rows of the predict fits' distribution (titer-like, p 32: half U(0,1), half integer 0..9)."""
+    rng = np.random.default_rng(seed)
+    x = np.empty((rows, MIX_P))
+    x[:, :MIX_P // 2] = rng.random((rows, MIX_P // 2))
+    x[:, MIX_P // 2:] = rng.integers(0, 10, (rows, MIX_P - MIX_P // 2))
+    return x
+
+
+def bench_mixed(args):
+    """Config 5: the mixed 256-chain batch in one persistent launch, with BART's proposal and with the learned
+    proposal (trained on this batch's accepted births from a collecting run), then compile_trees + bulk predict_draw
+    of the 10 p-32 fwbart fits' pooled 1,000 kept draws (200 trees each) on 1,000,000 fresh rows x 32 FP64 columns.
+    Sampled parity: the 4 smallest chains (2 fwbart, 2 fpbart) against the oracle's DEV arithmetic, full length, bit
+    for bit; predict on 2,000 rows x 3 draws against the oracle's restatement of predict_draw_cpp."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from fastbart_b200 import workloads as W
+    chains = W.mixed_batch(seed=0, nskip=NSKIP, ndpost=NDPOST)
+    S = NSKIP + NDPOST
+    ncores = os.cpu_count() or 1
+    pool = mp.get_context("spawn").Pool(ncores)
+    pool.map(_warm_worker, range(ncores), chunksize=1)
+    sweeps = cpu_sample_plan(ncores)
+    cpu = None
+    if not args.no_cpu_baseline or args.impl == "reference":
+        vals = []
+        for _ in range((args.warmup + args.steps) if args.impl == "reference" else 1):
+            v, kind, wall = run_cpu_sample(pool, chains, ncores, sweeps)
+            vals.append(v)
+        v = float(np.mean(vals[args.warmup:] if args.impl == "reference" else vals))
+        cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": kind,
+               "sample": cpu_sample_text(chains, ncores, sweeps)}
+    mcfg = {"workload": "mixed_256", "chains": len(chains), "fwbart": 128, "fpbart": 128, "nskip": NSKIP,
+            "ndpost": NDPOST, "n_total": int(sum(np.asarray(c["q"]).shape[1] for c in chains)),
+            "predict": {"draws": 1000, "ntree": 200, "rows": MIX_PRED_ROWS, "p": MIX_P},
+            "l2": "inputs resident; the GPU arm flushes L2 (512 MiB write) before every timed step"}
+    if args.impl == "reference":
+        line = {"metric": MIX_METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": mcfg, "impl": "reference",
+                "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                             "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        pool.terminate()
+        return 0
+    order = np.argsort([np.asarray(c["q"]).shape[1] * c["ntree"] for c in chains])
+    checks = [int(k) for k in order if chains[k]["probit"] == 0][:2] + \
+             [int(k) for k in order if chains[k]["probit"] == 1][:2]
+    dev = pool.map_async(_dev_oracle_fit, [chains[k] for k in checks])
+
+    import torch
+    import fastbart_b200 as F
+    from fastbart_b200 import diagnostics
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    b = F.Batch(chains, NSKIP, NDPOST)
+    info = b.launch_info()
+
+    def timed(steps, warmup):
+        for _ in range(warmup):
+            flush.zero_()
+            b.run(stream.cuda_stream)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, c in evs:
+            flush.zero_()
+            a.record(stream)
+            b.run(stream.cuda_stream)
+            c.record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(c) for a, c in evs) / 1000.0 / steps
+
+    # training examples from a collecting run, then the model
+    b.collect(400_000)
+    b.run(stream.cuda_stream)
+    b.sync()
+    x, y, m, births = b.training_data()
+    b.collect(0)
+    k = min(200_000, len(y))
+    model, losses = F.train_proposal(x[:k], y[:k], m[:k], epochs=10, batch=1024, lr=3e-3, seed=1)
+
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    res = {}
+    for name, mdl in (("plain", None), ("learned", dict(model, mix=0.5))):
+        b.set_proposal(mdl)
+        sec = timed(args.steps, args.warmup)
+        outs = b.download(trees=(name == "plain"))
+        es = [diagnostics.chain_ess(o["sigma"][NSKIP:], o["yhat"]) for o in outs]
+        wb = [i for i, c in enumerate(chains) if c["probit"] == 0]
+        res[name] = {"seconds_per_batch": sec, "chain_sweeps_per_s": len(chains) * S / sec,
+                     "ess_sigma_per_s": float(sum(es[i]["sigma"] for i in wb) / sec),
+                     "ess_f_median_per_s": float(sum(e["f_median"] for e in es) / sec),
+                     "births": int(sum(o["moves"][0] for o in outs))}
+        if name == "plain":
+            plain_outs = outs
+        else:
+            corr = [float(np.corrcoef(a["yhat_mean"], c["yhat_mean"])[0, 1]) for a, c in zip(plain_outs, outs)]
+            res["learned"]["corr_fmean_vs_plain_median"] = float(np.median(corr))
+            res["learned"]["corr_fmean_vs_plain_min"] = float(np.min(corr))
+    clk = clocks.stop()
+    b.set_proposal(None)
+
+    # sampled bit-exact parity of the plain run
+    parity = []
+    for kk, o in zip(checks, dev.get(timeout=1200)):
+        g = plain_outs[kk]
+        ok = all(np.array_equal(np.asarray(g[a]), o[bk]) for a, bk in
+                 (("sigma", "sigma"), ("yhat_mean", "fmean"), ("trees", "trees"), ("moves", "moves")))
+        parity.append({"chain": kk, "n": int(np.asarray(chains[kk]["q"]).shape[1]), "probit": chains[kk]["probit"],
+                       "bit_exact": bool(ok)})
+    assert all(p_["bit_exact"] for p_ in parity), parity
+
+    # end to end through fb_fit_batch with host buffers (allocation, H2D, MCMC, D2H of every output), one step
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        F.fit_batch(chains, NSKIP, NDPOST)
+        e2e_s = time.perf_counter() - t1
+        d2h = sum(8 * S + 8 * np.asarray(c["q"]).shape[1] * (1 + NDPOST) + 8 * NDPOST * c["ntree"] * 64 for c in chains)
+        h2d = sum(np.asarray(c["q"]).nbytes + 13 * np.asarray(c["q"]).shape[1] for c in chains)
+        e2e = {"value": len(chains) * S / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": 1, "ms_per_step": 1000 * e2e_s,
+               "api": "fb_fit_batch (pageable host buffers; allocation, H2D, MCMC, D2H of sigma/yhat/yhat_mean/trees)"}
+    b.close()
+
+    # bulk predict of the pooled 1,000 draws of the ten p-32 fits
+    trees = np.concatenate([plain_outs[c]["trees"] for c in range(W.MIXED_PREDICT_FITS)], axis=0)
+    grid = W.titer_like_grid(MIX_P)
+    text = F.trees_text_gpu(trees, MIX_P)
+    ct = F.CompiledTrees(text, grid, mu=0.0)
+    xh = _mix_newdata(MIX_PRED_ROWS)
+    xd = torch.tensor(np.ascontiguousarray(xh.T), device="cuda")
+    nd = trees.shape[0]
+    out = torch.empty((nd, MIX_PRED_ROWS), dtype=torch.float64, device="cuda")
+
+    def pred():
+        F.predict_draws_device(ct, xd.data_ptr(), MIX_P, MIX_PRED_ROWS, MIX_PRED_ROWS, 1, nd, out.data_ptr(),
+                               MIX_PRED_ROWS, stream.cuda_stream)
+    for _ in range(args.warmup):
+        flush.zero_()
+        pred()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, c in evs:
+        flush.zero_()
+        a.record(stream)
+        pred()
+        c.record(stream)
+    torch.cuda.synchronize()
+    psec = sum(a.elapsed_time(c) for a, c in evs) / 1000.0 / args.steps
+    from oracle import oracle as O
+    oct_ = O.compile_trees(text, grid)
+    sub = xh[:2000]
+    pparity = all(np.array_equal(out[d - 1, :2000].cpu().numpy(),
+                                 O.predict_draw(oct_, [np.ascontiguousarray(sub[:, v]) for v in range(MIX_P)], d, 0.0))
+                  for d in (1, 500, nd))
+    assert pparity, "bulk predict differs from the oracle"
+    alg = MIX_P * MIX_PRED_ROWS * 8 + nd * MIX_PRED_ROWS * 8 + ct.nnodes * 12
+    peak, peak_kind = measured_peak()
+    predict = {"row_draws_per_s": nd * MIX_PRED_ROWS / psec, "ms_per_call": 1000 * psec, "draws": nd,
+               "nodes": ct.nnodes, "hbm_gbs": alg / psec / 1e9, "frac_of_hbm": alg / psec / 1e9 / peak,
+               "peak": peak, "peak_source": peak_kind, "bit_exact_vs_oracle": bool(pparity),
+               "what": "1,000 draws (10 fits x 100 kept draws) x 200 trees on 1,000,000 fresh rows, one "
+                       "fb_predict_draws_device call, x and results resident"}
+    pool.terminate()
+    value = res["plain"]["chain_sweeps_per_s"]
+    line = {"metric": MIX_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * res["plain"]["seconds_per_batch"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64-fixed+f32+f64", "data": "synthetic",
+            "config": mcfg, "launch": {"threads": info["threads"], "grid": info["grid"], "smem_bytes": info["smem"],
+                                       "ctas_per_chain": info["cluster"]},
+            "e2e": e2e, "gpu_launches": 2 * (args.steps + args.warmup) + 1,
+            "roofline": {"bound": "hbm", "achieved": BYTES_PER_ROW_TREE * sum(np.asarray(c["q"]).shape[1] * (c["ntree"] + 1) for c in chains) * S / res["plain"]["seconds_per_batch"] / 1e9,
+                         "peak": peak, "unit": "GB/s", "traffic": None, "peak_source": peak_kind},
+            "cpu_baseline": cpu, "clocks": clk, "plain": res["plain"], "learned": res["learned"],
+            "learned_over_plain": {"ess_f_per_s": res["learned"]["ess_f_median_per_s"] / res["plain"]["ess_f_median_per_s"],
+                                   "ess_sigma_per_s": res["learned"]["ess_sigma_per_s"] / res["plain"]["ess_sigma_per_s"]},
+            "training": {"examples": int(k), "accepted_births_collected": int(births), "loss_first": float(losses[0]),
+                         "loss_last": float(losses[-1])},
+            "parity_sample": parity, "predict_draw": predict}
+    line["roofline"]["frac"] = line["roofline"]["achieved"] / peak
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -753,8 +1070,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-single", action="store_true", help="skip the one-chain-per-launch comparison")
     ap.add_argument("--workload", default="titer96",
-                    choices=["titer96", "small", "sparse", "probit", "predict", "learned", "text"])
+                    choices=["titer96", "small", "single", "sparse", "probit", "predict", "learned", "text",
+                             "mixed"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -764,6 +1083,8 @@ def main():
         return bench_learned(args)
     if args.workload == "text":
         return bench_text(args)
+    if args.workload == "mixed":
+        return bench_mixed(args)
     set_workload(args.workload)
     if args.impl == "reference":
         return bench_reference(args)

@@ -155,11 +155,13 @@ struct fb_batch {
     if (p) allocs.push_back(p);
     return static_cast<T*>(p);
   }
+  cudaEvent_t done = nullptr;  // recorded on the caller's stream after every run's launches
   ~fb_batch() {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(device);
-    cudaDeviceSynchronize();   // runs may be in flight on a caller's stream (cudaFree used to wait for them too)
+    // the last run may still be in flight on the caller's stream: wait for it alone, not for the whole device
+    if (done) { cudaEventSynchronize(done); cudaEventDestroy(done); }
     for (void* p : allocs) cudaFreeAsync(p, 0);
     cudaStreamSynchronize(0);
     cudaSetDevice(cur);
@@ -335,6 +337,11 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
                        stream) != 0)
       return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  if (!b->done && cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+    b->done = nullptr;
+    return fail(FB_ERR_CUDA, "cannot create the batch's completion event");
+  }
+  CK(cudaEventRecord(b->done, b->stream));
   return FB_OK;
 }
 
@@ -488,6 +495,9 @@ fb_status fb_batch_download(fb_batch* b, fb_chain_out* outs) {
   CK(cudaStreamSynchronize(b->stream));
   std::vector<DState> st(b->nchains);
   CK(cudaMemcpy(st.data(), b->d.states, sizeof(DState) * b->nchains, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < b->nchains; k++)
+    if (st[k].status != 0)
+      return fail(FB_ERR_CUDA, "chain %d: a bounded wait of the sampler on its own leaf-statistics copy gave up", k);
   const int S = b->nskip + b->ndpost;
   std::vector<double> tm;
   for (int k = 0; k < b->nchains; k++) {
@@ -798,7 +808,7 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
       v[k] = (int)vv; c[k] = (int)cc;
       pos[nid[k]] = (int)k;
     }
-    // breadth-first from the root (id 1), each node's two children placed next to each other (predict.cpp:87-101)
+    // breadth-first from the root (id 1), each node's two children placed next to each other (src/predict.cpp:23-38)
     auto it1 = pos.find(1ull);
     if (it1 == pos.end()) { delete ct; return fail(FB_ERR_PARSE, "tree %lld has no root (id 1)", t); }
     qk.assign(1, it1->second);

@@ -57,19 +57,22 @@ __host__ __device__ inline bool bins_hold_model(int threads) {
 struct Prop {                 // proposal of one tree for the current sweep
   double logpr, lu;
   unsigned long long cand;    // slots that can be leaves after the move (normals drawn ahead, in slot order)
-  uint8_t mode, nx, v, c, l, r, pad0, pad1;
+  uint8_t mode, nx, v, c, l, r, dnx, pad1;   // dnx: depth of node nx
 };
 struct Masks { unsigned long long used, leaf; };
 struct Ctl {                  // CTA-shared control state
   int pmode, pnx, pv, pc, pL, pR, pl, pr;   // the last decided move (tree j during pass j+1)
   float DL, DR;                             // apply deltas of a birth's left / right rows
-  long long sL0, sR0;                       // leaf weight sums of a birth's children
-  int nL, nR;                               // and their row counts
+  long long sL0, sR0;                       // leaf weight sums of a birth's children (death: sL0 of the merged node)
+  int nL, nR;                               // and their row counts (death: nL of the merged node)
+  int pd;                                   // depth of the decided move's node
   unsigned long long used, leaf;            // node masks of the tree after the move
   int nleaf[2];                             // leaves of the tree whose table is in buffer 0 / 1
   int births, deaths, caps, rtcaps;
   int chain;
   int accept;                               // MH decision of the current tree (handed from warp 2 to warps 0-1)
+  int err;                                  // a bounded wait gave up (reported in the chain's state)
+  unsigned fetches[2];                      // leaf-statistics copies issued into buffer 0 / 1 (mbarrier phases)
   double sigma;
 };
 
@@ -85,13 +88,41 @@ __device__ __forceinline__ long long warp_sum64(long long x) {
 
 __device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+// ---- bulk asynchronous copies (the copy engine writes shared memory and completes an mbarrier transaction; the
+// issuing warp's own shared-memory accesses do not queue behind the copy)
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+// one arrival that also expects `bytes` of copy transactions, then the copy of `bytes` (16-byte aligned, a multiple
+// of 16) from global memory into this CTA's shared memory, completing on `bar`
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Waits for the completion of phase `parity` of bar for at most MBAR_WAIT_NS nanoseconds; false when it gave up.
+constexpr unsigned long long MBAR_WAIT_NS = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (global_ns() - t0 < MBAR_WAIT_NS)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// generic-proxy global stores of this thread become visible to later bulk copies (async proxy)
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t bcast4(int v) { return (uint32_t)v * 0x01010101u; }
 __device__ __forceinline__ int byte_of(uint32_t w, int e) { return (int)((w >> (8 * e)) & 255u); }
@@ -605,7 +636,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
   const double ub = fbm::u32d(x.x), un = fbm::u32d(x.y), uv = fbm::u32d(x.z), uc = fbm::u32d(x.w);
   const bool model = MP && B.mvar != nullptr;
   Prop P;
-  P.mode = 0; P.nx = 0; P.v = 0; P.c = 0; P.l = 0; P.r = 0; P.pad0 = P.pad1 = 0; P.logpr = 0; P.lu = 0;
+  P.mode = 0; P.nx = 0; P.v = 0; P.c = 0; P.l = 0; P.r = 0; P.dnx = P.pad1 = 0; P.logpr = 0; P.lu = 0;
   double pr = 0;
   if (ub < PBx) {
     const int nx = select_kth(goodm, (int)(un * ngood));
@@ -636,7 +667,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
       const double Pbotx = (double)1 / ngood;
       pr = (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
       if (model) pr = pr * corr;
-      P.mode = 1; P.nx = (uint8_t)nx; P.v = (uint8_t)v; P.c = (uint8_t)c;
+      P.mode = 1; P.nx = (uint8_t)nx; P.v = (uint8_t)v; P.c = (uint8_t)c; P.dnx = (uint8_t)dnx;
     }
   } else if (nnogs > 0) {
     const int nx = select_kth(nogm, (int)(un * nnogs));
@@ -674,8 +705,8 @@ struct Smem {
   float* th;                    // [m][64]
   Prop* prop;                   // [m]
   Masks* masks;                 // [m]
-  DTree* tree;                  // [2] topology of trees j and j+1 (buffer j & 1)
-  long long* s0t;               // [2][LST] leaf statistics of the same trees (S0 [64], then row counts int [64])
+  unsigned long long* bar;      // [2] mbarriers of the leaf-statistics buffers
+  long long* s0t;               // [2][LST] leaf statistics of trees j and j+1 (buffer j & 1: S0 [64], counts int [64])
   float* D;                     // [64] apply deltas of the last decided move
   float2* tc;                   // [2][64] theta and compact leaf index
   double* z;                    // [64] mu normals of tree j beyond the first ZMAX candidates
@@ -704,7 +735,7 @@ __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_
   off[2] = o; o += align_up((size_t)m_max * NODES * 4, 16);                  // th
   off[3] = o; o += align_up((size_t)m_max * sizeof(Prop), 16);               // prop
   off[4] = o; o += align_up((size_t)m_max * sizeof(Masks), 16);              // masks
-  off[5] = o; o += 2 * align_up(sizeof(DTree), 16);                          // tree[2]
+  off[5] = o; o += 16;                                                       // bar[2]
   off[6] = o; o += 2 * LST * 8;                                              // s0t[2]
   off[7] = o; o += NODES * 4;                                                // D
   off[8] = o; o += 2 * NODES * 8;                                            // tc[2]
@@ -734,7 +765,7 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.th = reinterpret_cast<float*>(base + off[2]);
   S.prop = reinterpret_cast<Prop*>(base + off[3]);
   S.masks = reinterpret_cast<Masks*>(base + off[4]);
-  S.tree = reinterpret_cast<DTree*>(base + off[5]);
+  S.bar = reinterpret_cast<unsigned long long*>(base + off[5]);
   S.s0t = reinterpret_cast<long long*>(base + off[6]);
   S.D = reinterpret_cast<float*>(base + off[7]);
   S.tc = reinterpret_cast<float2*>(base + off[8]);
@@ -776,16 +807,23 @@ __device__ __forceinline__ void build_tc_slot(const Smem& S, int j, int s) {
   if (s == 0) S.ctl->nleaf[j & 1] = __popcll(lm);
 }
 
-// copy tree j (topology and leaf statistics) from global memory into buffer j & 1 (control warp); one cp.async group
-__device__ __forceinline__ void fetch_tree(const Smem& S, const DTree* trees, const long long* s0g, int j, int lane) {
-  constexpr int TW = (int)(sizeof(DTree) / 16), SW = LST * 8 / 16;
-  unsigned char* td = reinterpret_cast<unsigned char*>(S.tree + (j & 1));
-  unsigned char* sd = reinterpret_cast<unsigned char*>(S.s0t + (j & 1) * LST);
-  for (int k = lane; k < TW + SW; k += 32) {
-    if (k < TW) cp_async16(td + 16 * k, reinterpret_cast<const unsigned char*>(trees + j) + 16 * k);
-    else cp_async16(sd + 16 * (k - TW), reinterpret_cast<const unsigned char*>(s0g + (long long)j * LST) + 16 * (k - TW));
+// copy tree j's leaf statistics from global memory into buffer j & 1: one bulk copy issued by lane 0 of the control
+// warp, completing on the buffer's mbarrier (the topology stays in global memory: phase B needs only the statistics,
+// and a move's changes to the topology are known without reading it)
+__device__ __forceinline__ void fetch_stats(const Smem& S, const long long* s0g, int j, int lane) {
+  if (lane == 0) {
+    const int b = j & 1;
+    S.ctl->fetches[b]++;
+    bulk_copy_g2s(S.s0t + b * LST, s0g + (long long)j * LST, LST * 8, S.bar + b);
   }
-  cp_async_commit();
+  __syncwarp();
+}
+// wait for tree j's statistics in buffer j & 1 (the phase of its last copy); a wait that gives up is recorded
+// (after a wait has given up, later waits are skipped: the chain's results are then flagged as failed)
+__device__ __forceinline__ void wait_stats(const Smem& S, int j) {
+  const int b = j & 1;
+  if (S.ctl->err) return;
+  if (!mbar_wait(S.bar + b, (S.ctl->fetches[b] - 1u) & 1u)) S.ctl->err = 1;
 }
 
 // An accepted birth of tree j becomes a training example (control warp).
@@ -800,8 +838,11 @@ __device__ __forceinline__ void collect_example(const DBufs& B, const DChain& C,
   }
 }
 
-// apply the decided move of tree j (ctl) to its topology and leaf statistics in buffer j & 1 and write the tree back
-// (control warp)
+// Write the decided move of tree j (ctl) into its topology and leaf statistics in global memory (control warp).  Only
+// what the move changes is stored, one field per lane: nothing for a rejected move; for a birth the node's split and
+// children, the children's parent, depth, children and unknown goodvar count, both masks and the children's sums and
+// counts; for a death the node's split fields, masks, sum and count.  The move is src/bart_kernel.cpp:492-500 / 509-512;
+// the reference stores its whole tree after every step instead (store_tree, :229-236, called at :533).
 template <bool LP>
 __device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTree* trees, long long* s0g, int j,
                             int lane, bool lead) {
@@ -809,30 +850,54 @@ __device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTre
   if constexpr (LP) {
     if (B.train_cap > 0 && lead && ctl.pmode == 1) collect_example(B, C, j, ctl.pv, lane);
   }
-  DTree* t = S.tree + (j & 1);
-  long long* s0 = S.s0t + (j & 1) * LST;
+  const int mode = ctl.pmode;
+  if (mode == 0) return;
+  uint8_t* tb = reinterpret_cast<uint8_t*>(trees + j);
+  long long* s0 = s0g + (long long)j * LST;
   int* cnt = reinterpret_cast<int*>(s0 + NODES);
-  const int mode = ctl.pmode, nx = ctl.pnx;
-  if (lane == 0) {
-    if (mode == 1) {
-      const int L = ctl.pL, R = ctl.pR;
-      t->v[nx] = (uint8_t)ctl.pv; t->c[nx] = (uint8_t)ctl.pc; t->l[nx] = (uint8_t)L; t->r[nx] = (uint8_t)R;
-      t->par[L] = (uint8_t)nx; t->par[R] = (uint8_t)nx; t->l[L] = t->r[L] = t->l[R] = t->r[R] = 0;
-      t->d[L] = t->d[R] = (uint8_t)(t->d[nx] + 1);
-      t->ngv[L] = t->ngv[R] = 255;   // counted by the next sweep's proposal step
-      s0[L] = ctl.sL0; s0[R] = ctl.sR0; cnt[L] = ctl.nL; cnt[R] = ctl.nR;
-    } else if (mode == 2) {
-      const int l = ctl.pl, r = ctl.pr;
-      s0[nx] = s0[l] + s0[r]; cnt[nx] = cnt[l] + cnt[r];
-      t->l[nx] = 0; t->r[nx] = 0; t->v[nx] = 0; t->c[nx] = 0;
+  const int nx = ctl.pnx;
+  constexpr int FL = 0, FR = NODES, FPAR = 2 * NODES, FV = 3 * NODES, FC = 4 * NODES, FD = 5 * NODES,
+                FNGV = 6 * NODES, FUSED = 7 * NODES;
+  if (mode == 1) {
+    const int L = ctl.pL, R = ctl.pR;
+    const uint8_t d1 = (uint8_t)(ctl.pd + 1);
+    switch (lane) {
+      case 0: tb[FV + nx] = (uint8_t)ctl.pv; break;
+      case 1: tb[FC + nx] = (uint8_t)ctl.pc; break;
+      case 2: tb[FL + nx] = (uint8_t)L; break;
+      case 3: tb[FR + nx] = (uint8_t)R; break;
+      case 4: tb[FPAR + L] = (uint8_t)nx; break;
+      case 5: tb[FPAR + R] = (uint8_t)nx; break;
+      case 6: tb[FL + L] = 0; break;
+      case 7: tb[FR + L] = 0; break;
+      case 8: tb[FL + R] = 0; break;
+      case 9: tb[FR + R] = 0; break;
+      case 10: tb[FD + L] = d1; break;
+      case 11: tb[FD + R] = d1; break;
+      case 12: tb[FNGV + L] = 255; break;   // counted by the next sweep's proposal step
+      case 13: tb[FNGV + R] = 255; break;
+      case 14: reinterpret_cast<unsigned long long*>(tb + FUSED)[0] = ctl.used; break;
+      case 15: reinterpret_cast<unsigned long long*>(tb + FUSED)[1] = ctl.leaf; break;
+      case 16: s0[L] = ctl.sL0; break;
+      case 17: s0[R] = ctl.sR0; break;
+      case 18: cnt[L] = ctl.nL; break;
+      case 19: cnt[R] = ctl.nR; break;
+      default: break;
     }
-    if (mode) { t->used = ctl.used; t->leaf = ctl.leaf; }
+  } else {
+    switch (lane) {
+      case 0: tb[FL + nx] = 0; break;
+      case 1: tb[FR + nx] = 0; break;
+      case 2: tb[FV + nx] = 0; break;
+      case 3: tb[FC + nx] = 0; break;
+      case 4: reinterpret_cast<unsigned long long*>(tb + FUSED)[0] = ctl.used; break;
+      case 5: reinterpret_cast<unsigned long long*>(tb + FUSED)[1] = ctl.leaf; break;
+      case 6: s0[nx] = ctl.sL0; break;
+      case 7: cnt[nx] = ctl.nL; break;
+      default: break;
+    }
   }
-  __syncwarp();
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(t);
-  uint32_t* dst = reinterpret_cast<uint32_t*>(trees + j);
-  for (int k = lane; k < (int)(sizeof(DTree) / 4); k += 32) dst[k] = src[k];
-  for (int k = lane; k < LST; k += 32) s0g[(long long)j * LST + k] = s0[k];
+  fence_proxy_async_global();   // the next sweep's bulk copy of these statistics sees the stores
   __syncwarp();
 }
 
@@ -947,6 +1012,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       ctl.rtcaps = lead ? st.rtcaps : 0;   // latent-z caps are counted per CTA and summed at the end
     }
     ctl.pmode = 0;
+    ctl.err = 0;
   }
   for (int k = tid; k < (NBS + NSPLIT) * RT; k += T) S.bins[k] = 0;
   __syncthreads();
@@ -996,6 +1062,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       else if (w == NODES) v = (long long)(unsigned)n;   // cnt[0] = n (little endian: low half of word 64)
       s0g[k] = v;
     }
+    fence_proxy_async_global();   // the bulk copies of the first sweep see these statistics
   } else {
     if (B.rows_in_smem)
       for (int li = tid; li < ns; li += T) S.r[li] = rg[li];
@@ -1007,6 +1074,9 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   uint32_t lcr[G > 0 ? G : 1], qcr[G > 0 ? G : 1], nlc[G > 0 ? G : 1], nqc[G > 0 ? G : 1];
 
   for (int it = it0; it < it1; it++) {
+    // a bounded wait gave up: a chain on one CTA stops here (its state says so); the CTAs of a cluster keep their
+    // barriers in step and finish with the error recorded
+    if (!CL && ctl.err) break;
     const double inv_s2 = 1.0 / (ctl.sigma * ctl.sigma);
     // ---------------------------------------------------------------- learned model, one warp per tree
     if (MP && B.mvar) {
@@ -1035,12 +1105,11 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     for (int k = tid; k < 2 * NODES; k += T) S.ovb[k] = 0ull;
     __syncthreads();
     if (warp == 0) {
-      fetch_tree(S, trees, s0g, 0, lane);
-      if (m > 1) fetch_tree(S, trees, s0g, 1, lane);
+      fetch_stats(S, s0g, 0, lane);
+      if (m > 1) fetch_stats(S, s0g, 1, lane);
       build_tc_slot(S, 0, lane);
       build_tc_slot(S, 0, lane + 32);
       if (lane == 0) ctl.pmode = 0;
-      cp_async_wait_all();
     }
     __syncthreads();
     // the first pass of a sweep loads its words itself: the held words are dead until here (keeps them out of the
@@ -1084,15 +1153,12 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         // can be a leaf of tree j after its move (current leaves, the two slots a birth would take, the node a death
         // would restore)
         if (j > 0) commit_tree<LP>(S, C, B, trees, s0g, j - 1, lane, lead);
-        if (j + 1 < m && j > 0) fetch_tree(S, trees, s0g, j + 1, lane);
+        if (j + 1 < m && j > 0) fetch_stats(S, s0g, j + 1, lane);
         const unsigned long long cand = P.cand;
         if (__popcll(cand) > ZMAX)
           for (int s = lane; s < NODES; s += 32)
             if (((cand >> s) & 1ull) && __popcll(cand & ((1ull << s) - 1ull)) >= ZMAX)
               S.z[s] = fbm::fb_normal(seed, (uint32_t)s << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
-        // tree j's copy (issued one step earlier) must have landed before phase B; tree j+1's may stay in flight
-        if (j + 1 < m && j > 0) cp_async_wait_prev();
-        else cp_async_wait_all();
       }
       __syncthreads();
       reduce_totals(S.bins, RT, ctl.nleaf[cur], P.mode, S.tot + cur * TOT);
@@ -1111,6 +1177,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       const bool sep = T >= 96;
       if (tid < (sep ? NODES + 32 : NODES)) {
         const int s = tid;
+        wait_stats(S, j);   // tree j's statistics (copy issued one step earlier, normally landed long ago)
         const Masks mk = S.masks[j];
         const long long* tot = (CL ? S.ctot : S.tot) + cur * TOT;
         const unsigned long long* ovb = (CL ? S.covb : S.ovb) + cur * NODES;
@@ -1219,7 +1286,8 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
             if (nmode == 1) ctl.births++;
             if (nmode == 2) ctl.deaths++;
             ctl.pmode = nmode; ctl.pnx = P.nx; ctl.pv = P.v; ctl.pc = P.c; ctl.pL = L; ctl.pR = R;
-            ctl.pl = P.l; ctl.pr = P.r; ctl.sL0 = sL0; ctl.sR0 = sR0; ctl.nL = nL; ctl.nR = nR;
+            ctl.pl = P.l; ctl.pr = P.r; ctl.sL0 = sL0; ctl.sR0 = sR0; ctl.nL = nL; ctl.nR = nR; ctl.pd = P.dnx;
+            if (nmode == 2) { ctl.sL0 = s0[P.l] + s0[P.r]; ctl.nL = cnt[P.l] + cnt[P.r]; }   // the merged node
             ctl.used = used; ctl.leaf = leafm;
           }
         }
@@ -1344,6 +1412,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   if (tid == 0 && lead) {
     st.sigma = ctl.sigma; st.births = ctl.births; st.deaths = ctl.deaths; st.caps = ctl.caps; st.rtcaps = rtcaps;
     st.it_done = it1;
+    st.status = (it0 == 0 ? 0 : st.status) | ctl.err;
   }
   __syncthreads();
   if (CL) cg::this_cluster().sync();   // no CTA reuses or leaves its shared memory while others read it
@@ -1356,6 +1425,13 @@ template <int G, bool CL, int MODE>
 __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it0, int it1) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem, B.cluster);
+  if (threadIdx.x == 0) {   // the leaf-statistics buffers' mbarriers, once per launch
+    mbar_init(S.bar, 1);
+    mbar_init(S.bar + 1, 1);
+    S.ctl->fetches[0] = S.ctl->fetches[1] = 0u;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
   if constexpr (MODE != MODE_PLAIN) {   // the proposal model's weights, once per launch
     if (B.mvar && B.model_smem && !bins_hold_model(blockDim.x)) {
       for (int k = threadIdx.x; k < MIMG_WORDS / 4; k += blockDim.x)

@@ -11,6 +11,10 @@ shipped, so these generators stand in for them with the same shapes, sizes and v
                     x 16 multinomial bootstrap resamples; half U(0,1) and half integer 0..9 columns;
                     y = linear term on 4 columns + sin(pi xa xb) + N(0, .5^2); w ~ Gamma(4, 4); ntree 200
   friedman_large    n 65,536, p 32, numcut 255, Friedman-5 on x1..x5 + N(0,1), 16 chains
+  mixed_batch       256 chains in one batch: 128 fwbart chains of titer-like data (n uniform in 2,000..65,536, p in
+                    8..32, ntree 200) and 128 fpbart chains of hazard data (n uniform in 4,096..24,576, ntree 50);
+                    ten of the fwbart chains (p 32) share one cutpoint grid, so their kept draws pool into one
+                    1,000-draw forest for bulk predict on fresh rows of the same distribution
   random_forest     posterior draws of trees grown from BART's tree prior (packed node format), for bulk predict
 """
 from __future__ import annotations
@@ -30,9 +34,10 @@ def friedman(x: np.ndarray) -> np.ndarray:
 
 
 def fwbart_chain(x, y, w=None, *, ntree=200, nskip=1000, ndpost=100, numcut=100, k=2.0, power=2.0, base=0.95,
-                 sigdf=3.0, sigquant=0.9, seed=1, fmean=None) -> dict:
-    """Prepares one fwbart chain exactly as the R wrapper does (R/fwbart.R:8-27); returns the chain dict."""
-    d = prep.model_matrix(x, numcut)
+                 sigdf=3.0, sigquant=0.9, seed=1, fmean=None, xinfo=None) -> dict:
+    """Prepares one fwbart chain exactly as the R wrapper does (R/fwbart.R:8-27); returns the chain dict.  xinfo:
+    fixed cutpoints per column (as R's xinfo argument), else the cutpoint rule of prep.cutpoints."""
+    d = prep.model_matrix(x, numcut, True, xinfo)
     y = np.asarray(y, dtype=np.float64)
     n = y.size
     w = np.ones(n) if w is None else np.asarray(w, dtype=np.float64)
@@ -51,9 +56,9 @@ def fwbart_chain(x, y, w=None, *, ntree=200, nskip=1000, ndpost=100, numcut=100,
 
 
 def fpbart_chain(x, y, *, ntree=50, nskip=1000, ndpost=100, numcut=100, k=2.0, power=2.0, base=0.95,
-                 binary_offset=None, seed=1) -> dict:
+                 binary_offset=None, seed=1, xinfo=None) -> dict:
     """Prepares one fpbart chain as R/fpbart.R:7-24 does."""
-    d = prep.model_matrix(x, numcut)
+    d = prep.model_matrix(x, numcut, True, xinfo)
     y = np.asarray(y).astype(np.int32)
     n = y.size
     off = float(stats.norm.ppf(np.mean(y))) if binary_offset is None else float(binary_offset)
@@ -125,6 +130,50 @@ def titer_bootstrap(reps=16, shapes=range(6), seed=0, **kw) -> list:
             kw2.setdefault("seed", 12345 + len(chains))
             chains.append(fwbart_chain(x[idx], y[idx], w[idx], **kw2))
     return chains
+
+
+def titer_like(n: int, p: int, seed=0):
+    """Titer-like data of any shape: the first p // 2 columns U(0,1), the rest integer 0..9; y = a linear term on 4
+    columns (coefficients N(0,1)) + sin(pi xa xb) on two U(0,1) columns + N(0, 0.5^2); w ~ Gamma(4, rate 4)."""
+    rng = np.random.default_rng(seed)
+    half = p // 2
+    x = np.empty((n, p))
+    x[:, :half] = rng.random((n, half))
+    x[:, half:] = rng.integers(0, 10, (n, p - half))
+    lin = rng.choice(p, 4, replace=False)
+    a, b = rng.choice(half, 2, replace=False)
+    y = x[:, lin] @ rng.normal(0, 1, 4) + np.sin(np.pi * x[:, a] * x[:, b]) + rng.normal(0, 0.5, n)
+    return x, y, rng.gamma(4.0, 1.0 / 4.0, n)
+
+
+def titer_like_grid(p: int, numcut: int = 100) -> list:
+    """The shared cutpoint grid of titer_like columns: numcut uniform interior points of (0, 1) for the U(0,1)
+    columns, the midpoints 0.5 .. 8.5 for the integer columns."""
+    half = p // 2
+    u = np.arange(1, numcut + 1, dtype=np.float64) / (numcut + 1)
+    return [u.copy() for _ in range(half)] + [np.arange(9, dtype=np.float64) + 0.5 for _ in range(p - half)]
+
+
+MIXED_PREDICT_FITS = 10
+
+
+def mixed_batch(seed=0, n_wbart=128, n_pbart=128, nskip=1000, ndpost=100, predict_fits=MIXED_PREDICT_FITS) -> list:
+    """The mixed 256-chain workload (see the module docstring).  Chains 0 .. predict_fits-1 are the p = 32 fwbart
+    fits on the shared grid of titer_like_grid(32)."""
+    rng = np.random.default_rng(90_000 + seed)
+    out = []
+    for c in range(n_wbart):
+        n = int(rng.integers(2000, 65537))
+        p = 32 if c < predict_fits else int(rng.integers(8, 33))
+        x, y, w = titer_like(n, p, seed=91_000 + 1000 * seed + c)
+        xinfo = titer_like_grid(p) if c < predict_fits else None
+        out.append(fwbart_chain(x, y, w, ntree=200, nskip=nskip, ndpost=ndpost, seed=500_000 + 1000 * seed + c,
+                                xinfo=xinfo))
+    for c in range(n_pbart):
+        n = int(rng.integers(4096, 24577))
+        x, y = hazard_data(n, seed=92_000 + 1000 * seed + c)
+        out.append(fpbart_chain(x, y, ntree=50, nskip=nskip, ndpost=ndpost, seed=600_000 + 1000 * seed + c))
+    return out
 
 
 def friedman_large(nchains=16, n=65536, p=32, seed=0, **kw) -> list:

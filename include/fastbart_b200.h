@@ -209,8 +209,10 @@ fb_status fb_predict_draws_device(const fb_compiled* ct, const double* x_dev, in
  * cudaMalloc: a process whose device memory is already held by another framework's caching allocator or by a fixed
  * budget, where a new allocation can fail, and latency-sensitive loops, where cudaFree synchronizes the whole device
  * and stalls every other stream.
- * Limit: n * (ncol + 1) <= 1048576 doubles; larger inputs fail with FB_ERR_LIMIT (split the rows over several calls).
- * The first call on a device does the set-up: it looks up the array's device address with that device current.
+ * Limits: n * (ncol + 1) <= 1048576 doubles, and device ordinals 0..63; beyond either the call fails with
+ * FB_ERR_LIMIT (split the rows over several calls).
+ * The first call on a device does the set-up: it looks up the array's device address with that device current and
+ * keeps it for the life of the process, so the process must not reset that device (cudaDeviceReset) afterwards.
  * Make that first call before any stream capture.  Nothing in the array needs to start at zero, because each call
  * copies in all its columns and the kernel writes every result.  All calls on a device share the one array, so calls
  * that overlap on the GPU (from several host threads) race; serialize them. */

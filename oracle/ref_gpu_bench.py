@@ -22,6 +22,7 @@ import os
 import re
 import subprocess
 import sys
+import tempfile
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -72,13 +73,15 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reps", type=int, default=16)
     ap.add_argument("--threads", type=int, default=256)
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "refgpu"))
+    ap.add_argument("--out", default=None, help="folder for the input files and logs (default: a new temporary folder)")
     ap.add_argument("--no-single", action="store_true")
     args = ap.parse_args()
     exe = os.path.join(HERE, "_ref", "bart_batch")
     if not os.path.exists(exe):
         print(json.dumps({"reference_gpu": "unavailable", "why": "oracle/_ref/bart_batch was not built"}))
         return 0
+    if args.out is None:
+        args.out = tempfile.mkdtemp(prefix="fastbart_refgpu_")
     os.makedirs(args.out, exist_ok=True)
     import multiprocessing as mp
     bases = []

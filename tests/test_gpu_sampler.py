@@ -1,5 +1,6 @@
 """GPU parity of the sampler: the fused per-tree pass and whole chains are bit-exact against the oracle's DEV
-arithmetic on identical state; statistical agreement with the reference sampler (oracle/_ref)."""
+arithmetic on identical state.  Statistical agreement with the reference sampler at the benchmark shapes is in
+test_gpu_parity_shapes.py."""
 import ctypes as C
 
 import numpy as np
@@ -141,31 +142,6 @@ def test_cluster_rows_beyond_one_cta(orc):
     eight = fit_batch([ch], 3, 2, cluster=8)[0]
     _compare(eight, one)
     _compare(one, orc.fit(ch, orc.MODE_DEV))
-
-
-def _ref_pool_fit(ch):
-    from oracle import oracle as O
-    return O.ref_fit(ch)
-
-
-def test_statistical_agreement_with_reference(orc):
-    """Whole chains agree with the reference sampler as closely as two reference seeds agree with each other:
-    posterior-mean f correlation within 0.003 of the reference's own seed-to-seed correlation (and >= 0.98), and the
-    mean of sigma over the kept draws, averaged over 6 chains per sampler, within 2%."""
-    if not orc.ref_available():
-        pytest.skip("reference library not built")
-    import multiprocessing as mp
-    x, y, w = W.friedman_data(2000, 10, 31)
-    chains = [W.fwbart_chain(x, y, w, ntree=100, nskip=800, ndpost=200, seed=77 + k) for k in range(6)]
-    gs = fit_batch(chains, 800, 200)
-    with mp.get_context("spawn").Pool(6) as pool:
-        rs = pool.map(_ref_pool_fit, chains)
-    seed_spread = np.corrcoef(rs[0]["fmean"], rs[1]["fmean"])[0, 1]
-    corr = np.corrcoef(gs[0]["yhat_mean"], rs[2]["fmean"])[0, 1]
-    sg = np.mean([g["sigma"][800:].mean() for g in gs])
-    sr = np.mean([r["sigma"][800:].mean() for r in rs])
-    assert corr >= 0.98 and corr >= seed_spread - 0.003, (corr, seed_spread)
-    assert abs(sg / sr - 1) < 0.02, (sg, sr)
 
 
 def test_autotune_picks_a_shape_with_identical_results():

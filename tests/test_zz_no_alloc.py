@@ -48,6 +48,23 @@ def test_two_calls_in_a_row_match_predict_draw(compiled):
         assert np.array_equal(got, ref)   # bit-exact, as every predict test here
 
 
+def test_calls_leave_free_device_memory_unchanged(compiled):
+    """After a first (set-up) call, further calls take no device memory: the driver's free-memory figure stays put."""
+    import torch
+    ct, p, mu = compiled
+    X, _ = W.hazard_data(SCRATCH_DOUBLES // (p + 1), 79)
+    st, first = _call("fb_predict_draw_static", ct, X, 1, mu)
+    assert st == _lib.FB_OK
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for draw in (2, 3, 4, 1):
+        st, got = _call("fb_predict_draw_static", ct, X, draw, mu)
+        assert st == _lib.FB_OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert np.array_equal(got, first)
+
+
 def test_limit_and_argument_errors(compiled):
     ct, p, mu = compiled
     too_big = np.zeros((SCRATCH_DOUBLES // (p + 1) + 1, p))
