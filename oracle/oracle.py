@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBORC = os.path.join(HERE, "liborc.so")
 LIBREF = os.path.join(HERE, "_ref", "libbartref.so")
 REF_BATCH = os.path.join(HERE, "_ref", "bart_batch")
+LIBPREDREF = os.path.join(HERE, "_ref", "libpredref.so")
 
 NODES = 64
 MODE_REF, MODE_DEV = 0, 1
@@ -317,6 +318,70 @@ def predict_draw(ct: Compiled, cols, draw1: int, mu: float) -> np.ndarray:
     if rc == -2:
         raise ValueError(f"draw {draw1} out of range 1..{ct.ndpost}")
     return out
+
+
+# ---- the reference's own evaluator (src/predict.cpp built from source into oracle/_ref/libpredref.so)
+_predref = None
+
+
+def ref_predict_available() -> bool:
+    return os.path.exists(LIBPREDREF)
+
+
+def predreflib():
+    global _predref
+    if _predref is None:
+        R = C.CDLL(LIBPREDREF)
+        R.refp_compile.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_int]
+        R.refp_compile.restype = C.c_void_p
+        R.refp_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 4
+        R.refp_info.restype = None
+        R.refp_arrays.argtypes = [C.c_void_p] * 6
+        R.refp_arrays.restype = None
+        R.refp_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p,
+                                   C.c_char_p, C.c_int]
+        R.refp_predict.restype = C.c_int
+        R.refp_free.argtypes = [C.c_void_p]
+        R.refp_free.restype = None
+        _predref = R
+    return _predref
+
+
+class RefCompiled:
+    """compile_trees_cpp's result list as computed by the reference's own code: the node arrays, and a handle for
+    predict_draw_cpp."""
+
+    def __init__(self, text: str, cutpoints):
+        R = predreflib()
+        xs = [np.ascontiguousarray(c, dtype=np.float64) for c in cutpoints]
+        ptrs = (C.c_void_p * max(1, len(xs)))(*[x.ctypes.data for x in xs])
+        nc = np.array([len(x) for x in xs], dtype=np.int32)
+        err = C.create_string_buffer(256)
+        self._h = R.refp_compile(text.encode(), ptrs, nc.ctypes.data, len(xs), err, 256)
+        if not self._h:
+            raise ValueError(err.value.decode())
+        nd, m, p, nn = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        R.refp_info(self._h, C.byref(nd), C.byref(m), C.byref(p), C.byref(nn))
+        self.ndpost, self.ntree, self.p, self.nnodes = nd.value, m.value, p.value, nn.value
+        self.var, self.child = np.zeros(nn.value, np.int32), np.zeros(nn.value, np.int32)
+        self.cut, self.theta = np.zeros(nn.value), np.zeros(nn.value)
+        self.root = np.zeros(nd.value * m.value, np.int32)
+        R.refp_arrays(self._h, *(a.ctypes.data for a in (self.var, self.child, self.cut, self.theta, self.root)))
+
+    def predict_draw(self, cols, draw1: int, mu: float) -> np.ndarray:
+        xs = [np.ascontiguousarray(c, dtype=np.float64) for c in cols]
+        n = len(xs[0]) if xs else 0
+        ptrs = (C.c_void_p * max(1, len(xs)))(*[x.ctypes.data for x in xs])
+        out = np.zeros(n)
+        err = C.create_string_buffer(256)
+        if predreflib().refp_predict(self._h, ptrs, len(xs), n, int(draw1), float(mu), out.ctypes.data, err, 256):
+            raise ValueError(err.value.decode())
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _predref is not None:
+            _predref.refp_free(self._h)
+            self._h = None
 
 
 def trees_text(trees: np.ndarray, p: int) -> str:

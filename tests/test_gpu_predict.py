@@ -1,4 +1,5 @@
-"""GPU parity of compile_trees / predict_draw: bit-exact against the oracle's restatement of src/predict.cpp."""
+"""GPU parity of compile_trees / predict_draw: bit-exact against the oracle's restatement of src/predict.cpp and
+against golden vectors made by the reference's own src/predict.cpp (tests/golden/ref_predict_*.npz)."""
 import numpy as np
 import pytest
 
@@ -100,3 +101,28 @@ def test_cut_codes_match_find_interval():
         ref = np.searchsorted(d.xi[v], col, side="right")
         ref[np.isnan(col)] = 0
         assert np.array_equal(q[v], ref.astype(np.uint8)), v
+
+
+@pytest.mark.parametrize("name", ["ref_predict_fit", "ref_predict_dup"])
+def test_predict_matches_reference_golden(name):
+    """fb_compile_trees / fb_predict_draw / fb_predict_draws_device against golden vectors made by the reference's own
+    src/predict.cpp: compiled arrays and every draw, bit for bit, on rows with values on cutpoints, NaN and
+    infinities (the dup case has a repeated cutpoint, so it runs the FP64-compare evaluator)."""
+    import os
+    import sys
+    import torch
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    text, cps, x, mu, out, arrays = make_golden.load_predict(name)
+    ct = F.CompiledTrees(text, cps, mu=mu)
+    got = ct.arrays()
+    for k, v in arrays.items():
+        assert np.array_equal(got[k], v), k
+    for d in range(out.shape[0]):
+        assert np.array_equal(F.predict_draw(ct, x, d + 1), out[d]), d
+    n, p = x.shape
+    xd = torch.tensor(np.ascontiguousarray(x.T), device="cuda")
+    od = torch.full((out.shape[0], n), float("nan"), dtype=torch.float64, device="cuda")
+    F.predict_draws_device(ct, xd.data_ptr(), p, n, n, 1, out.shape[0], od.data_ptr(), n)
+    torch.cuda.synchronize()
+    assert np.array_equal(od.cpu().numpy(), out)

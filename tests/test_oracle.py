@@ -182,3 +182,42 @@ def test_oracle_mlp_gradient_finite_differences(orc):
         fd = (orc.mlp_loss_grad(mp, x, y, m)[0] - orc.mlp_loss_grad(mm, x, y, m)[0]) / (
             float(mp[key][idx]) - float(mm[key][idx]))
         assert abs(fd - g[key][idx]) <= 2e-3 + 2e-2 * abs(g[key][idx]), (key, idx, fd, g[key][idx])
+
+
+@pytest.mark.parametrize("name", make_golden.PREDICT_CASES)
+def test_predict_oracle_matches_reference_golden(orc, name):
+    """The oracle's restatement of compile_trees_cpp / predict_draw_cpp equals the reference's own src/predict.cpp
+    (golden made by it): node arrays, and every draw on rows with values on cutpoints, NaN and infinities."""
+    text, cps, x, mu, out, arrays = make_golden.load_predict(name)
+    ct = orc.compile_trees(text, cps)
+    for k, v in arrays.items():
+        assert np.array_equal(getattr(ct, k), v), k
+    cols = [np.ascontiguousarray(x[:, v]) for v in range(x.shape[1])]
+    for d in range(out.shape[0]):
+        assert np.array_equal(orc.predict_draw(ct, cols, d + 1, mu), out[d]), d
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_predict_oracle_matches_reference_library(orc, seed):
+    """Live comparison with the reference evaluator built here (oracle/_ref/libpredref.so): arrays, predictions and
+    the two error cases of src/predict.cpp:51-52."""
+    if not orc.ref_predict_available():
+        pytest.skip("reference evaluator not built (needs the reference sources)")
+    rng = np.random.default_rng(seed)
+    p, ncut = 4 + seed, 30
+    cps = [np.sort(rng.normal(size=ncut)) for _ in range(p)]
+    trees = W.random_forest(5, 17, p, ncut, seed=seed, base=0.9, power=0.8, max_depth=6)
+    text = orc.trees_text(trees, p)
+    ref = orc.RefCompiled(text, cps)
+    ct = orc.compile_trees(text, cps)
+    for k in ("var", "child", "cut", "theta", "root"):
+        assert np.array_equal(getattr(ct, k), getattr(ref, k)), k
+    x = rng.normal(size=(700, p))
+    x[::11, 0] = cps[0][rng.integers(0, ncut, x[::11].shape[0])]
+    cols = [x[:, v] for v in range(p)]
+    for d in (1, 3, 5):
+        assert np.array_equal(orc.predict_draw(ct, cols, d, 0.5), ref.predict_draw(cols, d, 0.5))
+    with pytest.raises(ValueError, match="out of range"):
+        ref.predict_draw(cols, 6, 0.0)
+    with pytest.raises(ValueError, match="columns"):
+        ref.predict_draw(cols[:-1], 1, 0.0)
