@@ -531,7 +531,8 @@ def bench_ours(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64-fixed+f32+f64", "data": "synthetic",
                 "config": config_of(chains),
                 "launch": {"threads": info["threads"], "grid": info["grid"], "smem_bytes": info["smem"],
-                           "ctas_per_chain": info["cluster"], "shape": "autotuned" if tuned else "rules"},
+                           "ctas_per_chain": info["cluster"],
+                           "shape": "autotuned" if (tuned or info["autotuned"]) else "rules"},
                 "e2e": e2e, "gpu_launches": args.steps * info["launches"], "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "ess_per_s": ess_line, "agreement_with_reference": r_f,
                 "one_chain_per_launch": per_launch, "wall_s": wall}

@@ -21,7 +21,7 @@ EXPORTS = ["fb_last_error", "fb_version", "fb_fit_batch", "fb_batch_create", "fb
            "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass",
            "fb_batch_set_proposal", "fb_batch_collect", "fb_batch_training_data", "fb_train_proposal",
            "fb_mlp_loss_grad", "fb_autotune", "fb_cut_codes", "fb_trees_text_gpu", "fb_batch_trees_text",
-           "fb_release_cached_memory"]
+           "fb_release_cached_memory", "fb_batch_autotuned"]
 
 MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
 
@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         L.fb_batch_launch_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(sz), C.POINTER(i)]
         L.fb_batch_destroy.argtypes = [vp]
         L.fb_batch_destroy.restype = None
+        L.fb_batch_autotuned.argtypes = [vp]
         L.fb_fbart.argtypes = [vp, i, i, vp, vp, vp, vp, vp, i, i, i, d, d, d, d, C.c_uint64, i, d, vp, vp, vp, vp,
                                C.c_char_p, sz, C.POINTER(sz), vp]
         L.fb_trees_text.argtypes = [vp, i, i, i, C.c_char_p, sz]

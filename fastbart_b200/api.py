@@ -68,8 +68,16 @@ def _options(nskip, ndpost, threads=0, sweeps_per_launch=0, device=0, cluster=0)
 
 
 def fit_batch(chains: Sequence[dict], nskip: int, ndpost: int, threads: int = 0, sweeps_per_launch: int = 0,
-              device: int = 0, trees: bool = True, cluster: int = 0) -> list:
-    """Runs prepared chains (dicts as built by workloads.fwbart_chain / fpbart_chain) in one device batch."""
+              device: int = 0, trees: bool = True, cluster: int = 0, devices: Sequence[int] | None = None) -> list:
+    """Runs prepared chains (dicts as built by workloads.fwbart_chain / fpbart_chain) in one device batch.  With
+    `devices` (several GPU ordinals) the chains are partitioned across those GPUs, one batch per GPU run from its own
+    host thread, and the outputs are returned in the order of `chains` (shard.fit_sharded)."""
+    if devices is not None and len(devices) > 1:
+        from . import shard
+        return shard.fit_sharded(chains, nskip, ndpost, devices, threads=threads, sweeps_per_launch=sweeps_per_launch,
+                                 trees=trees, cluster=cluster)
+    if devices is not None and len(devices) == 1:
+        device = int(devices[0])
     keep: list = []
     arr = (_lib.Chain * len(chains))(*[_as_chain(c, keep) for c in chains])
     outs = [_alloc_out(c, nskip, ndpost, trees) for c in chains]
@@ -114,7 +122,8 @@ class Batch:
     def launch_info(self) -> dict:
         a, b, c, d, e = C.c_int(), C.c_int(), C.c_int(), C.c_size_t(), C.c_int()
         check(_lib.lib().fb_batch_launch_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e)))
-        return dict(launches=a.value, threads=b.value, grid=c.value, smem=d.value, cluster=e.value)
+        return dict(launches=a.value, threads=b.value, grid=c.value, smem=d.value, cluster=e.value,
+                    autotuned=bool(_lib.lib().fb_batch_autotuned(self._h)))
 
     def download(self, trees: bool = True, alloc=np.empty) -> list:
         outs = [_alloc_out(c, self.nskip, self.ndpost, trees, alloc) for c in self.chains]

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -156,6 +157,7 @@ struct fb_batch {
     return static_cast<T*>(p);
   }
   cudaEvent_t done = nullptr;  // recorded on the caller's stream after every run's launches
+  int autotuned = 0;           // the launch shape came from the autotuner
   ~fb_batch() {
     int cur = 0;
     cudaGetDevice(&cur);
@@ -173,6 +175,35 @@ extern "C" {
 const char* fb_last_error(void) { return g_err.c_str(); }
 const char* fb_version(void) { return "fastbart_b200 0.1.0 (sm_100a)"; }
 
+}  // extern "C"
+
+namespace {
+// Launch shapes chosen by the autotuner, per device and batch signature, for the life of the process.
+std::mutex g_tune_mu;
+std::unordered_map<std::string, std::pair<int, int>> g_tuned;
+
+std::string batch_signature(const fb_chain* chains, int nchains, int device) {
+  long long rows = 0, trees = 0;
+  int nmax = 0, mmax = 0, pmax = 0, probit = 0;
+  for (int k = 0; k < nchains; k++) {
+    rows += chains[k].n; trees += chains[k].ntree; probit += chains[k].probit ? 1 : 0;
+    nmax = std::max(nmax, chains[k].n); mmax = std::max(mmax, chains[k].ntree); pmax = std::max(pmax, chains[k].p);
+  }
+  char buf[160];
+  std::snprintf(buf, sizeof buf, "%d:%d:%lld:%lld:%d:%d:%d:%d", device, nchains, rows, trees, nmax, mmax, pmax, probit);
+  return buf;
+}
+
+// whether an automatic launch shape (threads = cluster = 0) is picked by the autotuner (default) or by the measured
+// rules of fb_batch_create (FASTBART_AUTOTUNE=0)
+bool autotune_by_default() {
+  const char* e = std::getenv("FASTBART_AUTOTUNE");
+  return !(e && e[0] == '0');
+}
+}  // namespace
+
+extern "C" {
+
 fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options* opt, fb_batch** out) {
   if (!out) return fail(FB_ERR_ARG, "out is NULL");
   *out = nullptr;
@@ -183,6 +214,33 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   for (int k = 0; k < nchains; k++) {
     fb_status s = check_chain(chains[k], k);
     if (s != FB_OK) return s;
+  }
+  // automatic shape: the autotuner's choice for this batch signature (timed once per process), else the rules below
+  if (opt->threads == 0 && opt->cluster == 0 && autotune_by_default()) {
+    const std::string sig = batch_signature(chains, nchains, opt->device);
+    std::pair<int, int> shape{0, 0};
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tuned.find(sig);
+      if (it != g_tuned.end()) shape = it->second;
+    }
+    if (shape.first == 0) {
+      fb_options best;
+      if (fb_autotune(chains, nchains, opt, 2, &best, nullptr) == FB_OK) {
+        shape = {best.threads, best.cluster};
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[sig] = shape;
+      } else {
+        g_err.clear();   // no trial shape worked: the rules decide
+      }
+    }
+    if (shape.first > 0) {
+      fb_options o = *opt;
+      o.threads = shape.first; o.cluster = shape.second;
+      fb_status s = fb_batch_create(chains, nchains, &o, out);
+      if (s == FB_OK) (*out)->autotuned = 1;
+      return s;
+    }
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
@@ -477,6 +535,8 @@ fb_status fb_batch_sync(fb_batch* b) {
   CK(cudaGetLastError());
   return FB_OK;
 }
+
+int fb_batch_autotuned(const fb_batch* b) { return b ? b->autotuned : 0; }
 
 fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes,
                                int* cluster) {

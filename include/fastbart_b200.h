@@ -63,7 +63,7 @@ typedef struct fb_chain {
 
 typedef struct fb_options {
   int nskip, ndpost;        /* burn-in and kept sweeps (shared by all chains of a batch) */
-  int threads;              /* threads per CTA; 0 = automatic */
+  int threads;              /* threads per CTA; 0 = automatic (with cluster 0: picked by fb_autotune, cached) */
   int sweeps_per_launch;    /* 0 = the whole MCMC in one launch; k > 0 = launches of k sweeps */
   int device;               /* CUDA device ordinal */
   int cluster;              /* CTAs per chain (a thread-block cluster sharing the rows): 0 = automatic, 1 = one CTA,
@@ -100,6 +100,10 @@ fb_status fb_release_cached_memory(int device);
  * CTAs per chain (thread-block cluster size; 1 without clusters).  Outputs may be NULL. */
 fb_status fb_batch_launch_info(const fb_batch* b, int* launches, int* threads, int* grid, size_t* smem_bytes,
                                int* cluster);
+/* 1 when the batch's launch shape was picked by the autotuner (options threads = cluster = 0, the default), 0 when
+ * it was given or picked by the built-in rules (environment FASTBART_AUTOTUNE=0).  The autotuner's choice is timed
+ * once per device and batch signature (chain count, rows, trees, largest n / ntree / p, probit chains) and reused. */
+int fb_batch_autotuned(const fb_batch* b);
 void fb_batch_destroy(fb_batch* b);
 /* Autotuner of the launch shape: runs trial_sweeps sweeps of the given chains for every candidate shape (threads per
  * CTA 256, 384, 416, 448, 512 x CTAs per chain 1..16 whose clusters are all resident at once), timed with CUDA
