@@ -765,96 +765,131 @@ def bench_text(args):
 
 
 # ------------------------------------------------------------------------------------------------ learned proposal
-LRN_N, LRN_P, LRN_CHAINS, LRN_TRAIN = 65_536, 32, 16, 200_000
-LRN_METRIC = "ESS/s of sigma and f, learned vs plain proposal (16 fwbart chains, n 65,536, p 32, 27 noise predictors)"
+LRN_N, LRN_P, LRN_CHAINS, LRN_TRAIN, LRN_NDPOST, LRN_SETS = 65_536, 32, 16, 200_000, 1000, 4
+LRN_METRIC = ("ESS/s of sigma and f, learned (variable and cutpoint heads) vs plain proposal (16 fwbart chains, "
+              "n 65,536, p 32, numcut 255, 27 noise predictors)")
 
 
 def bench_learned(args):
     """Sparse-signal configuration: Friedman-5 on x1..x5 of 32 uniform predictors, numcut 255, 16 chains, ntree 200,
-    nskip 1000, ndpost 100.  A plain batch (different seeds) supplies accepted births as training examples; the MLP
-    trains on 200,000 of them on the device; then plain and learned batches run from the same seeds, timed with CUDA
-    events, and their ESS/s (sigma; median over rows of f) and posterior agreement are reported."""
+    nskip 1000, ndpost 1000.  A plain batch (other seeds) supplies accepted births as training examples of both
+    heads: the variable head (node and tree features) and the cut head (node features with the residual mean and
+    spread of the node's rows, drawn after the pass); each trains on up to 200,000 of them on the device.  Then, for 4
+    seed sets, plain and learned batches (both heads, mix 0.5) run from the same seeds, each timed with CUDA events
+    after an untimed run; ESS/s (sigma; median over 256 sampled rows of f) and the posterior agreement are reported
+    per set, with the mean learned/plain ratio and a 95% t-interval over the sets, for both heads and for the variable
+    head alone; seed set 0 also runs the cut head alone."""
     import torch
     import fastbart_b200 as F
     from fastbart_b200 import diagnostics, workloads as W
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    S = NSKIP + NDPOST
+    nskip, ndpost = NSKIP, LRN_NDPOST
+    S = nskip + ndpost
+    base = W.friedman_large(nchains=LRN_CHAINS, n=LRN_N, p=LRN_P, seed=0, nskip=nskip, ndpost=ndpost, ntree=NTREE)
 
     def chains(seed0):
-        out = W.friedman_large(nchains=LRN_CHAINS, n=LRN_N, p=LRN_P, seed=0, nskip=NSKIP, ndpost=NDPOST, ntree=NTREE)
-        for k, c in enumerate(out):
-            c["seed"] = seed0 + k
+        out = []
+        for k, c in enumerate(base):
+            d = dict(c)
+            d["seed"] = seed0 + k
+            out.append(d)
         return out
 
     stream = torch.cuda.current_stream()
 
-    def timed(b, steps, warmup):
-        for _ in range(warmup):
-            b.run(stream.cuda_stream)
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        for a, c in evs:
-            a.record(stream)
-            b.run(stream.cuda_stream)
-            c.record(stream)
+    def timed(b):
+        b.run(stream.cuda_stream)
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        b.run(stream.cuda_stream)
+        c.record(stream)
         torch.cuda.synchronize()
-        return sum(a.elapsed_time(c) for a, c in evs) / 1000.0 / steps
+        return a.elapsed_time(c) / 1000.0
 
-    col = F.Batch(chains(900), NSKIP, NDPOST)
+    col = F.Batch(chains(900), nskip, 100)
     col.collect(2 * LRN_TRAIN)
     col.run(stream.cuda_stream)
     col.sync()
     x, y, m, births = col.training_data()
+    cx, cc, clo, chi = col.cut_training_data()
     col.close()
     k = min(LRN_TRAIN, len(y))
     t = time.perf_counter()
-    model, losses = F.train_proposal(x[:k], y[:k], m[:k], epochs=10, batch=1024, lr=3e-3, seed=1)
+    vmodel, vloss = F.train_proposal(x[:k], y[:k], m[:k], epochs=10, batch=1024, lr=3e-3, seed=1)
+    cmodel, closs = F.train_cut_proposal(cx[:k], cc[:k], clo[:k], chi[:k], epochs=10, batch=1024, lr=3e-3, seed=2)
     train_s = time.perf_counter() - t
-    res = {}
-    steps = max(1, min(args.steps, 2))
-    # the ceiling of a split-variable proposal here: a bias-only model that knows the signal predictors (logit +4 on
-    # x1..x5, 0 elsewhere: 81% of the model's mass on the signal), mixed 90% -- no trained network can beat it
-    z64 = np.zeros(64, np.float32)
-    b3 = np.zeros(32, np.float32)
-    b3[:5] = 4.0
-    ceiling = dict(w1=np.zeros((64, 98), np.uint16), b1=z64, w2=np.zeros((64, 64), np.uint16), b2=z64,
-                   w3=np.zeros((32, 64), np.uint16), b3=b3, mix=0.9)
-    for name, mdl in (("plain", None), ("learned", dict(model, mix=0.5)), ("signal_ceiling", ceiling)):
-        b = F.Batch(chains(100), NSKIP, NDPOST)
-        if mdl is not None:
-            b.set_proposal(mdl)
-        sec = timed(b, steps, 1)
+
+    def measure(seed0, vm, cm):
+        b = F.Batch(chains(seed0), nskip, ndpost)
+        if vm is not None:
+            b.set_proposal(dict(vm, mix=0.5))
+        if cm is not None:
+            b.set_cut_proposal(dict(cm, mix=0.5))
+        sec = timed(b)
+        info = b.launch_info()
         outs = b.download(trees=False)
         b.close()
-        es = [diagnostics.chain_ess(o["sigma"][NSKIP:], o["yhat"]) for o in outs]
-        res[name] = {"seconds_per_batch": sec, "chain_sweeps_per_s": LRN_CHAINS * S / sec,
-                     "ess_sigma_per_s": float(sum(e["sigma"] for e in es) / sec),
-                     "ess_f_median_per_s": float(sum(e["f_median"] for e in es) / sec),
-                     "births": int(sum(o["moves"][0] for o in outs)),
-                     "fmean": np.mean([o["yhat_mean"] for o in outs], axis=0),
-                     "sigma": float(np.mean([o["sigma"][NSKIP:].mean() for o in outs]))}
-    corr = float(np.corrcoef(res["plain"]["fmean"], res["learned"]["fmean"])[0, 1])
-    sig = res["learned"]["sigma"] / res["plain"]["sigma"]
-    ceil = {"ess_f_ratio": res["signal_ceiling"]["ess_f_median_per_s"] / res["plain"]["ess_f_median_per_s"],
-            "ess_sigma_ratio": res["signal_ceiling"]["ess_sigma_per_s"] / res["plain"]["ess_sigma_per_s"],
-            "corr_fmean": float(np.corrcoef(res["plain"]["fmean"], res["signal_ceiling"]["fmean"])[0, 1]),
-            "births": res["signal_ceiling"]["births"],
-            "what": "bias-only model, logit +4 on x1..x5, mix 0.9: what a perfect split-variable proposal gives"}
-    for r in res.values():
-        del r["fmean"]
-    line = {"metric": LRN_METRIC, "value": res["learned"]["ess_f_median_per_s"] / res["plain"]["ess_f_median_per_s"],
-            "unit": "x (ESS/s of f, learned / plain)", "n_gpus": 1, "steps": steps, "warmup": 1,
-            "ms_per_step": 1000 * res["learned"]["seconds_per_batch"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int64-fixed+f32+f64 (MLP bf16/f32)", "data": "synthetic",
+        es = [diagnostics.chain_ess(o["sigma"][nskip:], o["yhat"]) for o in outs]
+        r = {"seconds_per_batch": sec, "chain_sweeps_per_s": LRN_CHAINS * S / sec,
+             "ess_sigma_per_s": float(sum(e["sigma"] for e in es) / sec),
+             "ess_f_median_per_s": float(sum(e["f_median"] for e in es) / sec),
+             "ess_sigma_mean": float(np.mean([e["sigma"] for e in es])),
+             "ess_f_median_mean": float(np.mean([e["f_median"] for e in es])),
+             "births": int(sum(o["moves"][0] for o in outs)), "deaths": int(sum(o["moves"][1] for o in outs)),
+             "launch": {"threads": info["threads"], "ctas_per_chain": info["cluster"]}}
+        fm = np.mean([o["yhat_mean"] for o in outs], axis=0)
+        sg = float(np.mean([o["sigma"][nskip:].mean() for o in outs]))
+        del outs
+        return r, fm, sg
+
+    sets = []
+    for si in range(LRN_SETS):
+        seed0 = 100 + 1000 * si
+        rp, fp, sp = measure(seed0, None, None)
+        rl, fl, sl = measure(seed0, vmodel, cmodel)
+        rv, fv, sv = measure(seed0, vmodel, None)
+        sets.append({"plain": rp, "learned": rl, "variable_head_only": rv,
+                     "ratio_f": rl["ess_f_median_per_s"] / rp["ess_f_median_per_s"],
+                     "ratio_sigma": rl["ess_sigma_per_s"] / rp["ess_sigma_per_s"],
+                     "ratio_f_variable_head": rv["ess_f_median_per_s"] / rp["ess_f_median_per_s"],
+                     "ratio_sigma_variable_head": rv["ess_sigma_per_s"] / rp["ess_sigma_per_s"],
+                     "corr_fmean": float(np.corrcoef(fp, fl)[0, 1]), "sigma_ratio": sl / sp,
+                     "corr_fmean_variable_head": float(np.corrcoef(fp, fv)[0, 1]), "sigma_ratio_variable_head": sv / sp})
+    ablation = {}
+    for name, vm, cm in (("cut_head_only", None, cmodel),):
+        r, _, _ = measure(100, vm, cm)
+        ablation[name] = {"ratio_f": r["ess_f_median_per_s"] / sets[0]["plain"]["ess_f_median_per_s"],
+                          "ratio_sigma": r["ess_sigma_per_s"] / sets[0]["plain"]["ess_sigma_per_s"],
+                          "chain_sweeps_per_s": r["chain_sweeps_per_s"], "births": r["births"]}
+
+    def ci(vals):
+        v = np.asarray(vals, dtype=np.float64)
+        half = 3.182 * v.std(ddof=1) / np.sqrt(len(v)) if len(v) > 1 else float("nan")   # t(0.975, 3 df)
+        return {"mean": float(v.mean()), "ci95": [float(v.mean() - half), float(v.mean() + half)],
+                "per_set": [float(a) for a in v]}
+
+    rf, rs = ci([x_["ratio_f"] for x_ in sets]), ci([x_["ratio_sigma"] for x_ in sets])
+    rfv, rsv = ci([x_["ratio_f_variable_head"] for x_ in sets]), ci([x_["ratio_sigma_variable_head"] for x_ in sets])
+    uniform_cut_loss = float(np.mean(np.log(chi[:k] - clo[:k] + 1.0)))
+    line = {"metric": LRN_METRIC, "value": rf["mean"], "unit": "x (ESS/s of f, learned / plain)", "n_gpus": 1,
+            "steps": 1, "warmup": 1, "ms_per_step": 1000 * sets[0]["learned"]["seconds_per_batch"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64-fixed+f32+f64 (MLP bf16/f32)", "data": "synthetic",
             "config": {"workload": "friedman_sparse_16x65536", "chains": LRN_CHAINS, "n": LRN_N, "p": LRN_P,
-                       "numcut": 255, "ntree": NTREE, "nskip": NSKIP, "ndpost": NDPOST, "mix": 0.5,
-                       "training_examples": int(k), "accepted_births_collected": int(births)},
-            "sigma_ratio": float(res["learned"]["ess_sigma_per_s"] / res["plain"]["ess_sigma_per_s"]),
-            "plain": res["plain"], "learned": res["learned"],
-            "training": {"seconds": train_s, "epochs": 10, "loss_first": float(losses[0]),
-                         "loss_last": float(losses[-1]), "uniform_loss": float(np.log(LRN_P)),
-                         "signal_fraction_of_births": float(np.mean(y[:k] < 5))},
-            "agreement": {"corr_fmean": corr, "sigma_ratio": float(sig)}, "signal_ceiling": ceil,
-            "gpu_launches": 3 * steps}
+                       "numcut": 255, "ntree": NTREE, "nskip": nskip, "ndpost": ndpost, "mix": 0.5,
+                       "seed_sets": LRN_SETS, "training_examples": int(k), "accepted_births_collected": int(births)},
+            "ratio_f": rf, "ratio_sigma": rs, "ratio_f_variable_head": rfv, "ratio_sigma_variable_head": rsv,
+            "sets": sets, "ablation_seed_set_0": ablation,
+            "training": {"seconds": train_s, "epochs": 10,
+                         "variable_head": {"loss_first": float(vloss[0]), "loss_last": float(vloss[-1]),
+                                           "uniform_loss": float(np.log(LRN_P)),
+                                           "signal_fraction_of_births": float(np.mean(y[:k] < 5))},
+                         "cut_head": {"loss_first": float(closs[0]), "loss_last": float(closs[-1]),
+                                      "uniform_loss": uniform_cut_loss}},
+            "agreement": {"corr_fmean_min": min(x_["corr_fmean"] for x_ in sets),
+                          "sigma_ratio_range": [min(x_["sigma_ratio"] for x_ in sets),
+                                                max(x_["sigma_ratio"] for x_ in sets)]},
+            "gpu_launches": 6 * LRN_SETS + 2 + 1}
     print(json.dumps(line), flush=True)
     return 0
 

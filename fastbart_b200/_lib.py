@@ -21,7 +21,8 @@ EXPORTS = ["fb_last_error", "fb_version", "fb_fit_batch", "fb_batch_create", "fb
            "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass",
            "fb_batch_set_proposal", "fb_batch_collect", "fb_batch_training_data", "fb_train_proposal",
            "fb_mlp_loss_grad", "fb_autotune", "fb_cut_codes", "fb_trees_text_gpu", "fb_batch_trees_text",
-           "fb_release_cached_memory", "fb_batch_autotuned"]
+           "fb_release_cached_memory", "fb_batch_autotuned", "fb_batch_set_cut_proposal",
+           "fb_batch_cut_training_data", "fb_train_cut_proposal", "fb_cut_loss_grad"]
 
 MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
 
@@ -29,6 +30,15 @@ MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
 class ProposalModel(C.Structure):
     _fields_ = [("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
                 ("w3", C.c_void_p), ("b3", C.c_void_p), ("mix", C.c_double)]
+
+
+class CutModel(C.Structure):
+    _fields_ = [("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_void_p), ("emb", C.c_void_p), ("be", C.c_void_p),
+                ("mix", C.c_double)]
+
+
+CUT_IN, CUT_H, CUT_E, CUT_BINS = 40, 64, 16, 255
 
 
 class TrainOptions(C.Structure):
@@ -98,6 +108,10 @@ def lib() -> C.CDLL:
         L.fb_batch_destroy.argtypes = [vp]
         L.fb_batch_destroy.restype = None
         L.fb_batch_autotuned.argtypes = [vp]
+        L.fb_batch_set_cut_proposal.argtypes = [vp, C.POINTER(CutModel)]
+        L.fb_batch_cut_training_data.argtypes = [vp, vp, vp, vp, vp, i, C.POINTER(i)]
+        L.fb_train_cut_proposal.argtypes = [vp, vp, vp, vp, i, C.POINTER(TrainOptions), C.POINTER(CutModel)] + [vp] * 9
+        L.fb_cut_loss_grad.argtypes = [C.POINTER(CutModel), vp, vp, vp, vp, i, i, C.POINTER(d)] + [vp] * 8
         L.fb_fbart.argtypes = [vp, i, i, vp, vp, vp, vp, vp, i, i, i, d, d, d, d, C.c_uint64, i, d, vp, vp, vp, vp,
                                C.c_char_p, sz, C.POINTER(sz), vp]
         L.fb_trees_text.argtypes = [vp, i, i, i, C.c_char_p, sz]

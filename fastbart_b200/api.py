@@ -147,6 +147,24 @@ class Batch:
         ms = _model_struct(model, self._keep)
         check(_lib.lib().fb_batch_set_proposal(self._h, C.byref(ms)))
 
+    def set_cut_proposal(self, model: dict | None):
+        """Learned cutpoint proposal for the next runs (see `train_cut_proposal`); None restores BART's uniform cut."""
+        if model is None:
+            check(_lib.lib().fb_batch_set_cut_proposal(self._h, None))
+            return
+        ms = _cut_struct(model, self._keep)
+        check(_lib.lib().fb_batch_set_cut_proposal(self._h, C.byref(ms)))
+
+    def cut_training_data(self) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+        """(x [k][40] float32, cut [k], lo [k], hi [k] int32) of the births training_data() returns, same order."""
+        cap = getattr(self, "_cap", 0)
+        x = np.zeros((max(cap, 1), _lib.CUT_IN), np.float32)
+        c, lo, hi = (np.zeros(max(cap, 1), np.int32) for _ in range(3))
+        cnt = C.c_int()
+        check(_lib.lib().fb_batch_cut_training_data(self._h, ptr(x), ptr(c), ptr(lo), ptr(hi), cap, C.byref(cnt)))
+        k = min(cnt.value, cap)
+        return x[:k], c[:k], lo[:k], hi[:k]
+
     def collect(self, capacity: int):
         """Collect the accepted births of the next runs as training examples (at most `capacity` per run)."""
         self._cap = int(capacity)
@@ -186,6 +204,56 @@ def _model_struct(model: dict, keep: list) -> _lib.ProposalModel:
     ms = _lib.ProposalModel(*arrs, float(model.get("mix", 0.5)))
     keep.append(ms)
     return ms
+
+
+CUT_KEYS = (("w1", np.uint16), ("b1", np.float32), ("w2", np.uint16), ("b2", np.float32), ("w3", np.uint16),
+            ("b3", np.float32), ("emb", np.uint16), ("be", np.float32))
+
+
+def _cut_struct(model: dict, keep: list) -> _lib.CutModel:
+    arrs = []
+    for k, dt in CUT_KEYS:
+        a = np.ascontiguousarray(model[k], dtype=dt)
+        keep.append(a)
+        arrs.append(a.ctypes.data)
+    ms = _lib.CutModel(*arrs, float(model.get("mix", 0.5)))
+    keep.append(ms)
+    return ms
+
+
+def _cut_shapes() -> dict:
+    H, I, E, NB = _lib.CUT_H, _lib.CUT_IN, _lib.CUT_E, _lib.CUT_BINS
+    return dict(w1=(H, I), b1=(H,), w2=(H, H), b2=(H,), w3=(E, H), b3=(E,), emb=(NB, E), be=(NB,))
+
+
+def train_cut_proposal(x, c, lo, hi, epochs: int = 10, batch: int = 512, lr: float = 2e-3, seed: int = 0,
+                       init: dict | None = None, mix: float = 0.5, device: int = 0) -> tuple[dict, np.ndarray]:
+    """Trains the cut head on the device (softmax cross-entropy over each example's cut range, Adam); returns
+    (model, epoch losses)."""
+    x = np.ascontiguousarray(x, np.float32)
+    c, lo, hi = (np.ascontiguousarray(a, np.int32) for a in (c, lo, hi))
+    out = {k: np.zeros(sh, dtype=dt) for (k, dt), sh in zip(CUT_KEYS, _cut_shapes().values())}
+    losses = np.zeros(int(epochs))
+    keep: list = []
+    opt = _lib.TrainOptions(int(epochs), int(batch), float(lr), int(seed) & 0xFFFFFFFFFFFFFFFF, int(device))
+    ini = C.byref(_cut_struct(init, keep)) if init is not None else None
+    check(_lib.lib().fb_train_cut_proposal(ptr(x), ptr(c), ptr(lo), ptr(hi), len(c), C.byref(opt), ini,
+                                           *(ptr(out[k]) for k, _ in CUT_KEYS), ptr(losses)))
+    out["mix"] = float(mix)
+    return out, losses
+
+
+def cut_loss_grad(model: dict, x, c, lo, hi, device: int = 0) -> tuple[float, dict]:
+    """One forward/backward of the cut head's training kernels: mean loss and gradients (FP32)."""
+    x = np.ascontiguousarray(x, np.float32)
+    c, lo, hi = (np.ascontiguousarray(a, np.int32) for a in (c, lo, hi))
+    keep: list = []
+    ms = _cut_struct(model, keep)
+    g = {k: np.zeros(sh, np.float32) for k, sh in _cut_shapes().items()}
+    loss = C.c_double()
+    check(_lib.lib().fb_cut_loss_grad(C.byref(ms), ptr(x), ptr(c), ptr(lo), ptr(hi), len(c), int(device),
+                                      C.byref(loss), *(ptr(g[k]) for k, _ in CUT_KEYS)))
+    return loss.value, g
 
 
 def _empty_model() -> dict:

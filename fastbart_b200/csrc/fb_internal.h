@@ -74,7 +74,7 @@ struct DBufs {
   int nchains;
   int m_max;
   int n_pad_max;                   // rows of one CTA's slice (shared-memory capacity)
-  int rows_in_smem;
+  int rows_in_smem;                // 1: residuals and weights in shared memory, 2: residuals only, 0: neither
   int cluster;                     // CTAs per chain (a thread-block cluster when > 1)
   // learned split-variable proposal (null mvar: BART's uniform proposal): the model's weight image (see MIMG_*),
   // staged in shared memory behind the sampler's own layout when model_smem is set, else read from global memory
@@ -90,9 +90,35 @@ struct DBufs {
   unsigned* train_mask;
   int* train_count;
   int train_cap;
+  // learned cutpoint proposal (null cimg: BART's uniform cut): the cut head's weight image (see CIMG_*), staged in
+  // shared memory when cut_smem is set, else read from global memory; a birth's cut is then drawn after the pass
+  const uint32_t* cimg;
+  int cut_smem;
+  double cmix;                             // probability of the cut head's component, in (0, 1]
+  // the cut examples of the collected births (train_cx null: none): per tree, the features and (cut, lo, hi) of its
+  // accepted birth of the current step, copied to the example arrays with the variable example
+  float* cfeat;                            // [trees][CUT_IN]
+  int* cinfo;                              // [trees][3]
+  float* train_cx;                         // [train_cap][CUT_IN]
+  int* train_c;
+  int* train_lo;
+  int* train_hi;
 };
 
-size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster);
+// learned cutpoint proposal: CUT_IN node features (with the node's residual mean and spread) -> CUT_H -> CUT_H ->
+// CUT_E, then one logit per cutpoint index c < CUT_BINS: be[c] + emb[c] . e
+constexpr int CUT_IN = 40, CUT_H = 64, CUT_E = 16, CUT_BINS = 255;
+// the sampler's image of a cut head (32-bit words): BF16 pairs row by row, rows padded to an odd word count (distinct
+// banks for the threads reading one row each), then the FP32 biases b1 [H], b2 [H], b3 [E], be [BINS]
+constexpr int CIMG_W1S = CUT_IN / 2 + 1, CIMG_W2S = CUT_H / 2 + 1, CIMG_ES = CUT_E / 2 + 1;
+constexpr int CIMG_W2 = CUT_H * CIMG_W1S, CIMG_W3 = CIMG_W2 + CUT_H * CIMG_W2S, CIMG_EMB = CIMG_W3 + CUT_E * CIMG_W2S;
+constexpr int CIMG_B = CIMG_EMB + CUT_BINS * CIMG_ES;
+constexpr int CIMG_WORDS = (CIMG_B + 2 * CUT_H + CUT_E + CUT_BINS + 3) / 4 * 4;
+constexpr int CUT_NPARAM = CUT_H * CUT_IN + CUT_H + CUT_H * CUT_H + CUT_H + CUT_E * CUT_H + CUT_E + CUT_BINS * CUT_E +
+                           CUT_BINS;
+
+// cut: the layout of a launch with the learned cut proposal (its per-tree ratios, histograms and head)
+size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster, int cut = 0);
 // Tree text (without its header) of ntrees consecutive device trees: *total receives its length; with d_out
 // non-null, *d_out is allocated (cudaMalloc, caller frees) and receives the text.  0 on success.
 int trees_text_device(const uint64_t* d_trees, long long ntrees, char** d_out, unsigned long long* total,
@@ -164,6 +190,16 @@ int mlp_grad_launch(const MlpParams& P, const float* X, const int* Y, const unsi
 // Adam step `step` (1-based) with gradient grad * inv_batch; refreshes the BF16 weights of P
 int mlp_adam_launch(float* p, float* m1, float* m2, const float* g, float inv_batch, float lr, int step,
                     const MlpParams& P, void* stream);
+
+// Training of the cut head (mlp.cu); flat FP32 parameters in the order of CUT_NPARAM (see mlp.cu)
+struct CutParams {
+  uint16_t* w1; uint16_t* w2; uint16_t* w3; uint16_t* emb;   // BF16 weights (device)
+  const float* b1; const float* b2; const float* b3; const float* be;
+};
+int cut_grad_launch(const CutParams& P, const float* X, const int* Yc, const int* LO, const int* HI, const int* idx,
+                    int B, float* grad, float* loss, void* stream);
+int cut_adam_launch(float* p, float* m1, float* m2, const float* g, float inv_batch, float lr, int step,
+                    const CutParams& P, void* stream);
 
 // cutpoint codes of p columns of n values (x [p][n], cutpoints cuts[cutoff[v] .. cutoff[v + 1]), q [p][n])
 int launch_cut_codes(const double* x, int n, int p, const double* cuts, const int* cutoff, uint8_t* q, void* stream);

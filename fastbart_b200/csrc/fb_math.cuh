@@ -22,7 +22,7 @@
 namespace fbm {
 
 enum : uint32_t { TAG_PROP = 1, TAG_MH = 2, TAG_MU = 3, TAG_SIG_N = 4, TAG_SIG_U = 5, TAG_Z_N = 6, TAG_Z_E = 7,
-                  TAG_PROP2 = 8 };
+                  TAG_PROP2 = 8, TAG_PROP3 = 9 };
 constexpr uint32_t INIT_SWEEP = 0xFFFFFFFFu;
 
 struct U4 { uint32_t x, y, z, w; };

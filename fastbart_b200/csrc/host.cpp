@@ -144,7 +144,10 @@ struct fb_batch {
   cudaStream_t stream = nullptr;
   void* model_mem = nullptr;   // learned proposal weights (owned; also listed in allocs)
   int* mvar = nullptr;         // learned proposal: per-tree choices of the current sweep (owned)
-  size_t smem_model = 0;       // the sampler's shared memory with the proposal model's weight image
+  size_t smem_model = 0;       // the sampler's shared memory of model, cut and collecting launches (update_launch)
+  int rows_plain = 1;          // rows in shared memory in the plain layout
+  void* cut_mem = nullptr;     // the cut head's weight image (owned; also listed in allocs)
+  int cut_cap = 0;             // allocated capacity of the cut-example buffers
   double* mcorr = nullptr;
   int cluster = 1;             // CTAs per chain
   int slice_rows = 0;          // rows of one CTA's slice (shared-memory capacity)
@@ -192,6 +195,46 @@ std::string batch_signature(const fb_chain* chains, int nchains, int device) {
   char buf[160];
   std::snprintf(buf, sizeof buf, "%d:%d:%lld:%lld:%d:%d:%d:%d", device, nchains, rows, trees, nmax, mmax, pmax, probit);
   return buf;
+}
+
+// Shared memory and staging of the batch's model, cut and collecting launches: the cut layout (per-tree ratios,
+// scratch, one more bin row) when a cut head or collection is set, the proposal model's image behind the layout when
+// the bins cannot hold it, then the cut head's image, each staged only while every CTA of the launch stays resident
+// (else read from global memory); rows move to global memory when the cut layout cannot keep them in shared memory.
+fb_status update_launch(fb_batch* b) {
+  DBufs& d = b->d;
+  const bool special = d.mvar || d.cimg || d.train_cap > 0;
+  d.rows_in_smem = b->rows_plain;
+  d.model_smem = 0; d.cut_smem = 0;
+  b->smem_model = b->smem;
+  if (!special) return FB_OK;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device) != cudaSuccess) optin = 0;
+  const int cutl = (d.cimg || d.train_cap > 0) ? 1 : 0;
+  size_t base = sampler_smem_bytes(b->threads, d.m_max, d.n_pad_max, d.rows_in_smem, b->cluster, cutl);
+  auto resident = [&](size_t sm) {
+    return sm <= (size_t)optin && sampler_max_grid(b->threads, sm, b->device, b->gmax, b->cluster) >= b->grid;
+  };
+  if (!resident(base) && d.rows_in_smem == 1) {   // the weights to global memory
+    d.rows_in_smem = 2;
+    base = sampler_smem_bytes(b->threads, d.m_max, d.n_pad_max, 2, b->cluster, cutl);
+  }
+  if (!resident(base) && d.rows_in_smem == 2) {   // and the residuals
+    d.rows_in_smem = 0;
+    base = sampler_smem_bytes(b->threads, d.m_max, d.n_pad_max, 0, b->cluster, cutl);
+  }
+  if (!resident(base)) return fail(FB_ERR_LIMIT, "shared memory %zu of the learned proposal's layout does not fit", base);
+  size_t sm = (base + 15) / 16 * 16;
+  if (d.mvar && !sampler_bins_hold_model(b->threads) && resident(sm + 4 * (size_t)MIMG_WORDS)) {
+    d.model_smem = 1;
+    sm += 4 * (size_t)MIMG_WORDS;
+  }
+  if (d.cimg && resident(sm + 4 * (size_t)CIMG_WORDS)) {
+    d.cut_smem = 1;
+    sm += 4 * (size_t)CIMG_WORDS;
+  }
+  b->smem_model = sm;
+  return FB_OK;
 }
 
 // whether an automatic launch shape (threads = cluster = 0) is picked by the autotuner (default) or by the measured
@@ -326,6 +369,7 @@ fb_status fb_batch_create(const fb_chain* chains, int nchains, const fb_options*
   if (maxgrid <= 0) { delete b; return fail(FB_ERR_CUDA, "sampler kernel cannot be resident with %zu bytes of shared memory", smem); }
   b->cluster = CS;
   b->threads = T; b->smem = smem; b->grid = std::min(nchains * CS, maxgrid); b->gmax = gmax;
+  b->rows_plain = rows_in_smem; b->smem_model = smem;
   b->spl = opt->sweeps_per_launch > 0 ? opt->sweeps_per_launch : S;
   b->launches = (S + b->spl - 1) / b->spl;
 
@@ -391,7 +435,8 @@ fb_status fb_batch_run(fb_batch* b, void* stream) {
     return fail(FB_ERR_CUDA, "cannot reset the training-example counter");
   for (int it0 = 0; it0 < S; it0 += b->spl) {
     const int it1 = std::min(S, it0 + b->spl);
-    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, b->d.mvar ? b->smem_model : b->smem, b->gmax, b->cluster,
+    const bool special = b->d.mvar || b->d.cimg || b->d.train_cap > 0;
+    if (launch_sampler(b->d, it0, it1, b->threads, b->grid, special ? b->smem_model : b->smem, b->gmax, b->cluster,
                        stream) != 0)
       return fail(FB_ERR_CUDA, "sampler launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
@@ -449,7 +494,7 @@ fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
   CK(cudaSetDevice(b->device));
   if (!model || model->mix <= 0.0) {
     b->d.mvar = nullptr; b->d.mcorr = nullptr; b->d.mix = 0.0;
-    return FB_OK;
+    return update_launch(b);
   }
   if (!model->w1 || !model->b1 || !model->w2 || !model->b2 || !model->w3 || !model->b3)
     return fail(FB_ERR_ARG, "every weight and bias array of the model is required");
@@ -475,17 +520,9 @@ fb_status fb_batch_set_proposal(fb_batch* b, const fb_proposal_model* model) {
   CK(cudaStreamSynchronize(0));
   CK(cudaMemcpy(b->model_mem, img.data(), 4 * img.size(), cudaMemcpyHostToDevice));
   b->d.mimg = static_cast<const uint32_t*>(b->model_mem);
-  // the sampler stages the image in its pass bins when they are large enough (wide CTAs); otherwise behind its
-  // shared memory when that keeps every CTA of the launch resident, else it reads the image from global memory
-  int optin = 0;
-  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device) != cudaSuccess) optin = 0;
-  const size_t with = (b->smem + 15) / 16 * 16 + 4 * (size_t)MIMG_WORDS;
-  b->d.model_smem = !sampler_bins_hold_model(b->threads) && with <= (size_t)optin &&
-                    sampler_max_grid(b->threads, with, b->device, b->gmax, b->cluster) >= b->grid;
-  b->smem_model = b->d.model_smem ? with : b->smem;
   b->d.mix = model->mix;
   b->d.mvar = b->mvar; b->d.mcorr = b->mcorr;
-  return FB_OK;
+  return update_launch(b);
 }
 
 fb_status fb_batch_collect(fb_batch* b, int capacity) {
@@ -506,7 +543,74 @@ fb_status fb_batch_collect(fb_batch* b, int capacity) {
     b->d.train_mask = static_cast<unsigned*>(tm); b->d.train_count = static_cast<int*>(tc);
     b->collect_cap = capacity;
   }
+  if (capacity > b->cut_cap) {   // the cut examples of the same births
+    float* cf = b->alloc<float>((size_t)CUT_IN * b->ntrees);
+    int* ci = b->alloc<int>((size_t)3 * b->ntrees);
+    float* cx = b->alloc<float>((size_t)CUT_IN * capacity);
+    int* cc = b->alloc<int>((size_t)capacity);
+    int* clo = b->alloc<int>((size_t)capacity);
+    int* chi = b->alloc<int>((size_t)capacity);
+    if (!cf || !ci || !cx || !cc || !clo || !chi) return fail(FB_ERR_CUDA, "out of device memory");
+    CK(cudaStreamSynchronize(0));
+    b->d.cfeat = cf; b->d.cinfo = ci; b->d.train_cx = cx; b->d.train_c = cc; b->d.train_lo = clo; b->d.train_hi = chi;
+    b->cut_cap = capacity;
+  }
   b->d.train_cap = capacity;
+  return update_launch(b);
+}
+
+fb_status fb_batch_set_cut_proposal(fb_batch* b, const fb_cut_model* model) {
+  if (!b) return fail(FB_ERR_ARG, "batch is NULL");
+  CK(cudaSetDevice(b->device));
+  if (!model || model->mix <= 0.0) {
+    b->d.cimg = nullptr; b->d.cmix = 0.0;
+    return update_launch(b);
+  }
+  if (!model->w1 || !model->b1 || !model->w2 || !model->b2 || !model->w3 || !model->b3 || !model->emb || !model->be)
+    return fail(FB_ERR_ARG, "every weight and bias array of the cut model is required");
+  if (!(model->mix <= 1.0)) return fail(FB_ERR_ARG, "mix must be in (0, 1]");
+  if (b->threads < 256) return fail(FB_ERR_LIMIT, "the cut proposal needs CTAs of at least 256 threads (%d)", b->threads);
+  // the sampler's image (CIMG_* in fb_internal.h): BF16 pairs row by row in odd-length rows, then the biases
+  std::vector<uint32_t> img(CIMG_WORDS, 0u);
+  auto pack = [&](const uint16_t* w, int rows, int cols, int base, int stride) {
+    for (int o = 0; o < rows; o++)
+      for (int k = 0; k < cols; k++) {
+        const uint32_t h = w[o * cols + k];
+        img[base + o * stride + k / 2] |= (k & 1) ? (h << 16) : h;
+      }
+  };
+  pack(model->w1, CUT_H, CUT_IN, 0, CIMG_W1S);
+  pack(model->w2, CUT_H, CUT_H, CIMG_W2, CIMG_W2S);
+  pack(model->w3, CUT_E, CUT_H, CIMG_W3, CIMG_W2S);
+  pack(model->emb, CUT_BINS, CUT_E, CIMG_EMB, CIMG_ES);
+  std::memcpy(img.data() + CIMG_B, model->b1, 4 * CUT_H);
+  std::memcpy(img.data() + CIMG_B + CUT_H, model->b2, 4 * CUT_H);
+  std::memcpy(img.data() + CIMG_B + 2 * CUT_H, model->b3, 4 * CUT_E);
+  std::memcpy(img.data() + CIMG_B + 2 * CUT_H + CUT_E, model->be, 4 * CUT_BINS);
+  if (!b->cut_mem && !(b->cut_mem = b->alloc<uint32_t>(img.size()))) return fail(FB_ERR_CUDA, "out of device memory");
+  CK(cudaStreamSynchronize(0));
+  CK(cudaMemcpy(b->cut_mem, img.data(), 4 * img.size(), cudaMemcpyHostToDevice));
+  b->d.cimg = static_cast<const uint32_t*>(b->cut_mem);
+  b->d.cmix = model->mix;
+  return update_launch(b);
+}
+
+fb_status fb_batch_cut_training_data(fb_batch* b, float* x, int* c, int* lo, int* hi, int cap, int* count) {
+  if (!b || !count) return fail(FB_ERR_ARG, "batch and count are required");
+  CK(cudaSetDevice(b->device));
+  *count = 0;
+  if (b->d.train_cap <= 0 || !b->d.train_cx) return FB_OK;
+  CK(cudaStreamSynchronize(b->stream));
+  int total = 0;
+  CK(cudaMemcpy(&total, b->d.train_count, sizeof(int), cudaMemcpyDeviceToHost));
+  *count = total;
+  const int k = std::min(std::min(total, b->d.train_cap), std::max(cap, 0));
+  if (k > 0) {
+    if (x) CK(cudaMemcpy(x, b->d.train_cx, sizeof(float) * CUT_IN * (size_t)k, cudaMemcpyDeviceToHost));
+    if (c) CK(cudaMemcpy(c, b->d.train_c, sizeof(int) * (size_t)k, cudaMemcpyDeviceToHost));
+    if (lo) CK(cudaMemcpy(lo, b->d.train_lo, sizeof(int) * (size_t)k, cudaMemcpyDeviceToHost));
+    if (hi) CK(cudaMemcpy(hi, b->d.train_hi, sizeof(int) * (size_t)k, cudaMemcpyDeviceToHost));
+  }
   return FB_OK;
 }
 
@@ -1110,6 +1214,32 @@ struct MlpJob {
   }
 };
 
+// Examples in a canonical order (sorted by their bytes: features, then label and mask), so that training depends on
+// its seed only, whatever order the sampler's CTAs collected the examples in.
+std::vector<int> canonical_order(const float* x, int width, const int* y, const uint32_t* mask, const int* lo,
+                                 const int* hi, int count) {
+  std::vector<int> ord(count);
+  for (int k = 0; k < count; k++) ord[k] = k;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+    const int c = std::memcmp(x + (size_t)a * width, x + (size_t)b * width, sizeof(float) * (size_t)width);
+    if (c != 0) return c < 0;
+    if (y[a] != y[b]) return y[a] < y[b];
+    if (mask && mask[a] != mask[b]) return mask[a] < mask[b];
+    if (lo && lo[a] != lo[b]) return lo[a] < lo[b];
+    if (hi && hi[a] != hi[b]) return hi[a] < hi[b];
+    return false;
+  });
+  return ord;
+}
+
+fb_status check_cut_examples(const float* x, const int* c, const int* lo, const int* hi, int count) {
+  if (!x || !c || !lo || !hi || count < 1) return fail(FB_ERR_ARG, "x, c, lo, hi and count >= 1 are required");
+  for (int k = 0; k < count; k++)
+    if (lo[k] < 0 || hi[k] >= CUT_BINS || lo[k] > hi[k] || c[k] < lo[k] || c[k] > hi[k])
+      return fail(FB_ERR_ARG, "example %d: cut %d is not in its range [%d, %d]", k, c[k], lo[k], hi[k]);
+  return FB_OK;
+}
+
 fb_status check_examples(const float* x, const int* y, const uint32_t* mask, int count) {
   if (!x || !y || !mask || count < 1) return fail(FB_ERR_ARG, "x, y, mask and count >= 1 are required");
   for (int k = 0; k < count; k++)
@@ -1164,9 +1294,19 @@ fb_status fb_train_proposal(const float* x, const int* y, const uint32_t* mask, 
       !job.alloc(&didx, count) || !job.alloc(&dp, MLP_NPARAM) || !job.alloc(&dm1, MLP_NPARAM) ||
       !job.alloc(&dm2, MLP_NPARAM) || !job.alloc(&dg, MLP_NPARAM) || !job.alloc(&dl, 1) || !job.alloc(&dw, W.size()))
     return fail(FB_ERR_CUDA, "out of device memory");
-  CK(cudaMemcpy(dx, x, sizeof(float) * MLP_IN * (size_t)count, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dy, y, sizeof(int) * (size_t)count, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dmask, mask, sizeof(unsigned) * (size_t)count, cudaMemcpyHostToDevice));
+  {   // the examples in canonical order
+    const std::vector<int> ord = canonical_order(x, MLP_IN, y, mask, nullptr, nullptr, count);
+    std::vector<float> xs((size_t)count * MLP_IN);
+    std::vector<int> ys(count);
+    std::vector<unsigned> ms(count);
+    for (int k = 0; k < count; k++) {
+      std::memcpy(xs.data() + (size_t)k * MLP_IN, x + (size_t)ord[k] * MLP_IN, sizeof(float) * MLP_IN);
+      ys[k] = y[ord[k]]; ms[k] = mask[ord[k]];
+    }
+    CK(cudaMemcpy(dx, xs.data(), sizeof(float) * MLP_IN * (size_t)count, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dy, ys.data(), sizeof(int) * (size_t)count, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dmask, ms.data(), sizeof(unsigned) * (size_t)count, cudaMemcpyHostToDevice));
+  }
   CK(cudaMemcpy(dp, P.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dw, W.data(), sizeof(uint16_t) * W.size(), cudaMemcpyHostToDevice));
   CK(cudaMemset(dm1, 0, sizeof(float) * MLP_NPARAM));
@@ -1248,6 +1388,170 @@ fb_status fb_mlp_loss_grad(const fb_proposal_model* model, const float* x, const
   auto put = [&](float* dst, size_t off, size_t n) { if (dst) for (size_t k = 0; k < n; k++) dst[k] = G[off + k] * inv; };
   put(gw1, 0, kN1); put(gb1, kOffB1, MLP_H); put(gw2, kOffW2, kN2); put(gb2, kOffB2, MLP_H);
   put(gw3, kOffW3, kN3); put(gb3, kOffB3, MLP_OUT);
+  return FB_OK;
+}
+
+namespace {
+constexpr size_t cN1 = (size_t)CUT_H * CUT_IN, cN2 = (size_t)CUT_H * CUT_H, cN3 = (size_t)CUT_E * CUT_H,
+                 cN4 = (size_t)CUT_BINS * CUT_E;
+constexpr size_t cOffB1 = cN1, cOffW2 = cOffB1 + CUT_H, cOffB2 = cOffW2 + cN2, cOffW3 = cOffB2 + CUT_H,
+                 cOffB3 = cOffW3 + cN3, cOffE = cOffB3 + CUT_E, cOffBE = cOffE + cN4;
+static_assert(cOffBE + CUT_BINS == (size_t)CUT_NPARAM, "cut head parameter layout");
+bool cut_model_complete(const fb_cut_model* m) {
+  return m && m->w1 && m->b1 && m->w2 && m->b2 && m->w3 && m->b3 && m->emb && m->be;
+}
+// uploads the examples (canonical order when ordered) of the cut head's training
+struct CutData {
+  float* x = nullptr; int* c = nullptr; int* lo = nullptr; int* hi = nullptr;
+};
+bool upload_cut_examples(MlpJob& job, const float* x, const int* c, const int* lo, const int* hi, int count,
+                         bool ordered, CutData* d) {
+  if (!job.alloc(&d->x, (size_t)count * CUT_IN) || !job.alloc(&d->c, count) || !job.alloc(&d->lo, count) ||
+      !job.alloc(&d->hi, count))
+    return false;
+  std::vector<int> ord(count);
+  for (int k = 0; k < count; k++) ord[k] = k;
+  if (ordered) ord = canonical_order(x, CUT_IN, c, nullptr, lo, hi, count);
+  std::vector<float> xs((size_t)count * CUT_IN);
+  std::vector<int> cs(count), ls(count), hs(count);
+  for (int k = 0; k < count; k++) {
+    std::memcpy(xs.data() + (size_t)k * CUT_IN, x + (size_t)ord[k] * CUT_IN, sizeof(float) * CUT_IN);
+    cs[k] = c[ord[k]]; ls[k] = lo[ord[k]]; hs[k] = hi[ord[k]];
+  }
+  return cudaMemcpy(d->x, xs.data(), sizeof(float) * xs.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(d->c, cs.data(), sizeof(int) * (size_t)count, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(d->lo, ls.data(), sizeof(int) * (size_t)count, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(d->hi, hs.data(), sizeof(int) * (size_t)count, cudaMemcpyHostToDevice) == cudaSuccess;
+}
+}  // namespace
+
+fb_status fb_train_cut_proposal(const float* x, const int* c, const int* lo, const int* hi, int count,
+                                const fb_train_options* opt, const fb_cut_model* init, uint16_t* out_w1, float* out_b1,
+                                uint16_t* out_w2, float* out_b2, uint16_t* out_w3, float* out_b3, uint16_t* out_emb,
+                                float* out_be, double* losses) {
+  if (!opt || !out_w1 || !out_b1 || !out_w2 || !out_b2 || !out_w3 || !out_b3 || !out_emb || !out_be)
+    return fail(FB_ERR_ARG, "options and every output array are required");
+  if (opt->epochs < 1 || opt->batch < 1 || !(opt->lr > 0.0)) return fail(FB_ERR_ARG, "epochs, batch and lr must be > 0");
+  fb_status st = check_cut_examples(x, c, lo, hi, count);
+  if (st != FB_OK) return st;
+  if (init && !cut_model_complete(init)) return fail(FB_ERR_ARG, "every weight and bias array of the initial model is required");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  CK(cudaSetDevice(opt->device));
+  // initial parameters: the given model, or seeded uniform(-a, a), a = sqrt(6 / fan_in) (the last two layers scaled
+  // down, so that training starts near the uniform cut), zero biases
+  std::vector<float> P(CUT_NPARAM, 0.0f);
+  if (init) {
+    for (size_t k = 0; k < cN1; k++) P[k] = bf16_host(init->w1[k]);
+    for (size_t k = 0; k < cN2; k++) P[cOffW2 + k] = bf16_host(init->w2[k]);
+    for (size_t k = 0; k < cN3; k++) P[cOffW3 + k] = bf16_host(init->w3[k]);
+    for (size_t k = 0; k < cN4; k++) P[cOffE + k] = bf16_host(init->emb[k]);
+    for (int k = 0; k < CUT_H; k++) { P[cOffB1 + k] = init->b1[k]; P[cOffB2 + k] = init->b2[k]; }
+    for (int k = 0; k < CUT_E; k++) P[cOffB3 + k] = init->b3[k];
+    for (int k = 0; k < CUT_BINS; k++) P[cOffBE + k] = init->be[k];
+  } else {
+    std::mt19937_64 g(opt->seed);
+    std::uniform_real_distribution<float> u(-1.0f, 1.0f);
+    const float a1 = std::sqrt(6.0f / CUT_IN), a2 = std::sqrt(6.0f / CUT_H), a3 = 0.3f * std::sqrt(6.0f / CUT_H),
+                a4 = 0.3f * std::sqrt(6.0f / CUT_E);
+    for (size_t k = 0; k < cN1; k++) P[k] = bf16_host(bf16_round_host(a1 * u(g)));
+    for (size_t k = 0; k < cN2; k++) P[cOffW2 + k] = bf16_host(bf16_round_host(a2 * u(g)));
+    for (size_t k = 0; k < cN3; k++) P[cOffW3 + k] = bf16_host(bf16_round_host(a3 * u(g)));
+    for (size_t k = 0; k < cN4; k++) P[cOffE + k] = bf16_host(bf16_round_host(a4 * u(g)));
+  }
+  std::vector<uint16_t> W(cN1 + cN2 + cN3 + cN4);
+  for (size_t k = 0; k < cN1; k++) W[k] = bf16_round_host(P[k]);
+  for (size_t k = 0; k < cN2; k++) W[cN1 + k] = bf16_round_host(P[cOffW2 + k]);
+  for (size_t k = 0; k < cN3; k++) W[cN1 + cN2 + k] = bf16_round_host(P[cOffW3 + k]);
+  for (size_t k = 0; k < cN4; k++) W[cN1 + cN2 + cN3 + k] = bf16_round_host(P[cOffE + k]);
+  MlpJob job;
+  CutData d;
+  float *dp = nullptr, *dm1 = nullptr, *dm2 = nullptr, *dg = nullptr, *dl = nullptr;
+  int* didx = nullptr;
+  uint16_t* dw = nullptr;
+  if (!upload_cut_examples(job, x, c, lo, hi, count, true, &d) || !job.alloc(&didx, count) ||
+      !job.alloc(&dp, CUT_NPARAM) || !job.alloc(&dm1, CUT_NPARAM) || !job.alloc(&dm2, CUT_NPARAM) ||
+      !job.alloc(&dg, CUT_NPARAM) || !job.alloc(&dl, 1) || !job.alloc(&dw, W.size()))
+    return fail(FB_ERR_CUDA, "out of device memory");
+  CK(cudaMemcpy(dp, P.data(), sizeof(float) * CUT_NPARAM, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw, W.data(), sizeof(uint16_t) * W.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemset(dm1, 0, sizeof(float) * CUT_NPARAM));
+  CK(cudaMemset(dm2, 0, sizeof(float) * CUT_NPARAM));
+  CutParams CP{dw, dw + cN1, dw + cN1 + cN2, dw + cN1 + cN2 + cN3, dp + cOffB1, dp + cOffB2, dp + cOffB3, dp + cOffBE};
+  std::vector<int> perm(count);
+  for (int k = 0; k < count; k++) perm[k] = k;
+  std::mt19937_64 shuf(opt->seed ^ 0x5851F42D4C957F2Dull);
+  int step = 0;
+  for (int e = 0; e < opt->epochs; e++) {
+    std::shuffle(perm.begin(), perm.end(), shuf);
+    CK(cudaMemcpy(didx, perm.data(), sizeof(int) * (size_t)count, cudaMemcpyHostToDevice));
+    CK(cudaMemset(dl, 0, sizeof(float)));
+    for (int s0 = 0; s0 < count; s0 += opt->batch) {
+      const int B = std::min(opt->batch, count - s0);
+      CK(cudaMemsetAsync(dg, 0, sizeof(float) * CUT_NPARAM));
+      if (cut_grad_launch(CP, d.x, d.c, d.lo, d.hi, didx + s0, B, dg, dl, nullptr) != 0)
+        return fail(FB_ERR_CUDA, "gradient kernel failed: %s", cudaGetErrorString(cudaGetLastError()));
+      if (cut_adam_launch(dp, dm1, dm2, dg, 1.0f / (float)B, (float)opt->lr, ++step, CP, nullptr) != 0)
+        return fail(FB_ERR_CUDA, "update kernel failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    float l = 0.0f;
+    CK(cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost));
+    if (losses) losses[e] = (double)l / count;
+  }
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(P.data(), dp, sizeof(float) * CUT_NPARAM, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(W.data(), dw, sizeof(uint16_t) * W.size(), cudaMemcpyDeviceToHost));
+  std::memcpy(out_w1, W.data(), 2 * cN1);
+  std::memcpy(out_w2, W.data() + cN1, 2 * cN2);
+  std::memcpy(out_w3, W.data() + cN1 + cN2, 2 * cN3);
+  std::memcpy(out_emb, W.data() + cN1 + cN2 + cN3, 2 * cN4);
+  std::memcpy(out_b1, P.data() + cOffB1, 4 * CUT_H);
+  std::memcpy(out_b2, P.data() + cOffB2, 4 * CUT_H);
+  std::memcpy(out_b3, P.data() + cOffB3, 4 * CUT_E);
+  std::memcpy(out_be, P.data() + cOffBE, 4 * CUT_BINS);
+  return FB_OK;
+}
+
+fb_status fb_cut_loss_grad(const fb_cut_model* model, const float* x, const int* c, const int* lo, const int* hi,
+                           int count, int device, double* loss, float* gw1, float* gb1, float* gw2, float* gb2,
+                           float* gw3, float* gb3, float* gemb, float* gbe) {
+  if (!cut_model_complete(model) || !loss) return fail(FB_ERR_ARG, "model and loss are required");
+  fb_status st = check_cut_examples(x, c, lo, hi, count);
+  if (st != FB_OK) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  CK(cudaSetDevice(device));
+  std::vector<float> P(CUT_NPARAM, 0.0f);
+  for (int k = 0; k < CUT_H; k++) { P[cOffB1 + k] = model->b1[k]; P[cOffB2 + k] = model->b2[k]; }
+  for (int k = 0; k < CUT_E; k++) P[cOffB3 + k] = model->b3[k];
+  for (int k = 0; k < CUT_BINS; k++) P[cOffBE + k] = model->be[k];
+  MlpJob job;
+  CutData d;
+  float *dp = nullptr, *dg = nullptr, *dl = nullptr;
+  uint16_t* dw = nullptr;
+  if (!upload_cut_examples(job, x, c, lo, hi, count, false, &d) || !job.alloc(&dp, CUT_NPARAM) ||
+      !job.alloc(&dg, CUT_NPARAM) || !job.alloc(&dl, 1) || !job.alloc(&dw, cN1 + cN2 + cN3 + cN4))
+    return fail(FB_ERR_CUDA, "out of device memory");
+  CK(cudaMemcpy(dp, P.data(), sizeof(float) * CUT_NPARAM, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw, model->w1, 2 * cN1, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw + cN1, model->w2, 2 * cN2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw + cN1 + cN2, model->w3, 2 * cN3, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dw + cN1 + cN2 + cN3, model->emb, 2 * cN4, cudaMemcpyHostToDevice));
+  CK(cudaMemset(dg, 0, sizeof(float) * CUT_NPARAM));
+  CK(cudaMemset(dl, 0, sizeof(float)));
+  CutParams CP{dw, dw + cN1, dw + cN1 + cN2, dw + cN1 + cN2 + cN3, dp + cOffB1, dp + cOffB2, dp + cOffB3, dp + cOffBE};
+  if (cut_grad_launch(CP, d.x, d.c, d.lo, d.hi, nullptr, count, dg, dl, nullptr) != 0)
+    return fail(FB_ERR_CUDA, "gradient kernel failed: %s", cudaGetErrorString(cudaGetLastError()));
+  CK(cudaDeviceSynchronize());
+  std::vector<float> G(CUT_NPARAM);
+  float l = 0.0f;
+  CK(cudaMemcpy(G.data(), dg, sizeof(float) * CUT_NPARAM, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost));
+  const float inv = 1.0f / (float)count;
+  *loss = (double)l / count;
+  auto put = [&](float* dst, size_t off, size_t n) { if (dst) for (size_t k = 0; k < n; k++) dst[k] = G[off + k] * inv; };
+  put(gw1, 0, cN1); put(gb1, cOffB1, CUT_H); put(gw2, cOffW2, cN2); put(gb2, cOffB2, CUT_H);
+  put(gw3, cOffW3, cN3); put(gb3, cOffB3, CUT_E); put(gemb, cOffE, cN4); put(gbe, cOffBE, CUT_BINS);
   return FB_OK;
 }
 

@@ -197,4 +197,221 @@ int mlp_adam_launch(float* p, float* m1, float* m2, const float* g, float inv_ba
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+// ------------------------------------------------------------------------------------------------ cut head
+// Training of the learned cut proposal's head: CUT_IN features -> CUT_H -> CUT_H -> CUT_E -> logits be[c] + emb[c] . e,
+// softmax cross-entropy over each example's cut range [lo, hi].  Flat FP32 parameters w1 [H][IN], b1 [H], w2 [H][H],
+// b2 [H], w3 [E][H], b3 [E], emb [BINS][E], be [BINS]; the forward pass reads the BF16-rounded weights.
+constexpr int CT_ZS = 256;   // logits per example (padded)
+
+__global__ void __launch_bounds__(MT_THREADS) cut_grad_kernel(CutParams P, const float* __restrict__ X,
+                                                              const int* __restrict__ Yc, const int* __restrict__ LO,
+                                                              const int* __restrict__ HI, const int* __restrict__ idx,
+                                                              int B, float* __restrict__ grad,
+                                                              float* __restrict__ loss) {
+  extern __shared__ float cms[];
+  float* w1 = cms;                          // [H][IN]
+  float* w2 = w1 + CUT_H * CUT_IN;          // [H][H]
+  float* w3 = w2 + CUT_H * CUT_H;           // [E][H]
+  float* em = w3 + CUT_E * CUT_H;           // [BINS][E]
+  float* xs = em + CUT_BINS * CUT_E;        // [TILE][IN]
+  float* h1 = xs + MT_TILE * CUT_IN;        // [TILE][H]
+  float* h2 = h1 + MT_TILE * CUT_H;         // [TILE][H]
+  float* ev = h2 + MT_TILE * CUT_H;         // [TILE][E]
+  float* dz = ev + MT_TILE * CUT_E;         // [TILE][CT_ZS]: logits, then dLoss/dz
+  float* de = dz + MT_TILE * CT_ZS;         // [TILE][E]
+  float* d2 = de + MT_TILE * CUT_E;         // [TILE][H]
+  float* d1 = d2 + MT_TILE * CUT_H;         // [TILE][H]
+  float* lsum = d1 + MT_TILE * CUT_H;       // [1]
+  int* lo = reinterpret_cast<int*>(lsum + 1);   // [TILE]
+  int* hi = lo + MT_TILE;
+  int* yc = hi + MT_TILE;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int b0 = blockIdx.x * MT_TILE;
+  const int nb = min(MT_TILE, B - b0);
+  for (int k = tid; k < CUT_H * CUT_IN; k += MT_THREADS) w1[k] = bf16_to_f(P.w1[k]);
+  for (int k = tid; k < CUT_H * CUT_H; k += MT_THREADS) w2[k] = bf16_to_f(P.w2[k]);
+  for (int k = tid; k < CUT_E * CUT_H; k += MT_THREADS) w3[k] = bf16_to_f(P.w3[k]);
+  for (int k = tid; k < CUT_BINS * CUT_E; k += MT_THREADS) em[k] = bf16_to_f(P.emb[k]);
+  for (int k = tid; k < MT_TILE * CUT_IN; k += MT_THREADS) {
+    const int b = k / CUT_IN, f = k % CUT_IN;
+    xs[k] = b < nb ? X[(long long)(idx ? idx[b0 + b] : b0 + b) * CUT_IN + f] : 0.0f;
+  }
+  if (tid < MT_TILE) {
+    const long long e = tid < nb ? (idx ? idx[b0 + tid] : b0 + tid) : -1;
+    lo[tid] = e >= 0 ? LO[e] : 0; hi[tid] = e >= 0 ? HI[e] : -1; yc[tid] = e >= 0 ? Yc[e] : 0;
+  }
+  if (tid == 0) *lsum = 0.0f;
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
+    const int b = k / CUT_H, h = k % CUT_H;
+    float a = P.b1[h];
+    for (int f = 0; f < CUT_IN; f++) a += w1[h * CUT_IN + f] * xs[b * CUT_IN + f];
+    h1[k] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
+    const int b = k / CUT_H, h = k % CUT_H;
+    float a = P.b2[h];
+    for (int f = 0; f < CUT_H; f++) a += w2[h * CUT_H + f] * h1[b * CUT_H + f];
+    h2[k] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * CUT_E; k += MT_THREADS) {
+    const int b = k / CUT_E, q = k % CUT_E;
+    float a = P.b3[q];
+    for (int f = 0; f < CUT_H; f++) a += w3[q * CUT_H + f] * h2[b * CUT_H + f];
+    ev[k] = a;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * CT_ZS; k += MT_THREADS) {
+    const int b = k / CT_ZS, c = k % CT_ZS;
+    float a = 0.0f;
+    if (c >= lo[b] && c <= hi[b]) {
+      a = P.be[c];
+      for (int q = 0; q < CUT_E; q++) a += em[c * CUT_E + q] * ev[b * CUT_E + q];
+    }
+    dz[k] = a;
+  }
+  __syncthreads();
+  // softmax over [lo, hi] and cross-entropy, one warp per example: dz becomes dLoss/dz (summed, not averaged)
+  for (int b = warp; b < MT_TILE; b += MT_THREADS / 32) {
+    float* z = dz + b * CT_ZS;
+    const int L = lo[b], U = hi[b];
+    if (b >= nb) {
+      for (int c = lane; c < CT_ZS; c += 32) z[c] = 0.0f;
+      continue;
+    }
+    float zm = -3.0e38f;
+    for (int c = L + lane; c <= U; c += 32) zm = fmaxf(zm, z[c]);
+    for (int o = 16; o > 0; o >>= 1) zm = fmaxf(zm, __shfl_xor_sync(0xffffffffu, zm, o));
+    float S = 0.0f;
+    for (int c = L + lane; c <= U; c += 32) S += __expf(z[c] - zm);
+    for (int o = 16; o > 0; o >>= 1) S += __shfl_xor_sync(0xffffffffu, S, o);
+    const float zy = z[yc[b]];
+    __syncwarp();
+    for (int c = lane; c < CT_ZS; c += 32)
+      z[c] = (c >= L && c <= U) ? __expf(z[c] - zm) / S - (c == yc[b] ? 1.0f : 0.0f) : 0.0f;
+    if (lane == 0) atomicAdd(lsum, -(zy - zm - __logf(S)));
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * CUT_E; k += MT_THREADS) {
+    const int b = k / CUT_E, q = k % CUT_E;
+    float a = 0.0f;
+    for (int c = lo[b]; c <= hi[b]; c++) a += dz[b * CT_ZS + c] * em[c * CUT_E + q];
+    de[k] = a;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
+    const int b = k / CUT_H, f = k % CUT_H;
+    float a = 0.0f;
+    for (int q = 0; q < CUT_E; q++) a += de[b * CUT_E + q] * w3[q * CUT_H + f];
+    d2[k] = h2[k] > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
+    const int b = k / CUT_H, f = k % CUT_H;
+    float a = 0.0f;
+    for (int h = 0; h < CUT_H; h++) a += d2[b * CUT_H + h] * w2[h * CUT_H + f];
+    d1[k] = h1[k] > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  float* gw1 = grad;
+  float* gb1 = gw1 + CUT_H * CUT_IN;
+  float* gw2 = gb1 + CUT_H;
+  float* gb2 = gw2 + CUT_H * CUT_H;
+  float* gw3 = gb2 + CUT_H;
+  float* gb3 = gw3 + CUT_E * CUT_H;
+  float* gem = gb3 + CUT_E;
+  float* gbe = gem + CUT_BINS * CUT_E;
+  for (int k = tid; k < CUT_H * CUT_IN; k += MT_THREADS) {
+    const int h = k / CUT_IN, f = k % CUT_IN;
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += d1[b * CUT_H + h] * xs[b * CUT_IN + f];
+    atomicAdd(gw1 + k, a);
+  }
+  for (int k = tid; k < CUT_H * CUT_H; k += MT_THREADS) {
+    const int h = k / CUT_H, f = k % CUT_H;
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += d2[b * CUT_H + h] * h1[b * CUT_H + f];
+    atomicAdd(gw2 + k, a);
+  }
+  for (int k = tid; k < CUT_E * CUT_H; k += MT_THREADS) {
+    const int q = k / CUT_H, f = k % CUT_H;
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += de[b * CUT_E + q] * h2[b * CUT_H + f];
+    atomicAdd(gw3 + k, a);
+  }
+  for (int k = tid; k < CUT_BINS * CUT_E; k += MT_THREADS) {
+    const int c = k / CUT_E, q = k % CUT_E;
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += dz[b * CT_ZS + c] * ev[b * CUT_E + q];
+    atomicAdd(gem + k, a);
+  }
+  if (tid < CUT_H) {
+    float a = 0.0f, c = 0.0f;
+    for (int b = 0; b < nb; b++) { a += d1[b * CUT_H + tid]; c += d2[b * CUT_H + tid]; }
+    atomicAdd(gb1 + tid, a);
+    atomicAdd(gb2 + tid, c);
+  }
+  if (tid < CUT_E) {
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += de[b * CUT_E + tid];
+    atomicAdd(gb3 + tid, a);
+  }
+  for (int c = tid; c < CUT_BINS; c += MT_THREADS) {
+    float a = 0.0f;
+    for (int b = 0; b < nb; b++) a += dz[b * CT_ZS + c];
+    atomicAdd(gbe + c, a);
+  }
+  __syncthreads();
+  if (tid == 0) atomicAdd(loss, *lsum);
+}
+
+// Adam on the cut head's flat parameter vector; the weight matrices also refresh their BF16 copies.
+__global__ void cut_adam_kernel(float* __restrict__ p, float* __restrict__ m1, float* __restrict__ m2,
+                                const float* __restrict__ g, int n, float inv_batch, float lr, float c1, float c2,
+                                CutParams P) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float gk = g[k] * inv_batch;
+  const float a = 0.9f * m1[k] + 0.1f * gk;
+  const float b = 0.999f * m2[k] + 0.001f * gk * gk;
+  m1[k] = a;
+  m2[k] = b;
+  const float w = p[k] - lr * (a * c1) / (sqrtf(b * c2) + 1e-8f);
+  p[k] = w;
+  const int o1 = CUT_H * CUT_IN, o2 = o1 + CUT_H, o3 = o2 + CUT_H * CUT_H, o4 = o3 + CUT_H, o5 = o4 + CUT_E * CUT_H,
+            o6 = o5 + CUT_E, o7 = o6 + CUT_BINS * CUT_E;
+  if (k < o1) P.w1[k] = f_to_bf16(w);
+  else if (k >= o2 && k < o3) P.w2[k - o2] = f_to_bf16(w);
+  else if (k >= o4 && k < o5) P.w3[k - o4] = f_to_bf16(w);
+  else if (k >= o6 && k < o7) P.emb[k - o6] = f_to_bf16(w);
+}
+
+size_t cut_grad_smem() {
+  return sizeof(float) * ((size_t)CUT_H * CUT_IN + CUT_H * CUT_H + CUT_E * CUT_H + CUT_BINS * CUT_E +
+                          (size_t)MT_TILE * (CUT_IN + 4 * CUT_H + 2 * CUT_E + CT_ZS) + 1) +
+         sizeof(int) * 3 * MT_TILE;
+}
+
+int cut_grad_launch(const CutParams& P, const float* X, const int* Yc, const int* LO, const int* HI, const int* idx,
+                    int B, float* grad, float* loss, void* stream) {
+  if (B <= 0) return 0;
+  const size_t smem = cut_grad_smem();
+  if (cudaFuncSetAttribute(cut_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return -1;
+  cut_grad_kernel<<<(B + MT_TILE - 1) / MT_TILE, MT_THREADS, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+      P, X, Yc, LO, HI, idx, B, grad, loss);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cut_adam_launch(float* p, float* m1, float* m2, const float* g, float inv_batch, float lr, int step,
+                    const CutParams& P, void* stream) {
+  const int n = CUT_NPARAM;
+  const float c1 = 1.0f / (1.0f - powf(0.9f, (float)step)), c2 = 1.0f / (1.0f - powf(0.999f, (float)step));
+  cut_adam_kernel<<<(n + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(p, m1, m2, g, n, inv_batch,
+                                                                                       lr, c1, c2, P);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 }  // namespace fb

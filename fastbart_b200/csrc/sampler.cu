@@ -45,19 +45,34 @@ namespace fb {
 
 constexpr int NBS = NB_MAX;   // per-thread shared-memory bins (compact leaf index < NBS); beyond: shared atomics
 constexpr int TOT = 16;       // CTA totals per tree: [0, NBS) leaf sums, NBS.. sL0 sL1 nL
-constexpr int NSPLIT = 3;     // split partials per row thread: sum fx(w), sum fx(w*R), count of the left child
+constexpr int NSPLIT = 4;     // split partials per row thread: sum fx(w), sum fx(w*R), count of the left child, and
+                              // sum fx2(w*R^2) of the rows of the learned cut proposal's node
 constexpr int LST = LEAF_STAT_WORDS;
 constexpr int ZMAX = 16;      // leaf-mu normals drawn ahead per tree (candidate slots beyond are drawn in the step)
+constexpr int ZMAX_CUT = 8;   // the same in cut layouts (smaller; the normals are the same counter-based draws)
 constexpr int MODE_PLAIN = 0, MODE_MODEL = 1, MODE_COLLECT = 2;   // sampler kernel variants (see sampler_kernel)
+constexpr int BIN_ROWS = NBS + 3;       // rows of the bin matrix: leaf rows, split rows (sum fx(w), fx(w R), count)
+constexpr int BIN_ROWS_CUT = NBS + 4;   // with the learned cut proposal: and sum fx2(w R^2) of its node's rows
 // the pass bins of a CTA of `threads` can hold the proposal model's weight image at sweep start
 __host__ __device__ inline bool bins_hold_model(int threads) {
-  return (size_t)(NBS + NSPLIT) * (size_t)(threads - 32) * 8 >= (size_t)MIMG_WORDS * 4;
+  return (size_t)BIN_ROWS * (size_t)(threads - 32) * 8 >= (size_t)MIMG_WORDS * 4;
 }
+// the split rows of the bins hold the cut proposal's code histogram (cut launches accumulate no split sums)
+__host__ __device__ inline bool bins_hold_hist(int threads) { return (size_t)3 * (threads - 32) * 8 >= 256 * 20; }
 
 struct Prop {                 // proposal of one tree for the current sweep
   double logpr, lu;
   unsigned long long cand;    // slots that can be leaves after the move (normals drawn ahead, in slot order)
-  uint8_t mode, nx, v, c, l, r, dnx, pad1;   // dnx: depth of node nx
+  uint8_t mode, nx, v, c, l, r, dnx, flags;   // dnx: depth of node nx; flags bit 0: the cut is drawn after the pass
+};
+constexpr int PROP_DEFER = 1;
+// What the learned cut proposal needs of tree j's proposal beyond Prop (launches with a cut head, and collecting
+// launches): for a birth, BART's ratio (times the variable proposal's factor) for a cut at the inside of the range or
+// at its ends, pr4[(c == L) + 2 (c == U)]; for a death, pr4[0] is the ratio; L, U: the cut range of the variable at
+// the node; uses: internal nodes splitting on the variable (other than the node itself).
+struct PropX {
+  double pr4[4];
+  uint8_t L, U, uses, pad[5];
 };
 struct Masks { unsigned long long used, leaf; };
 struct Ctl {                  // CTA-shared control state
@@ -143,6 +158,12 @@ struct PassU {
   long long* bins;            // [NBS + NSPLIT][RT]: per-thread leaf sums, then split partials
   unsigned long long* ovb;    // [64] leaves with compact index >= NBS
   long long* tot;             // [TOT] CTA totals
+  unsigned long long* h0;     // learned cut proposal: per code of the birth variable, sum fx(w) / sum fx(w*R) [256]
+  unsigned long long* h1;
+  int* hc;                    // and the row count [256]
+  float sqs;                  // 2^(rss_shift - fx_shift): fx2(w R^2) = llrint(w 2^S R R sqs)
+  int xhist;                  // accumulate the histogram of the rows of leaf sqa
+  int sqa, sqb;               // rows of leaves sqa and sqb accumulate fx2(w R^2) (-1: none)
   float DL, DR;
   int n, g0, g1, rt, RT, nleaf;   // rows: groups [g0, g1) of this CTA (r and ws are indexed from group g0)
   int apply, pmode, pnx, pc, pL, pR, pl, pr;
@@ -158,8 +179,9 @@ struct GroupWords { uint32_t lp, lc, qp, qc; };
 // matrix (compact leaf index < NBS; conflict-free, RT * 8 bytes is a multiple of the 32 banks), leaves beyond to
 // shared atomics.  For a birth proposal only the left child's sums and count are accumulated: the right child's
 // follow from the node's totals.
+template <bool XP>
 __device__ __forceinline__ void pass_group(const PassU& P, int g, const GroupWords& W, long long& sl0, long long& sl1,
-                                           int& nl) {
+                                           int& nl, long long& sq) {
   float* __restrict__ rp = P.r;
   const float* __restrict__ wp = P.ws;
   const float* __restrict__ Dp = P.D;
@@ -195,38 +217,64 @@ __device__ __forceinline__ void pass_group(const PassU& P, int g, const GroupWor
     if (left < 4) inl &= (1u << (8 * (left > 0 ? left : 0))) - 1u;
     nl += __popc(inl) >> 3;
   }
+  // rows of the learned cut proposal's node (extras kernels only): fx2(w R^2), and the code histogram of a birth
+  uint32_t insq = 0u;
+  if constexpr (XP) {
+    if (P.sqa >= 0) {
+      insq = __vcmpeq4(W.lc, bcast4(P.sqa)) | __vcmpeq4(W.lc, bcast4(P.sqb));
+      const int left = P.n - 4 * g;
+      if (left < 4) insq &= (1u << (8 * (left > 0 ? left : 0))) - 1u;
+    }
+  }
   long long* mybins = P.bins + P.rt;
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     const int lc = byte_of(W.lc, e);
     const float2 t = tcp[lc];
     const float R = __fadd_rn(rr[e], t.x);
-    const long long wr = __float2ll_rn(__fmul_rn(ww[e], R));
+    const float wrf = __fmul_rn(ww[e], R);
+    const long long wr = __float2ll_rn(wrf);
     const int ci = __float_as_int(t.y);
     if (ci < NBS) mybins[ci * P.RT] += wr;
     else atomicAdd(&P.ovb[lc], (unsigned long long)wr);
     if (byte_of(inl, e)) { sl0 += __float2ll_rn(ww[e]); sl1 += wr; }
+    if constexpr (XP) {
+      if (byte_of(insq, e)) {
+        sq += __float2ll_rn(__fmul_rn(__fmul_rn(wrf, R), P.sqs));
+        if (P.xhist) {
+          const int cd = byte_of(W.qc, e);
+          atomicAdd(&P.h0[cd], (unsigned long long)__float2ll_rn(ww[e]));
+          atomicAdd(&P.h1[cd], (unsigned long long)wr);
+          atomicAdd(&P.hc[cd], 1);
+        }
+      }
+    }
   }
 }
 
 // End of the pass: the split partials join this thread's column of the bin matrix (rows NBS..); the CTA totals are
 // formed afterwards by reduce_totals(), one warp per total.
-__device__ __forceinline__ void pass_store(const PassU& P, long long sl0, long long sl1, int nl) {
+template <bool XP>
+__device__ __forceinline__ void pass_store(const PassU& P, long long sl0, long long sl1, int nl, long long sq) {
+  long long* mybins = P.bins + P.rt;
   if (P.cmode == 1) {
-    long long* mybins = P.bins + P.rt;
     mybins[(NBS + 0) * P.RT] = sl0; mybins[(NBS + 1) * P.RT] = sl1; mybins[(NBS + 2) * P.RT] = nl;
+  }
+  if constexpr (XP) {
+    if (P.sqa >= 0) mybins[(NBS + 3) * P.RT] = sq;
   }
 }
 
 // CTA totals of one pass: warp w sums row w of the bin matrix over the RT row threads (lanes read consecutive
 // threads' partials, and clears the leaf rows for the next pass), then reduces across the warp.  Exact int64.  Called
 // by every warp of the CTA after the pass and a barrier.
-__device__ __forceinline__ void reduce_totals(long long* bins, int RT, int nleaf, int cmode, long long* tot) {
+__device__ __forceinline__ void reduce_totals(long long* bins, int RT, int nleaf, int cmode, long long* tot,
+                                              bool sq = false) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, NW = blockDim.x >> 5;
   const int nb = nleaf < NBS ? nleaf : NBS;
   for (int row = warp; row < NBS + NSPLIT; row += NW) {
     const bool leafrow = row < NBS;
-    if (leafrow ? row >= nb : cmode != 1) continue;
+    if (leafrow ? row >= nb : (row < NBS + 3 ? cmode != 1 : !sq)) continue;
     long long* br = bins + (long long)row * RT;
     long long v = 0;
     for (int k = lane; k < RT; k += 32) {
@@ -239,27 +287,28 @@ __device__ __forceinline__ void reduce_totals(long long* bins, int RT, int nleaf
 }
 
 // Pass with words streamed from L2 in the pass itself (any n).
+template <bool XP>
 __device__ void pass_rows_stream(const PassU& P) {
-  long long sl0 = 0, sl1 = 0;
+  long long sl0 = 0, sl1 = 0, sq = 0;
   int nl = 0;
   for (int g = P.g0 + P.rt; g < P.g1; g += P.RT) {
     GroupWords W;
     W.lc = ld_u32(P.leaf_cur + 4 * g);
     W.lp = P.apply ? ld_u32(P.leaf_prev + 4 * g) : 0u;
     W.qp = (P.apply && P.pmode == 1) ? __ldg(reinterpret_cast<const uint32_t*>(P.qprev + 4 * g)) : 0u;
-    W.qc = P.cmode == 1 ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
-    pass_group(P, g, W, sl0, sl1, nl);
+    W.qc = (P.cmode == 1 || P.xhist) ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
+    pass_group<XP>(P, g, W, sl0, sl1, nl, sq);
   }
-  pass_store(P, sl0, sl1, nl);
+  pass_store<XP>(P, sl0, sl1, nl, sq);
 }
 
 // Pass with register-held words (each row thread owns at most G groups).  lcr/qcr hold tree j-1's words on entry
 // (tree j's on exit); nlc/nqc hold tree j's prefetched words on entry (tree j+1's on exit).  first: tree 0 of a
 // sweep (no prefetch available, nothing to apply).
-template <int G>
+template <int G, bool XP>
 __device__ __forceinline__ void pass_rows_regs(const PassU& P, bool first, uint32_t (&lcr)[G], uint32_t (&qcr)[G],
                                                uint32_t (&nlc)[G], uint32_t (&nqc)[G]) {
-  long long sl0 = 0, sl1 = 0;
+  long long sl0 = 0, sl1 = 0, sq = 0;
   int nl = 0;
 #pragma unroll
   for (int k = 0; k < G; k++) {
@@ -268,14 +317,14 @@ __device__ __forceinline__ void pass_rows_regs(const PassU& P, bool first, uint3
       GroupWords W;
       if (first) {
         W.lc = ld_u32(P.leaf_cur + 4 * g);
-        W.qc = P.cmode == 1 ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
+        W.qc = (P.cmode == 1 || P.xhist) ? __ldg(reinterpret_cast<const uint32_t*>(P.qcur + 4 * g)) : 0u;
       } else {
         W.lc = nlc[k];
         W.qc = nqc[k];
       }
       W.lp = lcr[k];
       W.qp = qcr[k];
-      pass_group(P, g, W, sl0, sl1, nl);
+      pass_group<XP>(P, g, W, sl0, sl1, nl, sq);
       lcr[k] = W.lc;
       qcr[k] = W.qc;
     }
@@ -289,7 +338,7 @@ __device__ __forceinline__ void pass_rows_regs(const PassU& P, bool first, uint3
       nqc[k] = P.qnext ? __ldg(reinterpret_cast<const uint32_t*>(P.qnext + 4 * g)) : 0u;
     }
   }
-  pass_store(P, sl0, sl1, nl);
+  pass_store<XP>(P, sl0, sl1, nl, sq);
 }
 
 // ------------------------------------------------------------------------------------------------ tree helpers
@@ -613,9 +662,21 @@ __device__ __forceinline__ void model_phase(const DBufs& B, const DChain& C, con
 // reverse birth of a death, come from model_phase, and pr carries the correction, so the chain keeps BART's target.
 // cnt: the tree's per-slot row counts.  When training examples are collected, the birth node's features go to
 // feat / *fvalid.
+// internal nodes of t splitting on v, other than `exclude`
+__device__ __forceinline__ int uses_of(const DTree* t, int v, int exclude) {
+  int u = 0;
+  for (unsigned long long im = t->used & ~t->leaf; im; im &= im - 1ull) {
+    const int s = __ffsll((long long)im) - 1;
+    u += s != exclude && (int)t->v[s] == v;
+  }
+  return u;
+}
+
+// With px (model and collecting kernels) the learned cut proposal's view of the proposal is filled in, and with a
+// cut head (B.cimg) a birth's cut is left to the step (PROP_DEFER).
 template <bool LP, bool MP>
 __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cnt, int j, int it, Masks& mk,
-                        float* feat, unsigned* fvalid) {
+                        float* feat, unsigned* fvalid, PropX* px) {
   const double pb = 0.5;
   const unsigned long long used = t->used, leafm = t->leaf;
   mk.used = used; mk.leaf = leafm;
@@ -636,7 +697,7 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
   const double ub = fbm::u32d(x.x), un = fbm::u32d(x.y), uv = fbm::u32d(x.z), uc = fbm::u32d(x.w);
   const bool model = MP && B.mvar != nullptr;
   Prop P;
-  P.mode = 0; P.nx = 0; P.v = 0; P.c = 0; P.l = 0; P.r = 0; P.dnx = P.pad1 = 0; P.logpr = 0; P.lu = 0;
+  P.mode = 0; P.nx = 0; P.v = 0; P.c = 0; P.l = 0; P.r = 0; P.dnx = P.flags = 0; P.logpr = 0; P.lu = 0;
   double pr = 0;
   if (ub < PBx) {
     const int nx = select_kth(goodm, (int)(un * ngood));
@@ -668,6 +729,19 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
       pr = (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
       if (model) pr = pr * corr;
       P.mode = 1; P.nx = (uint8_t)nx; P.v = (uint8_t)v; P.c = (uint8_t)c; P.dnx = (uint8_t)dnx;
+      if (MP && px) {   // the ratio for a cut inside the range or at either end (c == bL: k & 1, c == bU: k & 2)
+        px->L = (uint8_t)bL; px->U = (uint8_t)bU; px->uses = (uint8_t)uses_of(t, v, -1);
+        for (int k = 0; k < 4; k++) {
+          double gl, gr;
+          if (t->ngv[nx] > 1) { gl = gr = C.pg[dnx + 1]; }
+          else { gl = (k & 1) ? 0 : C.pg[dnx + 1]; gr = (k & 2) ? 0 : C.pg[dnx + 1]; }
+          const double pdy = (ngood > 1) ? 1 - pb : ((gr == 0 && gl == 0) ? 1 : 1 - pb);
+          double prk = (PGnx * (1 - gl) * (1 - gr) * pdy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
+          if (model) prk = prk * corr;
+          px->pr4[k] = prk;
+        }
+        if (B.cimg) P.flags = PROP_DEFER;
+      }
     }
   } else if (nnogs > 0) {
     const int nx = select_kth(nogm, (int)(un * nnogs));
@@ -680,6 +754,14 @@ __device__ Prop propose(DTree* t, const DChain& C, const DBufs& B, const int* cn
     pr = ((1 - PGny) * PBy * Pboty) / (PGny * (1 - PGlx) * (1 - PGrx) * PDx * Pnogx);
     if (model) pr = pr * B.mcorr[C.off_tree + j];   // the reverse birth
     P.mode = 2; P.nx = (uint8_t)nx; P.l = (uint8_t)l; P.r = (uint8_t)r;
+    if (MP && px) {   // the reverse birth's variable, cut and cut range
+      const int vn = t->v[nx];
+      int Ln, Un;
+      node_range(t, nx, vn, C.numcut[vn], Ln, Un);
+      P.v = (uint8_t)vn; P.c = t->c[nx]; P.dnx = (uint8_t)dny;
+      px->L = (uint8_t)Ln; px->U = (uint8_t)Un; px->uses = (uint8_t)uses_of(t, vn, nx);
+      px->pr4[0] = pr;
+    }
   }
   if (P.mode) {
     P.logpr = fbm::fb_log(pr);
@@ -710,7 +792,8 @@ struct Smem {
   float* D;                     // [64] apply deltas of the last decided move
   float2* tc;                   // [2][64] theta and compact leaf index
   double* z;                    // [64] mu normals of tree j beyond the first ZMAX candidates
-  double* zall;                 // [m][ZMAX] mu normals drawn ahead
+  double* zall;                 // [m][zmax] mu normals drawn ahead
+  int zmax;                     // normals drawn ahead per tree in this layout
   long long* bins;              // [NBS + NSPLIT][RT]
   long long* tot;               // [2][TOT]
   unsigned long long* ovb;      // [2][64]
@@ -722,16 +805,34 @@ struct Smem {
   long long* xtot;              // [2][cluster][TOT] every CTA's pass totals, pushed by their owners
   unsigned long long* xovb;     // [2][cluster][64]
   uint32_t* mimg;               // [MIMG_WORDS] the proposal model's weight image, behind the layout (B.model_smem)
+  int binrows;                  // rows of the bin matrix in this layout
+  // learned cut proposal (cut layouts)
+  PropX* px;                    // [m]
+  struct CutScr* cs;            // the cut stage's scratch
+  unsigned long long* h0;       // [256] code histogram of the birth node (in the split rows of the bins)
+  unsigned long long* h1;       // [256]
+  int* hc;                      // [256]
+  uint32_t* cimg;               // [CIMG_WORDS] the cut head's weight image, behind mimg (B.cut_smem)
+  long long* xcut;              // [cluster][4] every CTA's split sums of the drawn cut, pushed by their owners
+};
+// scratch of the cut stage (in the bins' leaf rows, which are zero between passes; cleared again after the stage):
+// features, hidden layers, logits, exponentials, block sums; the decision
+struct CutScr {
+  float cx[CUT_IN], h1[CUT_H], h2[CUT_H], e[CUT_E], z[256];
+  double ex[256], bs[32];
+  double zmax, logpr;
+  long long sL0, sL1;
+  int nL, c, pad0, pad1;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster,
-                                               size_t* off) {
+                                               size_t* off, int cut = 0) {
   const int NW = threads / 32, RT = threads - 32;
   size_t o = 0;
   off[0] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // r
-  off[1] = o; o += rows_in_smem ? align_up((size_t)n_pad_max * 4, 16) : 0;   // ws
+  off[1] = o; o += rows_in_smem == 1 ? align_up((size_t)n_pad_max * 4, 16) : 0;   // ws
   off[2] = o; o += align_up((size_t)m_max * NODES * 4, 16);                  // th
   off[3] = o; o += align_up((size_t)m_max * sizeof(Prop), 16);               // prop
   off[4] = o; o += align_up((size_t)m_max * sizeof(Masks), 16);              // masks
@@ -740,25 +841,32 @@ __host__ __device__ inline size_t smem_layout(int threads, int m_max, int n_pad_
   off[7] = o; o += NODES * 4;                                                // D
   off[8] = o; o += 2 * NODES * 8;                                            // tc[2]
   off[9] = o; o += NODES * 8;                                                // z
-  off[10] = o; o += (size_t)(NBS + NSPLIT) * RT * 8;                         // bins (leaf rows, split rows)
+  off[10] = o; o += (size_t)(cut ? BIN_ROWS_CUT : BIN_ROWS) * RT * 8;         // bins (leaf rows, split rows)
   off[11] = o; o += 2 * TOT * 8;                                             // tot[2]
   off[12] = o; o += 2 * NODES * 8;                                           // ovb[2]
   off[13] = o; o += align_up((size_t)NW * 8, 16);                            // red
   off[14] = o; o += align_up(sizeof(Ctl), 16);                               // ctl
-  off[15] = o; o += (size_t)m_max * ZMAX * 8;                                // zall
+  off[15] = o; o += (size_t)m_max * (cut ? ZMAX_CUT : ZMAX) * 8;            // zall
   off[16] = o; o += 2 * TOT * 8;                                             // ctot[2]
   off[17] = o; o += 2 * NODES * 8;                                           // covb[2]
   off[18] = o; o += 2 * 4 * 8;                                               // xch[2][4]
   const size_t cs = cluster > 1 ? (size_t)cluster : 0;
   off[19] = o; o += 2 * cs * TOT * 8;                                        // xtot[2][cluster][TOT]
   off[20] = o; o += 2 * cs * NODES * 8;                                      // xovb[2][cluster][64]
+  off[21] = o; o += cut ? align_up((size_t)m_max * sizeof(PropX), 16) : 0;  // px
+  off[22] = o; o += cut ? (size_t)(cs ? cs : 1) * 4 * 8 : 0;                   // xcut[cluster][4]
   return o;
 }
-constexpr int NOFF = 21;
+constexpr int NOFF = 23;
+// words staged behind the layout: the proposal model's image (when the bins cannot hold it), then the cut head's
+__host__ __device__ inline size_t model_words(int threads, bool mimg_smem) {
+  return mimg_smem && !bins_hold_model(threads) ? (size_t)MIMG_WORDS : 0;
+}
 
-__device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster) {
+__device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster,
+                      int cut, bool mimg_smem) {
   size_t off[NOFF];
-  smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off);
+  const size_t end = smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off, cut);
   Smem S;
   S.r = reinterpret_cast<float*>(base + off[0]);
   S.ws = reinterpret_cast<float*>(base + off[1]);
@@ -781,8 +889,17 @@ __device__ Smem carve(unsigned char* base, int threads, int m_max, int n_pad_max
   S.xch = reinterpret_cast<long long*>(base + off[18]);
   S.xtot = reinterpret_cast<long long*>(base + off[19]);
   S.xovb = reinterpret_cast<unsigned long long*>(base + off[20]);
-  S.mimg = reinterpret_cast<uint32_t*>(base + align_up(smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off),
-                                                       16));
+  S.mimg = reinterpret_cast<uint32_t*>(base + align_up(end, 16));
+  S.binrows = cut ? BIN_ROWS_CUT : BIN_ROWS;
+  S.px = cut ? reinterpret_cast<PropX*>(base + off[21]) : nullptr;
+  S.cs = cut ? reinterpret_cast<CutScr*>(S.bins) : nullptr;   // in the leaf rows of the bins, zeroed after use
+  S.zmax = cut ? ZMAX_CUT : ZMAX;
+  S.xcut = reinterpret_cast<long long*>(base + off[22]);
+  const int RT = threads - 32;
+  S.h0 = reinterpret_cast<unsigned long long*>(S.bins + (size_t)NBS * RT);
+  S.h1 = S.h0 + 256;
+  S.hc = reinterpret_cast<int*>(S.h1 + 256);
+  S.cimg = S.mimg + model_words(threads, mimg_smem);
   return S;
 }
 
@@ -835,6 +952,14 @@ __device__ __forceinline__ void collect_example(const DBufs& B, const DChain& C,
     const float* f = B.feat + (C.off_tree + j) * MLP_IN;
     for (int k = lane; k < MLP_IN; k += 32) B.train_x[(long long)idx * MLP_IN + k] = f[k];
     if (lane == 0) { B.train_y[idx] = v; B.train_mask[idx] = B.feat_valid[C.off_tree + j]; }
+    if (B.train_cx) {   // the same birth's cut example, written by its step
+      const float* cf = B.cfeat + (C.off_tree + j) * CUT_IN;
+      for (int k = lane; k < CUT_IN; k += 32) B.train_cx[(long long)idx * CUT_IN + k] = cf[k];
+      if (lane == 0) {
+        const int* ci3 = B.cinfo + (C.off_tree + j) * 3;
+        B.train_c[idx] = ci3[0]; B.train_lo[idx] = ci3[1]; B.train_hi[idx] = ci3[2];
+      }
+    }
   }
 }
 
@@ -901,8 +1026,211 @@ __device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTre
   __syncwarp();
 }
 
-// ------------------------------------------------------------------------------------------------ one chain
+// ------------------------------------------------------------------------------------------------ cut proposal
 namespace cg = cooperative_groups;
+
+// Features of the learned cut proposal at a node (see the oracle's orc_cut_features): depth, row count, the weighted
+// residual mean and sd of the node's rows from its exact sums (S0 = sum fx(w), S1 = sum fx(w R), Q = sum fx2(w R^2))
+// relative to sigma, the cut range [L, U] of v and v's uses in the tree, and v one-hot.
+__device__ void cut_features(int depth, int cnt, long long S0, long long S1, long long Q, int fx_shift, int rss_shift,
+                             double sigma, int L, int U, int nc, int uses, int v, float* x) {
+  for (int k = 0; k < CUT_IN; k++) x[k] = 0.0f;
+  x[0] = __fdiv_rn((float)depth, 8.0f);
+  x[1] = __fdiv_rn((float)(31 - __clz(cnt + 1)), 16.0f);
+  double mean = 0.0, sd = 0.0;
+  if (S0 > 0) {
+    const double w = (double)S0 * pow2(-fx_shift);
+    mean = (double)S1 / (double)S0;
+    const double msq = ((double)Q * pow2(-rss_shift)) / w;
+    const double var = msq - mean * mean;
+    sd = var > 0.0 ? sqrt(var) : 0.0;
+  }
+  double fm = mean / sigma;
+  fm = fm < -4.0 ? -4.0 : (fm > 4.0 ? 4.0 : fm);
+  double fs = sd / sigma;
+  fs = fs > 4.0 ? 4.0 : fs;
+  x[2] = (float)(fm * 0.25);
+  x[3] = (float)(fs * 0.25);
+  x[4] = __fdiv_rn((float)(U - L + 1), (float)nc);
+  x[5] = __fdiv_rn((float)L, (float)nc);
+  x[6] = __fdiv_rn((float)(uses < 8 ? uses : 8), 8.0f);
+  if (v >= 0 && v < 32) x[8 + v] = 1.0f;
+}
+
+__device__ __forceinline__ float cimg_w(const uint32_t* row, int k) {   // BF16 element k of a packed row
+  const uint32_t w = row[k >> 1];
+  return __uint_as_float((k & 1) ? (w & 0xFFFF0000u) : (w << 16));
+}
+
+// The learned cut proposal of tree j's step, after the pass totals (every thread of the CTA calls it; it ends with a
+// barrier).  A deferred birth draws its cut from the mixture of the head's softmax over [L, U] and the uniform cut
+// (Philox tag PROP3), takes the split sums of that cut from the code histogram of the node's rows (in cluster mode
+// every CTA pushes its three sums to every CTA, and a cluster barrier precedes their sum), and scales BART's ratio by
+// (1 / range) / q(c); a death scales its ratio by
+// q(c of the node) * range, the reverse birth's cut probability at the collapsed node.  Results in S.cs: c, logpr,
+// sL0, sL1, nL.  Every sum runs in the oracle's order, so the decision is bit-exact.
+struct CutOut { double logpr; long long sL0, sL1; int nL, c; };
+template <bool CL>
+__device__ void cut_stage(const Smem& S, const DBufs& B, const DChain& C, const Prop& P, int j, int it, int cur, int CS,
+                          double sigma, bool birth, bool lead, CutOut& out) {
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  CutScr& cs = *S.cs;
+  const PropX px = S.px[j];
+  const int L = px.L, U = px.U, range = U - L + 1, v = P.v;
+  const uint32_t* W = B.cut_smem ? S.cimg : B.cimg;
+  if (tid == 0) {
+    wait_stats(S, j);
+    const long long* tot = (CL ? S.ctot : S.tot) + cur * TOT;
+    const unsigned long long* ovb = (CL ? S.covb : S.ovb) + cur * NODES;
+    const float2* tcj = S.tc + cur * NODES;
+    const long long* s0 = S.s0t + cur * LST;
+    const int* cnt = reinterpret_cast<const int*>(s0 + NODES);
+    auto s1of = [&](int slot) -> long long {
+      const int c = __float_as_int(tcj[slot].y);
+      return c < NBS ? tot[c] : (long long)ovb[slot];
+    };
+    long long S0, S1;
+    int n;
+    if (birth) { S0 = s0[P.nx]; S1 = s1of(P.nx); n = cnt[P.nx]; }
+    else { S0 = s0[P.l] + s0[P.r]; S1 = s1of(P.l) + s1of(P.r); n = cnt[P.l] + cnt[P.r]; }
+    cut_features(P.dnx, n, S0, S1, tot[NBS + 3], C.fx_shift, C.rss_shift, sigma, L, U, C.numcut[v], px.uses, v, cs.cx);
+  }
+  __syncthreads();
+  const float* b = reinterpret_cast<const float*>(W + CIMG_B);
+  if (tid < CUT_H) {
+    const uint32_t* row = W + tid * CIMG_W1S;
+    float a = b[tid];
+#pragma unroll   // (every weight load issued ahead: the image may be in global memory)
+    for (int f = 0; f < CUT_IN; f++) a = __fadd_rn(a, __fmul_rn(cimg_w(row, f), cs.cx[f]));
+    cs.h1[tid] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  if (tid < CUT_H) {
+    const uint32_t* row = W + CIMG_W2 + tid * CIMG_W2S;
+    float a = b[CUT_H + tid];
+#pragma unroll
+    for (int f = 0; f < CUT_H; f++) a = __fadd_rn(a, __fmul_rn(cimg_w(row, f), cs.h1[f]));
+    cs.h2[tid] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  if (tid < CUT_E) {
+    const uint32_t* row = W + CIMG_W3 + tid * CIMG_W2S;
+    float a = b[2 * CUT_H + tid];
+#pragma unroll
+    for (int f = 0; f < CUT_H; f++) a = __fadd_rn(a, __fmul_rn(cimg_w(row, f), cs.h2[f]));
+    cs.e[tid] = a;
+  }
+  __syncthreads();
+  for (int k = tid; k < range; k += T) {
+    const int c = L + k;
+    const uint32_t* row = W + CIMG_EMB + c * CIMG_ES;
+    float a = b[2 * CUT_H + CUT_E + c];
+#pragma unroll
+    for (int f = 0; f < CUT_E; f++) a = __fadd_rn(a, __fmul_rn(cimg_w(row, f), cs.e[f]));
+    cs.z[c] = a;
+  }
+  __syncthreads();
+  if (warp == 2) {   // the largest logit: lane l takes block l (cuts L + 8l .. L + 8l + 7)
+    double zm = -INFINITY;
+    for (int k = 8 * lane; k < 8 * lane + 8 && k < range; k++) zm = fmax(zm, (double)cs.z[L + k]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) zm = fmax(zm, __shfl_xor_sync(0xffffffffu, zm, o));
+    if (lane == 0) cs.zmax = zm;
+  }
+  __syncthreads();
+  for (int k = tid; k < range; k += T) cs.ex[L + k] = fbm::fb_exp((double)cs.z[L + k] - cs.zmax);
+  __syncthreads();
+  if (warp == 2) {
+    const int nb = (range + 7) / 8;
+    double bs = 0.0;
+    for (int k = 8 * lane; k < 8 * lane + 8 && k < range; k++) bs = bs + cs.ex[L + k];
+    if (lane < nb) cs.bs[lane] = bs;
+    __syncwarp();
+    int c = 0;
+    if (lane == 0) {
+      double Ssum = 0.0;
+      for (int k = 0; k < nb; k++) Ssum = Ssum + cs.bs[k];
+      const double mix = B.cmix;
+      double pr;
+      if (birth) {
+        const fbm::U4 x3 = fbm::philox(0u, (uint32_t)j, (uint32_t)it, fbm::TAG_PROP3, C.seed);
+        const double umix = fbm::u32d(x3.x), uc = fbm::u32d(x3.y);
+        c = U;
+        if (umix < mix) {
+          const double target = uc * Ssum;
+          double Pp = 0.0;
+          for (int bk = 0; bk < nb; bk++) {
+            const double P1 = Pp + cs.bs[bk];
+            if (P1 > target) {
+              double run = Pp;
+              const int c0 = L + 8 * bk;
+              c = c0 + 7 < U ? c0 + 7 : U;
+              for (int cc = c0; cc < c0 + 8 && cc <= U; cc++) {
+                run = run + cs.ex[cc];
+                if (run > target) { c = cc; break; }
+              }
+              break;
+            }
+            Pp = P1;
+          }
+        } else {
+          c = L + (int)(uc * range);
+          if (c > U) c = U;
+        }
+        const double q = mix * (cs.ex[c] / Ssum) + (1.0 - mix) * (1.0 / (double)range);
+        const double corr = (1.0 / (double)range) / q;
+        pr = px.pr4[(c == L ? 1 : 0) + (c == U ? 2 : 0)] * corr;
+      } else {
+        c = P.c;
+        const double q = mix * (cs.ex[c] / Ssum) + (1.0 - mix) * (1.0 / (double)range);
+        pr = px.pr4[0] * (q * (double)range);
+      }
+      cs.c = c;
+      cs.logpr = fbm::fb_log(pr);
+    }
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (birth) {   // split sums of the cut: codes <= c of this CTA's rows of the node
+      unsigned long long a0 = 0, a1 = 0;
+      int ac = 0;
+      for (int k = lane; k <= c; k += 32) { a0 += S.h0[k]; a1 += S.h1[k]; ac += S.hc[k]; }
+      const long long t0 = warp_sum64((long long)a0), t1 = warp_sum64((long long)a1);
+      const int tc = __reduce_add_sync(0xffffffffu, ac);
+      if (lane == 0) {
+        if constexpr (CL) {   // every CTA's three sums to every CTA (remote stores), summed after a cluster barrier
+          cg::cluster_group cl = cg::this_cluster();
+          const int me = (int)cl.block_rank();
+          for (int d = 0; d < CS; d++) {
+            long long* x = cl.map_shared_rank(S.xcut + 4 * me, d);
+            x[0] = t0; x[1] = t1; x[2] = tc;
+          }
+        } else {
+          cs.sL0 = t0; cs.sL1 = t1; cs.nL = tc;
+        }
+      }
+    }
+  }
+  if constexpr (CL) {
+    if (birth) {
+      cg::this_cluster().sync();
+      if (tid == 0) {
+        long long s0 = 0, s1 = 0, sc = 0;
+        for (int r = 0; r < CS; r++) { s0 += S.xcut[4 * r]; s1 += S.xcut[4 * r + 1]; sc += S.xcut[4 * r + 2]; }
+        cs.sL0 = s0; cs.sL1 = s1; cs.nL = (int)sc;
+      }
+    }
+  }
+  __syncthreads();
+  out.c = cs.c; out.logpr = cs.logpr; out.sL0 = cs.sL0; out.sL1 = cs.sL1; out.nL = cs.nL;
+  if (B.train_cx && lead && birth && tid < CUT_IN) B.cfeat[(C.off_tree + j) * CUT_IN + tid] = cs.cx[tid];
+  __syncthreads();
+  // the scratch's bin rows back to zero for the next pass, and the histogram for the next birth (only this CTA reads
+  // its own histogram)
+  for (int k = tid; k < (int)(sizeof(CutScr) / 8); k += T) S.bins[k] = 0;
+  if (birth)
+    for (int k = tid; k < 256; k += T) { S.h0[k] = 0ull; S.h1[k] = 0ull; S.hc[k] = 0; }
+}
+
+// ------------------------------------------------------------------------------------------------ one chain
 
 // Proposals of every tree of sweep it (one thread per tree) with the leaf-mu normals drawn ahead.
 template <bool LP, bool MP>
@@ -913,13 +1241,13 @@ __device__ __forceinline__ void proposals_body(const Smem& S, const DBufs& B, co
     Masks mk;
     float* featj = (LP && B.train_cap > 0 && lead) ? B.feat + (C.off_tree + j) * MLP_IN : nullptr;
     const Prop P = propose<LP, MP>(trees + j, C, B, reinterpret_cast<const int*>(s0g + (long long)j * LST + NODES), j, it,
-                               mk, featj, B.feat_valid + (C.off_tree + j));
+                               mk, featj, B.feat_valid + (C.off_tree + j), S.px ? S.px + j : nullptr);
     S.prop[j] = P;
     S.masks[j] = mk;
     int k = 0;
-    for (unsigned long long cm = P.cand; cm && k < ZMAX; cm &= cm - 1ull, k++) {
+    for (unsigned long long cm = P.cand; cm && k < S.zmax; cm &= cm - 1ull, k++) {
       const int sl = __ffsll((long long)cm) - 1;
-      S.zall[j * ZMAX + k] = fbm::fb_normal(C.seed, (uint32_t)sl << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
+      S.zall[j * S.zmax + k] = fbm::fb_normal(C.seed, (uint32_t)sl << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
     }
   }
 }
@@ -999,7 +1327,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
   float* wsg = B.wsave + C.off_row + 4 * g0;
   double* tm = B.tm + C.off_row;
   float* r = B.rows_in_smem ? S.r : rg;       // indexed from row 4 * g0
-  float* ws = B.rows_in_smem ? S.ws : wsg;
+  float* ws = B.rows_in_smem == 1 ? S.ws : wsg;
   Ctl& ctl = *S.ctl;
   DState& st = B.states[ci];
   const bool regs = G > 0 && (g1 - g0) <= G * RT;   // register-held words for this CTA's groups
@@ -1014,7 +1342,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     ctl.pmode = 0;
     ctl.err = 0;
   }
-  for (int k = tid; k < (NBS + NSPLIT) * RT; k += T) S.bins[k] = 0;
+  for (int k = tid; k < S.binrows * RT; k += T) S.bins[k] = 0;
   __syncthreads();
   for (int li = tid; li < ns; li += T) ws[li] = __fmul_rn(wg[4 * g0 + li], scale);   // exact: power-of-two scaling
   if (it0 == 0) {
@@ -1093,7 +1421,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       model_phase(B, C, trees, s0g, W, it, crank, CS);
       if (in_bins) {
         __syncthreads();
-        for (int k = tid; k < NBS * RT; k += T) S.bins[k] = 0;
+        for (int k = tid; k < (S.px ? BIN_ROWS : NBS) * RT; k += T) S.bins[k] = 0;
       }
       if constexpr (CL) { __threadfence(); cg::this_cluster().sync(); }   // every CTA's share, in global memory
       else __syncthreads();
@@ -1118,8 +1446,16 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
     for (int k = 0; k < (G > 0 ? G : 1); k++) lcr[k] = qcr[k] = nlc[k] = nqc[k] = 0u;
     // ---------------------------------------------------------------- trees
     for (int j = 0; j < m; j++) {
-      const Prop P = S.prop[j];
+      Prop P = S.prop[j];
       const int cur = j & 1;
+      // learned cut proposal: a deferred birth, or a death whose reverse birth's cut is scored; collecting launches
+      // also sum the squared residuals of a birth node for its cut example
+      const bool cutb = MP && (P.flags & PROP_DEFER);
+      const bool cutd = MP && B.cimg && P.mode == 2;
+      const bool csq = LP && B.train_cx && P.mode == 1 && !cutb;
+      const bool sqon = cutb || cutd || csq;
+      const int cmode = cutb ? 0 : P.mode;
+      CutOut co{0.0, 0, 0, 0, 0};
       // ------------------------------------------------------------ phase A: row pass | control prefetch
       if (warp > 0) {
         PassU U;
@@ -1141,12 +1477,17 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         U.n = n; U.g0 = g0; U.g1 = g1; U.rt = tid - 32; U.RT = RT; U.nleaf = ctl.nleaf[cur];
         U.apply = j > 0; U.pmode = ctl.pmode; U.pnx = ctl.pnx; U.pc = ctl.pc; U.pL = ctl.pL; U.pR = ctl.pR;
         U.pl = ctl.pl; U.pr = ctl.pr;
-        U.cmode = P.mode; U.cnx = P.nx; U.cc = P.c;
+        U.cmode = cmode; U.cnx = P.nx; U.cc = P.c;
+        U.h0 = S.h0; U.h1 = S.h1; U.hc = S.hc;
+        U.sqs = (float)pow2(C.rss_shift - C.fx_shift);
+        U.xhist = cutb ? 1 : 0;
+        U.sqa = (cutb || csq) ? P.nx : cutd ? P.l : -1;
+        U.sqb = cutd ? P.r : U.sqa;
         if constexpr (G > 0) {
-          if (regs) pass_rows_regs<G>(U, j == 0, lcr, qcr, nlc, nqc);
-          else pass_rows_stream(U);
+          if (regs) pass_rows_regs<G, MP>(U, j == 0, lcr, qcr, nlc, nqc);
+          else pass_rows_stream<MP>(U);
         } else {
-          pass_rows_stream(U);
+          pass_rows_stream<MP>(U);
         }
       } else {
         // control warp: commit tree j-1, fetch tree j+1 into the freed buffer, draw the normals of every slot that
@@ -1155,13 +1496,13 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         if (j > 0) commit_tree<LP>(S, C, B, trees, s0g, j - 1, lane, lead);
         if (j + 1 < m && j > 0) fetch_stats(S, s0g, j + 1, lane);
         const unsigned long long cand = P.cand;
-        if (__popcll(cand) > ZMAX)
+        if (__popcll(cand) > S.zmax)
           for (int s = lane; s < NODES; s += 32)
-            if (((cand >> s) & 1ull) && __popcll(cand & ((1ull << s) - 1ull)) >= ZMAX)
+            if (((cand >> s) & 1ull) && __popcll(cand & ((1ull << s) - 1ull)) >= S.zmax)
               S.z[s] = fbm::fb_normal(seed, (uint32_t)s << 8, (uint32_t)j, (uint32_t)it, fbm::TAG_MU);
       }
       __syncthreads();
-      reduce_totals(S.bins, RT, ctl.nleaf[cur], P.mode, S.tot + cur * TOT);
+      reduce_totals(S.bins, RT, ctl.nleaf[cur], cmode, S.tot + cur * TOT, sqon);
       if (CL) {   // the chain's totals: every CTA's partial totals, pushed through distributed shared memory
         const bool ovf = ctl.nleaf[cur] > NBS;
         __syncthreads();
@@ -1170,6 +1511,13 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         cluster_sum(S, cur, CS, ovf);
       }
       __syncthreads();
+      if constexpr (MP) {
+        if (cutb || cutd) {   // the learned cut (all threads; ends with a barrier)
+          cut_stage<CL>(S, B, C, P, j, it, cur, CS, ctl.sigma, cutb, lead, co);
+          if (cutb) P.c = (uint8_t)co.c;
+          P.logpr = co.logpr;
+        }
+      }
       // ------------------------------------------------------------ phase B: MH and leaf draws, one thread per slot
       // With at least 3 warps, warp 2 evaluates Metropolis-Hastings while warps 0-1 draw every slot's leaf value for
       // the outcome in which that slot is a leaf (a slot is a leaf with the same statistics in both outcomes, or in
@@ -1193,7 +1541,8 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         long long sL0 = 0, sL1 = 0, sR0 = 0, sR1 = 0;
         int nL = 0, nR = 0;
         if (P.mode == 1) {
-          sL0 = tot[NBS + 0]; sL1 = tot[NBS + 1]; nL = (int)tot[NBS + 2];
+          if (cutb) { sL0 = co.sL0; sL1 = co.sL1; nL = co.nL; }
+          else { sL0 = tot[NBS + 0]; sL1 = tot[NBS + 1]; nL = (int)tot[NBS + 2]; }
           sR0 = s0[P.nx] - sL0; sR1 = s1of(P.nx) - sL1; nR = cnt[P.nx] - nL;
         }
         const bool eval = (P.mode == 1 && nL >= 5 && nR >= 5) || P.mode == 2;
@@ -1239,7 +1588,7 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           if (has) {
             const double b = (double)S0s * sci * inv_s2, M = (double)S1s * sci * inv_s2;
             const int zi = __popcll(P.cand & ((1ull << s) - 1ull));
-            const double z = zi < ZMAX ? S.zall[j * ZMAX + zi] : S.z[s];
+            const double z = zi < S.zmax ? S.zall[j * S.zmax + zi] : S.z[s];
             nws = (float)(M / (a_prior + b) + z / sqrt(a_prior + b));
           }
         }
@@ -1282,6 +1631,20 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
           if (nmode == 1 && s == L) ctl.DL = __fsub_rn(nw, thj[P.nx]);
           if (nmode == 1 && s == R) ctl.DR = __fsub_rn(nw, thj[P.nx]);
           if (s == 0) {
+            if constexpr (LP) {   // the cut example of an accepted birth (features of the node before the split)
+              if (B.train_cx && lead && nmode == 1) {
+                const PropX px = S.px[j];
+                float* xf = B.cfeat + (C.off_tree + j) * CUT_IN;
+                if (!cutb) {   // (a deferred birth's features were written by its cut stage)
+                  float xl[CUT_IN];
+                  cut_features(P.dnx, cnt[P.nx], s0[P.nx], s1of(P.nx), tot[NBS + 3], C.fx_shift, C.rss_shift,
+                               ctl.sigma, px.L, px.U, C.numcut[P.v], px.uses, P.v, xl);
+                  for (int k = 0; k < CUT_IN; k++) xf[k] = xl[k];
+                }
+                int* ci3 = B.cinfo + (C.off_tree + j) * 3;
+                ci3[0] = P.c; ci3[1] = px.L; ci3[2] = px.U;
+              }
+            }
             if (cap) ctl.caps++;
             if (nmode == 1) ctl.births++;
             if (nmode == 2) ctl.deaths++;
@@ -1424,7 +1787,9 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
 template <int G, bool CL, int MODE>
 __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it0, int it1) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem, B.cluster);
+  const int cutl = (MODE != MODE_PLAIN && (B.cimg || B.train_cap > 0)) ? 1 : 0;   // the cut layout
+  const Smem S = carve(smem, blockDim.x, B.m_max, B.n_pad_max, B.rows_in_smem, B.cluster, cutl,
+                       B.mvar && B.model_smem);
   if (threadIdx.x == 0) {   // the leaf-statistics buffers' mbarriers, once per launch
     mbar_init(S.bar, 1);
     mbar_init(S.bar + 1, 1);
@@ -1432,6 +1797,13 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) sampler_kernel(DBufs B, int it
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
+  if constexpr (MODE != MODE_PLAIN) {   // the cut head's weights, once per launch
+    if (B.cimg && B.cut_smem) {
+      for (int k = threadIdx.x; k < CIMG_WORDS / 4; k += blockDim.x)
+        reinterpret_cast<uint4*>(S.cimg)[k] = __ldg(reinterpret_cast<const uint4*>(B.cimg) + k);
+      __syncthreads();
+    }
+  }
   if constexpr (MODE != MODE_PLAIN) {   // the proposal model's weights, once per launch
     if (B.mvar && B.model_smem && !bins_hold_model(blockDim.x)) {
       for (int k = threadIdx.x; k < MIMG_WORDS / 4; k += blockDim.x)
@@ -1467,11 +1839,18 @@ static KernelFn kernel_g(int gmax) {
     default: return sampler_kernel<0, CL, MODE>;
   }
 }
+// Collecting runs (training data for the learned proposal, not timed work) take fewer register variants: 3 groups
+// serve 1..3, 6 serve 4..6, larger slices stream.
+template <bool CL>
+static KernelFn kernel_collect(int gmax) {
+  return (gmax >= 1 && gmax <= 3) ? sampler_kernel<3, CL, MODE_COLLECT>
+       : (gmax == 4 || gmax == 6) ? sampler_kernel<6, CL, MODE_COLLECT> : sampler_kernel<0, CL, MODE_COLLECT>;
+}
 static KernelFn kernel_for(int gmax, bool cluster, int mode) {
   if (cluster)
-    return mode == MODE_COLLECT ? kernel_g<true, MODE_COLLECT>(gmax)
+    return mode == MODE_COLLECT ? kernel_collect<true>(gmax)
          : mode == MODE_MODEL ? kernel_g<true, MODE_MODEL>(gmax) : kernel_g<true, MODE_PLAIN>(gmax);
-  return mode == MODE_COLLECT ? kernel_g<false, MODE_COLLECT>(gmax)
+  return mode == MODE_COLLECT ? kernel_collect<false>(gmax)
        : mode == MODE_MODEL ? kernel_g<false, MODE_MODEL>(gmax) : kernel_g<false, MODE_PLAIN>(gmax);
 }
 
@@ -1483,9 +1862,9 @@ int sampler_gmax(int threads, int n_pad_max) {
 
 bool sampler_bins_hold_model(int threads) { return bins_hold_model(threads); }
 
-size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster) {
+size_t sampler_smem_bytes(int threads, int m_max, int n_pad_max, int rows_in_smem, int cluster, int cut) {
   size_t off[NOFF];
-  return smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off);
+  return smem_layout(threads, m_max, n_pad_max, rows_in_smem, cluster, off, cut);
 }
 
 int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster) {
@@ -1521,7 +1900,7 @@ int sampler_max_grid(int threads, size_t smem, int device, int gmax, int cluster
 int launch_sampler(const DBufs& b, int it0, int it1, int threads, int grid, size_t smem, int gmax, int cluster,
                    void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int mode = b.train_cap > 0 ? MODE_COLLECT : b.mvar ? MODE_MODEL : MODE_PLAIN;
+  const int mode = b.train_cap > 0 ? MODE_COLLECT : (b.mvar || b.cimg) ? MODE_MODEL : MODE_PLAIN;
   const KernelFn k = kernel_for(gmax, cluster > 1, mode);
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
   if (cluster > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
@@ -1596,7 +1975,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) debug_pass_kernel(DPassArgs a)
     U.n = a.n; U.g0 = 0; U.g1 = a.n_pad / 4; U.rt = tid - 32; U.RT = RT; U.nleaf = nleaf;
     U.apply = a.apply; U.pmode = a.pmode; U.pnx = a.pnx; U.pc = a.pc; U.pL = a.pL; U.pR = a.pR; U.pl = a.pl; U.pr = a.pr;
     U.cmode = a.stats ? a.cmode : 0; U.cnx = a.cnx; U.cc = a.cc;
-    pass_rows_stream(U);
+    U.h0 = U.h1 = nullptr; U.hc = nullptr; U.sqs = 0.0f; U.xhist = 0; U.sqa = U.sqb = -1;
+    pass_rows_stream<false>(U);
   }
   __syncthreads();
   reduce_totals(bins, RT, nleaf, a.stats ? a.cmode : 0, tot);

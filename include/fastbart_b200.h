@@ -140,6 +140,34 @@ fb_status fb_batch_collect(fb_batch* b, int capacity);
  * births of the run (it can exceed the capacity). */
 fb_status fb_batch_training_data(fb_batch* b, float* x, int* y, uint32_t* mask, int cap, int* count);
 
+/* Learned cutpoint proposal, the second head of the learned proposal: once the tree's fused pass has run, a birth
+ * draws its cutpoint index c from a small MLP over features of the node that include the weighted mean and spread of
+ * the node's current residuals (exact fixed-point sums from that pass): FB_CUT_IN features -> FB_CUT_H -> FB_CUT_H ->
+ * FB_CUT_E (ReLU between the hidden layers), then the logit of cut c is be[c] + emb[c] . e, a softmax over the cut
+ * range of the birth's variable at the node, mixed with BART's uniform cut (src/bart_kernel.cpp:437) with probability
+ * 1 - mix.  The pass keeps a histogram of the node's rows over the variable's codes, so the split sums of the drawn cut
+ * are exact prefix sums.  The Metropolis-Hastings ratio carries the exact probability of the drawn cut and, for a
+ * death, of the reverse birth's cut at the collapsed node, so the posterior is unchanged.  Features: depth / 8,
+ * floor(log2(rows + 1)) / 16, clamp(mean / sigma, -4, 4) / 4, min(sd / sigma, 4) / 4, (U - L + 1) / numcut,
+ * L / numcut, min(uses of the variable in the tree, 8) / 8, 0, then the variable one-hot (32).
+ * Needs CTAs of at least 256 threads.  No counterpart in the reference. */
+#define FB_CUT_IN 40
+#define FB_CUT_H 64
+#define FB_CUT_E 16
+#define FB_CUT_BINS 255
+typedef struct fb_cut_model {
+  const uint16_t* w1; const float* b1;    /* [FB_CUT_H][FB_CUT_IN], [FB_CUT_H] */
+  const uint16_t* w2; const float* b2;    /* [FB_CUT_H][FB_CUT_H], [FB_CUT_H] */
+  const uint16_t* w3; const float* b3;    /* [FB_CUT_E][FB_CUT_H], [FB_CUT_E] */
+  const uint16_t* emb; const float* be;   /* [FB_CUT_BINS][FB_CUT_E], [FB_CUT_BINS] */
+  double mix;                             /* probability of the head's component, in (0, 1]; <= 0: BART's cut */
+} fb_cut_model;
+/* Uses `model` (copied to the device) for the batch's next runs; NULL or mix <= 0 restores BART's uniform cut. */
+fb_status fb_batch_set_cut_proposal(fb_batch* b, const fb_cut_model* model);
+/* The cut examples of the births fb_batch_training_data returns, in the same order: features x [cap][FB_CUT_IN], the
+ * accepted cut c and the cut range [lo, hi] of its variable at the node. */
+fb_status fb_batch_cut_training_data(fb_batch* b, float* x, int* c, int* lo, int* hi, int cap, int* count);
+
 /* Training of the proposal MLP on the device (masked softmax cross-entropy, Adam, minibatches in a fixed seeded
  * order).  Weights start from `init` when non-NULL (else a seeded scaled-uniform initialisation); the trained model
  * is written to out_* (host arrays of the fb_proposal_model shapes, FP32 master weights rounded to BF16).
@@ -159,6 +187,19 @@ fb_status fb_train_proposal(const float* x, const int* y, const uint32_t* mask, 
 fb_status fb_mlp_loss_grad(const fb_proposal_model* model, const float* x, const int* y, const uint32_t* mask,
                            int count, int device, double* loss, float* gw1, float* gb1, float* gw2, float* gb2,
                            float* gw3, float* gb3);
+
+/* Training of the cut head on the device, as fb_train_proposal: softmax cross-entropy over each example's cut range
+ * [lo, hi], Adam, minibatches in a fixed seeded order; the trained head goes to out_* (host arrays of the
+ * fb_cut_model shapes). */
+fb_status fb_train_cut_proposal(const float* x, const int* c, const int* lo, const int* hi, int count,
+                                const fb_train_options* opt, const fb_cut_model* init, uint16_t* out_w1, float* out_b1,
+                                uint16_t* out_w2, float* out_b2, uint16_t* out_w3, float* out_b3, uint16_t* out_emb,
+                                float* out_be, double* losses);
+/* One forward and backward pass of the cut head's training kernels: mean loss and FP32 gradients (fb_cut_model
+ * shapes). */
+fb_status fb_cut_loss_grad(const fb_cut_model* model, const float* x, const int* c, const int* lo, const int* hi,
+                           int count, int device, double* loss, float* gw1, float* gb1, float* gw2, float* gb2,
+                           float* gw3, float* gb3, float* gemb, float* gbe);
 
 /* fbart_cpp (src/glue.cpp:10-62) with R's memory layouts: q is the n x p integer code matrix (column-major), yhat is
  * ndpost x n and varcount ndpost x p (column-major, as Rcpp::NumericMatrix / IntegerMatrix).  trees_text receives

@@ -210,7 +210,7 @@ static void tree_root(otree* t, int root_ngv) {
 
 /* Proposal (bart_kernel.cpp:413-464).  `u` yields the uniforms in order: birth?, node, variable, cutpoint. */
 typedef double (*unif_fn)(void* ctx);
-typedef struct { int mode, nx, v, c; double pr; } oprop;
+typedef struct { int mode, nx, v, c; double pr, corr; } oprop;   /* corr: the learned variable's ratio factor (1: none) */
 static oprop propose(const otree* t, const double* PG, const int* nc, int p, unif_fn u, void* uctx, int guard_death) {
   const double pb = 0.5;
   uint64_t goodm = 0, nogm = 0;
@@ -222,7 +222,7 @@ static oprop propose(const otree* t, const double* PG, const int* nc, int p, uni
   int ngood = popc64(goodm), nnogs = popc64(nogm);
   int single = (t->used == 1ull);
   double PBx = ngood == 0 ? 0 : (single ? 1 : pb);
-  oprop o = {0, 0, 0, 0, 0.0};
+  oprop o = {0, 0, 0, 0, 0.0, 1.0};
   int birth = u(uctx) < PBx;
   if (birth) {
     int nx = select_kth(goodm, (int)(u(uctx) * ngood));
@@ -350,7 +350,7 @@ static oprop propose_model(const otree* t, const double* PG, const int* nc, int 
   int ngood = popc64(goodm), nnogs = popc64(nogm);
   int single = (t->used == 1ull);
   double PBx = ngood == 0 ? 0 : (single ? 1 : pb);
-  oprop o = {0, 0, 0, 0, 0.0};
+  oprop o = {0, 0, 0, 0, 0.0, 1.0};
   *valid_out = 0;
   if (u4[0] < PBx) {
     int nx = select_kth(goodm, (int)(u4[1] * ngood));
@@ -389,7 +389,8 @@ static oprop propose_model(const otree* t, const double* PG, const int* nc, int 
       }
       double Pbotx = (double)1 / ngood;
       o.pr = (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
-      o.pr = o.pr * ((1.0 / (double)p) / mix_prob(M, q, v, p));
+      o.corr = (1.0 / (double)p) / mix_prob(M, q, v, p);
+      o.pr = o.pr * o.corr;
       o.mode = 1; o.nx = nx; o.v = v; o.c = c;
     }
   } else if (nnogs > 0) {
@@ -407,10 +408,230 @@ static oprop propose_model(const otree* t, const double* PG, const int* nc, int 
     uint32_t valid = orc_features(t, nx, count_rows(lf, n, l, r), nx, nc, p, fx);
     orc_mlp_logits(M, fx, z);
     orc_mlp_probs(z, valid, q);
-    o.pr = o.pr * (mix_prob(M, q, (int)t->v[nx], p) * (double)p);
+    o.corr = mix_prob(M, q, (int)t->v[nx], p) * (double)p;
+    o.pr = o.pr * o.corr;
     o.mode = 2; o.nx = nx;
   }
   return o;
+}
+
+/* ================================================================ learned cutpoint proposal (DEV mode) */
+void orc_cut_features(int depth, int cnt, int64_t S0, int64_t S1, int64_t Q, int fx_shift, int rss_shift,
+                      double sigma, int L, int U, int nc, int uses, int v, float* x) {
+  for (int k = 0; k < ORC_CUT_IN; k++) x[k] = 0.0f;
+  x[0] = (float)depth / 8.0f;
+  int bl = 0;
+  for (unsigned c = (unsigned)cnt + 1u; c > 1u; c >>= 1) bl++;
+  x[1] = (float)bl / 16.0f;
+  double mean = 0.0, sd = 0.0;
+  if (S0 > 0) {
+    const double w = (double)S0 * ldexp(1.0, -fx_shift);
+    mean = (double)S1 / (double)S0;
+    const double msq = ((double)Q * ldexp(1.0, -rss_shift)) / w;
+    const double var = msq - mean * mean;
+    sd = var > 0.0 ? sqrt(var) : 0.0;
+  }
+  double fm = mean / sigma;
+  fm = fm < -4.0 ? -4.0 : (fm > 4.0 ? 4.0 : fm);
+  double fs = sd / sigma;
+  fs = fs > 4.0 ? 4.0 : fs;
+  x[2] = (float)(fm * 0.25);
+  x[3] = (float)(fs * 0.25);
+  x[4] = (float)(U - L + 1) / (float)nc;
+  x[5] = (float)L / (float)nc;
+  x[6] = (float)(uses < 8 ? uses : 8) / 8.0f;
+  if (v >= 0 && v < 32) x[8 + v] = 1.0f;
+}
+
+void orc_cut_logits(const orc_cut_model* M, const float* x, int L, int U, float* z) {
+  float h1[ORC_CUT_H], h2[ORC_CUT_H], e[ORC_CUT_E];
+  for (int h = 0; h < ORC_CUT_H; h++) {
+    float a = M->b1[h];
+    for (int k = 0; k < ORC_CUT_IN; k++) a = a + bf16f(M->w1[h * ORC_CUT_IN + k]) * x[k];
+    h1[h] = a > 0.0f ? a : 0.0f;
+  }
+  for (int h = 0; h < ORC_CUT_H; h++) {
+    float a = M->b2[h];
+    for (int k = 0; k < ORC_CUT_H; k++) a = a + bf16f(M->w2[h * ORC_CUT_H + k]) * h1[k];
+    h2[h] = a > 0.0f ? a : 0.0f;
+  }
+  for (int k = 0; k < ORC_CUT_E; k++) {
+    float a = M->b3[k];
+    for (int f = 0; f < ORC_CUT_H; f++) a = a + bf16f(M->w3[k * ORC_CUT_H + f]) * h2[f];
+    e[k] = a;
+  }
+  for (int c = L; c <= U; c++) {
+    float a = M->be[c];
+    for (int k = 0; k < ORC_CUT_E; k++) a = a + bf16f(M->emb[c * ORC_CUT_E + k]) * e[k];
+    z[c] = a;
+  }
+}
+
+double orc_cut_softmax(const float* z, int L, int U, double* ex) {
+  double zmax = (double)z[L];
+  for (int c = L + 1; c <= U; c++)
+    if ((double)z[c] > zmax) zmax = (double)z[c];
+  for (int c = L; c <= U; c++) ex[c] = orc_exp((double)z[c] - zmax);
+  double S = 0.0;
+  for (int b0 = L; b0 <= U; b0 += 8) {
+    double bs = 0.0;
+    for (int c = b0; c < b0 + 8 && c <= U; c++) bs = bs + ex[c];
+    S = S + bs;
+  }
+  return S;
+}
+
+/* Draws the cut of a birth from the mixture (mix: the model's softmax over [L, U], else uniform on [L, U]); *q_out
+ * receives the mixture's probability of the drawn cut. */
+static int cut_draw(const double* ex, double S, int L, int U, double umix, double uc, double mix, double* q_out) {
+  const int range = U - L + 1;
+  int c = U;
+  if (umix < mix) {
+    const double target = uc * S;
+    double P = 0.0;
+    int found = 0;
+    for (int b0 = L; b0 <= U && !found; b0 += 8) {
+      double bs = 0.0;
+      for (int k = b0; k < b0 + 8 && k <= U; k++) bs = bs + ex[k];
+      const double P1 = P + bs;
+      if (P1 > target) {
+        double run = P;
+        c = b0 + 7 < U ? b0 + 7 : U;
+        for (int k = b0; k < b0 + 8 && k <= U; k++) {
+          run = run + ex[k];
+          if (run > target) { c = k; break; }
+        }
+        found = 1;
+      }
+      P = P1;
+    }
+  } else {
+    c = L + (int)(uc * range);
+    if (c > U) c = U;
+  }
+  *q_out = mix * (ex[c] / S) + (1.0 - mix) * (1.0 / (double)range);
+  return c;
+}
+
+/* the mixture's probability of cut c of [L, U] */
+static double cut_prob(const double* ex, double S, int L, int U, int c, double mix) {
+  return mix * (ex[c] / S) + (1.0 - mix) * (1.0 / (double)(U - L + 1));
+}
+
+static int uses_of(const otree* t, int v, int exclude) {
+  int u = 0;
+  for (int s = 0; s < ORC_NODES; s++)
+    if (BIT(t->used, s) && !BIT(t->leaf, s) && s != exclude && (int)t->v[s] == v) u++;
+  return u;
+}
+
+/* BART's birth ratio of propose() (bart_kernel.cpp:441-451) at node nx for cut c of range [bL, bU] */
+static double birth_pr_at(const otree* t, const double* PG, int nx, int c, int bL, int bU) {
+  const double pb = 0.5;
+  uint64_t goodm = 0, nogm = 0;
+  for (int s = 0; s < ORC_NODES; s++) {
+    int isleaf = (int)BIT(t->leaf, s), isused = (int)BIT(t->used, s);
+    if (isused && isleaf && t->ngv[s] > 0) goodm |= 1ull << s;
+    if (isused && !isleaf && BIT(t->leaf, (int)t->l[s]) && BIT(t->leaf, (int)t->r[s])) nogm |= 1ull << s;
+  }
+  int ngood = popc64(goodm), nnogs = popc64(nogm);
+  double PBx = ngood == 0 ? 0 : (t->used == 1ull ? 1 : pb);
+  int dnx = t->d[nx];
+  double PGnx = PG[dnx], PGly, PGry;
+  if (t->ngv[nx] > 1) { PGly = PGry = PG[dnx + 1]; }
+  else { PGly = (c - 1 < bL) ? 0 : PG[dnx + 1]; PGry = (bU < c + 1) ? 0 : PG[dnx + 1]; }
+  double PDy = (ngood > 1) ? 1 - pb : ((PGry == 0 && PGly == 0) ? 1 : 1 - pb);
+  double Pnogy;
+  if (nx == 0) Pnogy = 1;
+  else {
+    int pa = t->par[nx];
+    int panog = BIT(t->leaf, (int)t->l[pa]) && BIT(t->leaf, (int)t->r[pa]);
+    Pnogy = panog ? (double)1 / nnogs : (double)1 / (nnogs + 1);
+  }
+  double Pbotx = (double)1 / ngood;
+  return (PGnx * (1 - PGly) * (1 - PGry) * PDy * Pnogy) / ((1 - PGnx) * Pbotx * PBx);
+}
+
+double orc_cut_loss_grad(const orc_cut_model* M, const float* X, const int* cy, const int* lo, const int* hi, int B,
+                         double* gw1, double* gb1, double* gw2, double* gb2, double* gw3, double* gb3, double* gemb,
+                         double* gbe) {
+  const int I = ORC_CUT_IN, H = ORC_CUT_H, E = ORC_CUT_E, NB = ORC_CUT_BINS;
+  memset(gw1, 0, sizeof(double) * H * I); memset(gb1, 0, sizeof(double) * H);
+  memset(gw2, 0, sizeof(double) * H * H); memset(gb2, 0, sizeof(double) * H);
+  memset(gw3, 0, sizeof(double) * E * H); memset(gb3, 0, sizeof(double) * E);
+  memset(gemb, 0, sizeof(double) * NB * E); memset(gbe, 0, sizeof(double) * NB);
+  double loss = 0.0;
+  for (int b = 0; b < B; b++) {
+    const float* x = X + (size_t)b * I;
+    double h1[ORC_CUT_H], h2[ORC_CUT_H], e[ORC_CUT_E], z[ORC_CUT_BINS], dz[ORC_CUT_BINS], de[ORC_CUT_E];
+    double d2[ORC_CUT_H], d1[ORC_CUT_H];
+    for (int h = 0; h < H; h++) {
+      double a = M->b1[h];
+      for (int k = 0; k < I; k++) a += (double)bf16f(M->w1[h * I + k]) * x[k];
+      h1[h] = a > 0 ? a : 0;
+    }
+    for (int h = 0; h < H; h++) {
+      double a = M->b2[h];
+      for (int k = 0; k < H; k++) a += (double)bf16f(M->w2[h * H + k]) * h1[k];
+      h2[h] = a > 0 ? a : 0;
+    }
+    for (int k = 0; k < E; k++) {
+      double a = M->b3[k];
+      for (int f = 0; f < H; f++) a += (double)bf16f(M->w3[k * H + f]) * h2[f];
+      e[k] = a;
+    }
+    const int L = lo[b], U = hi[b];
+    double zmax = -1e300;
+    for (int c = L; c <= U; c++) {
+      double a = M->be[c];
+      for (int k = 0; k < E; k++) a += (double)bf16f(M->emb[c * E + k]) * e[k];
+      z[c] = a;
+      if (a > zmax) zmax = a;
+    }
+    double S = 0.0;
+    for (int c = L; c <= U; c++) S += exp(z[c] - zmax);
+    loss += -(z[cy[b]] - zmax - log(S));
+    for (int k = 0; k < E; k++) de[k] = 0.0;
+    for (int c = L; c <= U; c++) {
+      dz[c] = exp(z[c] - zmax) / S - (c == cy[b] ? 1.0 : 0.0);
+      gbe[c] += dz[c];
+      for (int k = 0; k < E; k++) {
+        gemb[c * E + k] += dz[c] * e[k];
+        de[k] += dz[c] * (double)bf16f(M->emb[c * E + k]);
+      }
+    }
+    for (int k = 0; k < E; k++) {
+      gb3[k] += de[k];
+      for (int f = 0; f < H; f++) gw3[k * H + f] += de[k] * h2[f];
+    }
+    for (int f = 0; f < H; f++) {
+      double a = 0.0;
+      for (int k = 0; k < E; k++) a += de[k] * (double)bf16f(M->w3[k * H + f]);
+      d2[f] = h2[f] > 0 ? a : 0.0;
+    }
+    for (int h = 0; h < H; h++) {
+      gb2[h] += d2[h];
+      for (int k = 0; k < H; k++) gw2[h * H + k] += d2[h] * h1[k];
+    }
+    for (int k = 0; k < H; k++) {
+      double a = 0.0;
+      for (int h = 0; h < H; h++) a += d2[h] * (double)bf16f(M->w2[h * H + k]);
+      d1[k] = h1[k] > 0 ? a : 0.0;
+    }
+    for (int h = 0; h < H; h++) {
+      gb1[h] += d1[h];
+      for (int k = 0; k < I; k++) gw1[h * I + k] += d1[h] * x[k];
+    }
+  }
+  const double inv = 1.0 / (double)B;
+  for (int k = 0; k < H * I; k++) gw1[k] *= inv;
+  for (int k = 0; k < H; k++) { gb1[k] *= inv; gb2[k] *= inv; }
+  for (int k = 0; k < H * H; k++) gw2[k] *= inv;
+  for (int k = 0; k < E * H; k++) gw3[k] *= inv;
+  for (int k = 0; k < E; k++) gb3[k] *= inv;
+  for (int k = 0; k < NB * E; k++) gemb[k] *= inv;
+  for (int k = 0; k < NB; k++) gbe[k] *= inv;
+  return loss * inv;
 }
 
 double orc_mlp_loss_grad(const orc_model* M, const float* X, const int* y, const uint32_t* mask, int B,
@@ -771,6 +992,26 @@ void orc_pass_dev(int n, uint8_t* leaf_prev, const uint8_t* leaf_cur, float* r, 
   }
 }
 
+/* Over the rows of tree j's leaves a and b (after the pass applied tree j-1's move to r): Q = sum fx2(w R^2) with R =
+   r + theta of the row's leaf; with H0 non-NULL also, per code of qv, sum fx(w), sum fx(w R) and the row count. */
+static void node_extras(int n, const uint8_t* lf, int a, int b, const float* r, const float* w, const float* thc,
+                        const uint8_t* qv, int fx_shift, int rss_shift, int64_t* Q, int64_t* H0, int64_t* H1,
+                        int* Hc) {
+  const float scale = ldexpf(1.0f, fx_shift), sqs = ldexpf(1.0f, rss_shift - fx_shift);
+  *Q = 0;
+  for (int i = 0; i < n; i++) {
+    if (lf[i] != a && lf[i] != b) continue;
+    const float ws = w[i] * scale, R = r[i] + thc[lf[i]], wr = ws * R;
+    *Q += (int64_t)llrintf((wr * R) * sqs);
+    if (H0) {
+      const int cd = qv[i];
+      H0[cd] += (int64_t)llrintf(ws);
+      H1[cd] += (int64_t)llrintf(wr);
+      Hc[cd]++;
+    }
+  }
+}
+
 typedef struct { double u[4]; int k; } dunif;
 static double dunif_cb(void* ctx) { dunif* d = (dunif*)ctx; return d->u[d->k++ & 3]; }
 static inline double lh_dev(double b, double M, double t2) { double k = b * t2 + 1.0; return -0.5 * orc_log(k) + 0.5 * M * M * t2 / k; }
@@ -831,12 +1072,67 @@ static int fit_dev(const orc_chain* C, orc_out* o) {
           fvalid = orc_features(t, cp.nx, count_rows(LF + (size_t)j * n, n, cp.nx, cp.nx), -1, nc, p, feat);
         }
       }
-      orc_prop cpp = {cp.mode, cp.nx, cp.v, cp.c};
+      /* a learned cut proposal draws a birth's cut after the pass: the pass then accumulates no split sums */
+      const orc_cut_model* CM = (C->cut && C->cut->mix > 0.0) ? C->cut : NULL;
+      const int defer = CM && cp.mode == 1;
+      orc_prop cpp = {defer ? 0 : cp.mode, cp.nx, cp.v, cp.c};
       float thc[ORC_NODES];
       for (int s = 0; s < ORC_NODES; s++) thc[s] = t->th[s];
       orc_pass_dev(n, j > 0 ? LF + (size_t)(j - 1) * n : NULL, LF + (size_t)j * n, r, w,
                    pu.mode == 1 ? C->q + (size_t)pu.v * n : NULL, cp.mode == 1 ? C->q + (size_t)cp.v * n : NULL, &pu,
                    tho, thn, j > 0, &cpp, thc, C->fx_shift, &st);
+      /* the cut proposal's features (and, for a deferred birth, its cut and split sums) */
+      float cx[ORC_CUT_IN];
+      int cxL = 0, cxU = 0;
+      const int want_cx = o->train_cap > 0 && o->train_cx && cp.mode == 1;
+      if (cp.mode == 1 && (defer || want_cx)) {
+        static int64_t H0[256], H1[256];
+        static int Hc[256];
+        memset(H0, 0, sizeof H0); memset(H1, 0, sizeof H1); memset(Hc, 0, sizeof Hc);
+        const int nx = cp.nx, v = cp.v;
+        node_range(t, nx, v, nc[v], &cxL, &cxU);
+        int64_t Q;
+        const uint8_t* lfj = LF + (size_t)j * n;
+        node_extras(n, lfj, nx, nx, r, w, thc, C->q + (size_t)v * n, C->fx_shift, C->rss_shift, &Q, H0, H1, Hc);
+        const int cnt = count_rows(lfj, n, nx, nx);
+        orc_cut_features(t->d[nx], cnt, st.S0[nx], st.S1[nx], Q, C->fx_shift, C->rss_shift, sigma, cxL, cxU, nc[v],
+                         uses_of(t, v, -1), v, cx);
+        if (defer) {
+          float z[ORC_CUT_BINS];
+          double ex[ORC_CUT_BINS];
+          orc_cut_logits(CM, cx, cxL, cxU, z);
+          const double S = orc_cut_softmax(z, cxL, cxU, ex);
+          uint32_t x3[4];
+          philox_seed(seed, 0u, (uint32_t)j, (uint32_t)it, ORC_TAG_PROP3, x3);
+          double qc;
+          const int c = cut_draw(ex, S, cxL, cxU, u32d(x3[0]), u32d(x3[1]), CM->mix, &qc);
+          const double corr_c = (1.0 / (double)(cxU - cxL + 1)) / qc;
+          double pr = birth_pr_at(t, PG, nx, c, cxL, cxU);
+          pr = pr * cp.corr;
+          pr = pr * corr_c;
+          cp.pr = pr; cp.c = c;
+          int64_t sL0 = 0, sL1 = 0;
+          int nL = 0;
+          for (int k = 0; k <= c; k++) { sL0 += H0[k]; sL1 += H1[k]; nL += Hc[k]; }
+          st.sL0 = sL0; st.sL1 = sL1; st.nL = nL;
+          st.sR0 = st.S0[nx] - sL0; st.sR1 = st.S1[nx] - sL1; st.nR = cnt - nL;
+        }
+      } else if (CM && cp.mode == 2) {   /* the reverse birth's cut probability at the collapsed node */
+        const int nx = cp.nx, l = t->l[nx], rr = t->r[nx], v = t->v[nx], cn = t->c[nx];
+        int L, U;
+        node_range(t, nx, v, nc[v], &L, &U);
+        int64_t Q;
+        const uint8_t* lfj = LF + (size_t)j * n;
+        node_extras(n, lfj, l, rr, r, w, thc, NULL, C->fx_shift, C->rss_shift, &Q, NULL, NULL, NULL);
+        float z[ORC_CUT_BINS];
+        double ex[ORC_CUT_BINS];
+        orc_cut_features(t->d[nx], count_rows(lfj, n, l, rr), st.S0[l] + st.S0[rr], st.S1[l] + st.S1[rr], Q,
+                         C->fx_shift, C->rss_shift, sigma, L, U, nc[v], uses_of(t, v, nx), v, cx);
+        orc_cut_logits(CM, cx, L, U, z);
+        const double S = orc_cut_softmax(z, L, U, ex);
+        const double corr_c = cut_prob(ex, S, L, U, cn, CM->mix) * (double)(U - L + 1);
+        cp.pr = cp.pr * corr_c;
+      }
       orc_upd nu_ = {0, cp.nx, cp.v, cp.c, 0, 0, 0, 0};
       int64_t S0[ORC_NODES], S1[ORC_NODES];
       for (int s = 0; s < ORC_NODES; s++) { S0[s] = st.S0[s]; S1[s] = st.S1[s]; }
@@ -861,6 +1157,12 @@ static int fit_dev(const orc_chain* C, orc_out* o) {
                   memcpy(o->train_x + (size_t)o->train_count * ORC_MLP_IN, feat, sizeof feat);
                   o->train_y[o->train_count] = cp.v;
                   o->train_mask[o->train_count] = fvalid;
+                  if (o->train_cx) {
+                    memcpy(o->train_cx + (size_t)o->train_count * ORC_CUT_IN, cx, sizeof cx);
+                    o->train_c[o->train_count] = cp.c;
+                    o->train_lo[o->train_count] = cxL;
+                    o->train_hi[o->train_count] = cxU;
+                  }
                   o->train_count++;
                 }
               }

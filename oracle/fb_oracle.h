@@ -36,7 +36,7 @@ enum { ORC_MODE_REF = 0, ORC_MODE_DEV = 1 };
 
 /* Philox counter tags (word 3 of the counter) used by the DEV arithmetic. */
 enum { ORC_TAG_PROP = 1, ORC_TAG_MH = 2, ORC_TAG_MU = 3, ORC_TAG_SIG_N = 4, ORC_TAG_SIG_U = 5, ORC_TAG_Z_N = 6,
-       ORC_TAG_Z_E = 7, ORC_TAG_PROP2 = 8 };
+       ORC_TAG_Z_E = 7, ORC_TAG_PROP2 = 8, ORC_TAG_PROP3 = 9 };
 #define ORC_INIT_SWEEP 0xFFFFFFFFu
 
 /* Learned split-variable proposal (DEV mode): an MLP of ORC_MLP_IN node features -> ORC_MLP_H -> ORC_MLP_H ->
@@ -53,6 +53,26 @@ typedef struct {
   double mix;                            /* probability of the model component (0: plain proposal) */
 } orc_model;
 
+/* Learned cutpoint proposal (DEV mode), drawn after the tree's fused pass: node features including the residual
+ * mean and spread of the node's rows (ORC_CUT_IN) -> ORC_CUT_H -> ORC_CUT_H -> ORC_CUT_E (ReLU between the hidden
+ * layers), then one logit per cutpoint index c, be[c] + emb[c] . e; BF16 weights, FP32 sums without fused
+ * multiply-add.  A birth draws its cutpoint from the softmax over the variable's cut range at the node with probability
+ * mix, else uniformly as BART does; the MH ratio carries the exact probabilities of the birth's cut and of the
+ * reverse birth's cut of a death.  Features (orc_cut_features): x[0] depth / 8, x[1] floor(log2(cnt + 1)) / 16,
+ * x[2] clamp(mean / sigma, -4, 4) / 4, x[3] min(sd / sigma, 4) / 4 (weighted residual mean and sd of the node's rows),
+ * x[4] (U - L + 1) / numcut, x[5] L / numcut, x[6] min(uses of v, 8) / 8, x[7] 0, x[8 + k] = (k == v). */
+#define ORC_CUT_IN 40
+#define ORC_CUT_H 64
+#define ORC_CUT_E 16
+#define ORC_CUT_BINS 255
+typedef struct {
+  const uint16_t* w1; const float* b1;   /* [H][IN], [H] */
+  const uint16_t* w2; const float* b2;   /* [H][H], [H] */
+  const uint16_t* w3; const float* b3;   /* [E][H], [E] */
+  const uint16_t* emb; const float* be;  /* [BINS][E], [BINS] */
+  double mix;
+} orc_cut_model;
+
 typedef struct {
   int n, p, m, nskip, ndpost;
   const uint8_t* q;       /* [p][n] cutpoint codes: x < xi[v][c]  <=>  q <= c */
@@ -67,6 +87,7 @@ typedef struct {
   int fx_shift;           /* DEV: w and w*r are summed as llrint(x * 2^fx_shift) */
   int rss_shift;          /* DEV: w*e^2 is summed as llrint(x * 2^rss_shift) */
   const orc_model* model; /* DEV: learned proposal, or NULL */
+  const orc_cut_model* cut; /* DEV: learned cutpoint proposal, or NULL */
 } orc_chain;
 
 typedef struct {
@@ -82,6 +103,11 @@ typedef struct {
   int* train_y;
   uint32_t* train_mask;
   int train_cap, train_count;
+  /* DEV: the cutpoint examples of the same accepted births: features, cut, cut range [lo, hi] (when train_cx set) */
+  float* train_cx;        /* [train_cap][ORC_CUT_IN] */
+  int* train_c;
+  int* train_lo;
+  int* train_hi;
 } orc_out;
 
 /* Whole-chain sampler.  Returns 0 on success, <0 on a bad shape. */
@@ -110,6 +136,17 @@ void orc_mlp_probs(const float* z, uint32_t valid, double* q);
  * computed in FP64 from the same BF16 weights (the checker of the device training kernels). */
 double orc_mlp_loss_grad(const orc_model* M, const float* X, const int* y, const uint32_t* mask, int B,
                          double* gw1, double* gb1, double* gw2, double* gb2, double* gw3, double* gb3);
+/* Cutpoint-proposal features, logits over c in [L, U] (z[c]; other entries untouched) and the masked softmax in the
+ * device's summation order (blocks of 8 consecutive c from L, each summed in order, block sums in order); ex[c]
+ * receives exp(z[c] - max), the return value is the sum. */
+void orc_cut_features(int depth, int cnt, int64_t S0, int64_t S1, int64_t Q, int fx_shift, int rss_shift,
+                      double sigma, int L, int U, int nc, int uses, int v, float* x);
+void orc_cut_logits(const orc_cut_model* M, const float* x, int L, int U, float* z);
+double orc_cut_softmax(const float* z, int L, int U, double* ex);
+/* Mean cross-entropy of the cut head over a batch (softmax over [lo, hi] of each example) and its gradients. */
+double orc_cut_loss_grad(const orc_cut_model* M, const float* X, const int* c, const int* lo, const int* hi, int B,
+                         double* gw1, double* gb1, double* gw2, double* gb2, double* gw3, double* gb3, double* gemb,
+                         double* gbe);
 double orc_log(double x);
 double orc_exp(double x);
 double orc_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag);

@@ -35,16 +35,35 @@ class _Chain(C.Structure):
                 ("numcut", C.c_void_p), ("pgtab", C.c_void_p),
                 ("tau", C.c_double), ("lambda_", C.c_double), ("nu", C.c_double), ("sigest", C.c_double),
                 ("offset", C.c_double), ("seed", C.c_uint64), ("probit", C.c_int), ("fx_shift", C.c_int),
-                ("rss_shift", C.c_int), ("model", C.c_void_p)]
+                ("rss_shift", C.c_int), ("model", C.c_void_p), ("cut", C.c_void_p)]
 
 
 class _Out(C.Structure):
     _fields_ = [("sigma", C.c_void_p), ("fmean", C.c_void_p), ("yhat", C.c_void_p), ("trees", C.c_void_p),
                 ("moves", C.c_int * 3), ("rtnorm_caps", C.c_int), ("train_x", C.c_void_p), ("train_y", C.c_void_p),
-                ("train_mask", C.c_void_p), ("train_cap", C.c_int), ("train_count", C.c_int)]
+                ("train_mask", C.c_void_p), ("train_cap", C.c_int), ("train_count", C.c_int),
+                ("train_cx", C.c_void_p), ("train_c", C.c_void_p), ("train_lo", C.c_void_p), ("train_hi", C.c_void_p)]
 
 
 MLP_IN, MLP_H, MLP_OUT = 98, 64, 32
+CUT_IN, CUT_H, CUT_E, CUT_BINS = 40, 64, 16, 255
+
+
+class _CutModel(C.Structure):
+    _fields_ = [("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_void_p), ("emb", C.c_void_p), ("be", C.c_void_p), ("mix", C.c_double)]
+
+
+CUT_KEYS = (("w1", np.uint16), ("b1", np.float32), ("w2", np.uint16), ("b2", np.float32), ("w3", np.uint16),
+            ("b3", np.float32), ("emb", np.uint16), ("be", np.float32))
+
+
+def _cut_struct(model: dict, keep: list):
+    """orc_cut_model from a dict of w1 [64][40], w2 [64][64], w3 [16][64], emb [255][16] (uint16 BF16 bits), b1, b2, b3,
+    be (float32), mix."""
+    arrs = {k: np.ascontiguousarray(model[k], dtype=dt) for k, dt in CUT_KEYS}
+    keep += list(arrs.values())
+    return _CutModel(*(arrs[k].ctypes.data for k, _ in CUT_KEYS), float(model.get("mix", 0.5)))
 
 
 class _Model(C.Structure):
@@ -118,6 +137,10 @@ def lib():
         L.orc_mlp_logits.restype = None
         L.orc_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 6
         L.orc_mlp_loss_grad.restype = C.c_double
+        L.orc_cut_logits.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.orc_cut_logits.restype = None
+        L.orc_cut_loss_grad.argtypes = [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 8
+        L.orc_cut_loss_grad.restype = C.c_double
         L.orc_predict_draw.argtypes = [C.POINTER(_CT), C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, _f64p]
         L.orc_predict_draw.restype = C.c_int
         L.orc_trees_text.argtypes = [_u64p, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
@@ -149,7 +172,8 @@ def _keep(*arrs):
     return [np.ascontiguousarray(a) for a in arrs]
 
 
-def fit(ch: dict, mode: int, want_trees: bool = True, model: dict | None = None, train_cap: int = 0) -> dict:
+def fit(ch: dict, mode: int, want_trees: bool = True, model: dict | None = None, train_cap: int = 0,
+        cut: dict | None = None) -> dict:
     """Runs one chain in the oracle.  ch keys: q [p][n] u8, y, wt, ybin, numcut, pgtab, tau, lambda, nu, sigest,
     offset, seed, probit, nskip, ndpost, ntree, fx_shift, rss_shift.  DEV mode: `model` = learned proposal (see
     _model_struct); train_cap > 0 collects accepted births as training examples (train_x, train_y, train_mask)."""
@@ -171,6 +195,10 @@ def fit(ch: dict, mode: int, want_trees: bool = True, model: dict | None = None,
         ms = _model_struct(model, keep)
         keep.append(ms)
         c.model = C.cast(C.pointer(ms), C.c_void_p)
+    if cut is not None:
+        cs = _cut_struct(cut, keep)
+        keep.append(cs)
+        c.cut = C.cast(C.pointer(cs), C.c_void_p)
     S = nskip + ndpost
     sigma = np.zeros(S)
     fmean = np.zeros(n)
@@ -181,12 +209,39 @@ def fit(ch: dict, mode: int, want_trees: bool = True, model: dict | None = None,
     tm = np.zeros(max(train_cap, 1), dtype=np.uint32)
     o = _Out(sigma.ctypes.data, fmean.ctypes.data, yhat.ctypes.data, trees.ctypes.data if trees is not None else None)
     o.train_x, o.train_y, o.train_mask, o.train_cap = tx.ctypes.data, ty.ctypes.data, tm.ctypes.data, int(train_cap)
+    cx = np.zeros((max(train_cap, 1), CUT_IN), dtype=np.float32)
+    cc, clo, chi = (np.zeros(max(train_cap, 1), dtype=np.int32) for _ in range(3))
+    o.train_cx, o.train_c, o.train_lo, o.train_hi = cx.ctypes.data, cc.ctypes.data, clo.ctypes.data, chi.ctypes.data
     rc = lib().orc_fit(C.byref(c), mode, C.byref(o))
     if rc != 0:
         raise ValueError(f"orc_fit returned {rc}")
     k = o.train_count
     return dict(sigma=sigma, fmean=fmean, yhat=yhat, trees=trees, moves=np.array(list(o.moves)),
-                rtnorm_caps=o.rtnorm_caps, train_x=tx[:k], train_y=ty[:k], train_mask=tm[:k])
+                rtnorm_caps=o.rtnorm_caps, train_x=tx[:k], train_y=ty[:k], train_mask=tm[:k], train_cx=cx[:k],
+                train_c=cc[:k], train_lo=clo[:k], train_hi=chi[:k])
+
+
+def cut_logits(cut: dict, x: np.ndarray, lo: int, hi: int) -> np.ndarray:
+    """The cut head's logits over [lo, hi] (float32, other entries 0)."""
+    keep: list = []
+    cs = _cut_struct(cut, keep)
+    xs = np.ascontiguousarray(x, dtype=np.float32)
+    z = np.zeros(CUT_BINS, dtype=np.float32)
+    lib().orc_cut_logits(C.byref(cs), xs.ctypes.data, int(lo), int(hi), z.ctypes.data)
+    return z
+
+
+def cut_loss_grad(cut: dict, X, c, lo, hi) -> tuple[float, dict]:
+    keep: list = []
+    cs = _cut_struct(cut, keep)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    c, lo, hi = (np.ascontiguousarray(a, dtype=np.int32) for a in (c, lo, hi))
+    shapes = dict(w1=(CUT_H, CUT_IN), b1=(CUT_H,), w2=(CUT_H, CUT_H), b2=(CUT_H,), w3=(CUT_E, CUT_H), b3=(CUT_E,),
+                  emb=(CUT_BINS, CUT_E), be=(CUT_BINS,))
+    g = {k: np.zeros(v) for k, v in shapes.items()}
+    loss = lib().orc_cut_loss_grad(C.byref(cs), X.ctypes.data, c.ctypes.data, lo.ctypes.data, hi.ctypes.data, len(c),
+                                   *(g[k].ctypes.data for k in ("w1", "b1", "w2", "b2", "w3", "b3", "emb", "be")))
+    return float(loss), g
 
 
 def mlp_logits(model: dict, x: np.ndarray) -> np.ndarray:

@@ -221,3 +221,35 @@ def test_predict_oracle_matches_reference_library(orc, seed):
         ref.predict_draw(cols, 6, 0.0)
     with pytest.raises(ValueError, match="columns"):
         ref.predict_draw(cols[:-1], 1, 0.0)
+
+
+def test_oracle_cut_head_forward_and_examples(orc):
+    """The cut head's logits equal a float64 numpy forward of the same BF16 weights (to FP32 rounding); a collecting
+    chain's cut examples lie in their ranges, carry the variable one-hot, and a chain with the cut head is
+    deterministic and differs from BART's uniform cut."""
+    rng = np.random.default_rng(3)
+
+    def bf(a):
+        return (np.asarray(a, np.float32).view(np.uint32) >> 16).astype(np.uint16)
+
+    cut = dict(w1=bf(rng.normal(0, .3, (64, 40))), b1=rng.normal(0, .1, 64).astype(np.float32),
+               w2=bf(rng.normal(0, .3, (64, 64))), b2=rng.normal(0, .1, 64).astype(np.float32),
+               w3=bf(rng.normal(0, .3, (16, 64))), b3=rng.normal(0, .1, 16).astype(np.float32),
+               emb=bf(rng.normal(0, 1, (255, 16))), be=rng.normal(0, .5, 255).astype(np.float32), mix=0.5)
+    f = {k: (v.astype(np.uint32) << 16).view(np.float32).astype(np.float64) if v.dtype == np.uint16 else
+         v.astype(np.float64) for k, v in cut.items() if k != "mix"}
+    x = rng.random(40).astype(np.float32)
+    h1 = np.maximum(f["w1"] @ x + f["b1"], 0)
+    h2 = np.maximum(f["w2"] @ h1 + f["b2"], 0)
+    e = f["w3"] @ h2 + f["b3"]
+    z = f["emb"] @ e + f["be"]
+    zo = orc.cut_logits(cut, x, 3, 200)
+    assert np.allclose(zo[3:201], z[3:201], rtol=1e-4, atol=1e-4)
+    ch = W.fwbart_friedman(n=600, p=6, seed=5, ntree=15, nskip=30, ndpost=10)
+    o = orc.fit(ch, orc.MODE_DEV, train_cap=5000)
+    assert len(o["train_c"]) == o["moves"][0] > 0
+    assert np.all((o["train_lo"] <= o["train_c"]) & (o["train_c"] <= o["train_hi"]))
+    assert np.array_equal(np.argmax(o["train_cx"][:, 8:], axis=1), o["train_y"])
+    a, b = orc.fit(ch, orc.MODE_DEV, cut=cut), orc.fit(ch, orc.MODE_DEV, cut=cut)
+    assert np.array_equal(a["trees"], b["trees"])
+    assert not np.array_equal(a["trees"], orc.fit(ch, orc.MODE_DEV)["trees"])
