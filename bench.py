@@ -118,6 +118,7 @@ def predict_fresh_rows(F, ch, out, stream, device):
     assert np.array_equal(chk, od[NDPOST - 1].cpu().numpy()), "bulk and single-draw predict disagree"
     return {"row_draws_per_s": NDPOST * n / sec, "ms_per_call": 1000 * sec, "draws": NDPOST, "rows": n,
             "ntree": ch["ntree"], "hbm_gbs": (n * p * 8 + NDPOST * n * 8) / sec / 1e9,
+            "evaluator": ct.evaluator(n, NDPOST)[0],
             "note": "all 100 draws on fresh rows in one fb_predict_draws_device call; x read once, results written once"}
 
 
@@ -549,6 +550,7 @@ def bench_ours(args):
 PRED_DRAWS, PRED_ROWS, PRED_P, PRED_CPU_ROWS = 1000, 1_000_000, 32, 100_000
 PRED_METRIC = "predict_draw row-draws/s (1,000 draws x 200 trees on 1,000,000 rows x 32 FP64 columns)"
 PRED_UNIT = "row-draws/s"
+PRED_CHANGE = 0.15   # share of trees whose structure changes from one posterior draw to the next (posterior leg)
 
 
 def _pred_newdata(rows: int, seed: int = 21):
@@ -668,6 +670,39 @@ def bench_predict(args):
             "frac": alg / per_s / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
             "algorithmic_bytes": alg,
             "node_steps_note": "x read once, every output written once, each draw's packed nodes and leaf values read"}
+    roof["evaluator"] = ct.evaluator(PRED_ROWS, PRED_DRAWS)[0]
+    # the same call on draws shaped like one chain's consecutive posterior draws (most tree structures kept from
+    # draw to draw, every leaf value redrawn): the evaluator then carries each row's leaves across draws
+    post = None
+    if not args.no_posterior:
+        from fastbart_b200 import workloads as W
+        trees2 = W.posterior_forest(PRED_DRAWS, 200, PRED_P, 100, change=PRED_CHANGE, seed=12)
+        ct2 = F.CompiledTrees(F.trees_text(trees2, PRED_P), cps, mu=mu, device=local)
+        ev2, shared2 = ct2.evaluator(PRED_ROWS, PRED_DRAWS)
+
+        def run2():
+            F.predict_draws_device(ct2, xd.data_ptr(), PRED_P, PRED_ROWS, PRED_ROWS, 1, PRED_DRAWS, out.data_ptr(),
+                                   PRED_ROWS, stream.cuda_stream)
+        for _ in range(args.warmup):
+            flush.zero_()
+            run2()
+        torch.cuda.synchronize()
+        assert np.array_equal(out[-1, :2000].cpu().numpy(), F.predict_draw(ct2, xh[:2000], PRED_DRAWS)), \
+            "bulk and single-draw predict disagree (posterior draws)"
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            run2()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms2 = shard.max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), device="cuda") / args.steps
+        post = {"row_draws_per_s": PRED_DRAWS * PRED_ROWS * world / (ms2 / 1000.0), "ms_per_call": ms2,
+                "evaluator": ev2, "shared_tree_fraction": shared2 / float(PRED_DRAWS * 200), "nodes": ct2.nnodes,
+                "over_tree_prior_forest": (PRED_DRAWS * PRED_ROWS * world / (ms2 / 1000.0)) / value,
+                "what": f"1,000 draws shaped like one chain's consecutive posterior draws ({PRED_CHANGE:.0%} of the "
+                        f"trees grown again per draw, every leaf value redrawn; workloads.posterior_forest), same rows"}
+        del ct2
     # end to end with host buffers: every step copies x (column-major, pinned) to the device, evaluates all draws
     # (fb_predict_draws_device) and copies every result back to pinned host memory
     e2e = None
@@ -702,7 +737,8 @@ def bench_predict(args):
                 "config": {"workload": "predict_bulk_1000x1M", "draws": PRED_DRAWS, "ntree": 200,
                            "rows": PRED_ROWS, "p": PRED_P, "nodes": ct.nnodes,
                            "l2": "flushed (512 MiB write) before every timed step; inputs and outputs exceed L2"},
-                "e2e": e2e, "gpu_launches": args.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+                "e2e": e2e, "gpu_launches": args.steps * (2 if post else 1), "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clk, "posterior_draws": post}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -1071,6 +1107,8 @@ def bench_mixed(args):
     predict = {"row_draws_per_s": nd * MIX_PRED_ROWS / psec, "ms_per_call": 1000 * psec, "draws": nd,
                "nodes": ct.nnodes, "hbm_gbs": alg / psec / 1e9, "frac_of_hbm": alg / psec / 1e9 / peak,
                "peak": peak, "peak_source": peak_kind, "bit_exact_vs_oracle": bool(pparity),
+               "evaluator": ct.evaluator(MIX_PRED_ROWS, nd)[0],
+               "shared_tree_fraction": ct.evaluator(MIX_PRED_ROWS, nd)[1] / float(nd * 200),
                "what": "1,000 draws (10 fits x 100 kept draws) x 200 trees on 1,000,000 fresh rows, one "
                        "fb_predict_draws_device call, x and results resident"}
     pool.terminate()
@@ -1094,6 +1132,69 @@ def bench_mixed(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------ head training
+TRAIN_N = 200_000
+
+
+def bench_train(args):
+    """Training of both learned heads on the device (fb_train_proposal, fb_train_cut_proposal: per minibatch one
+    gradient launch, whose GEMMs run on the tensor cores, and one Adam launch) on config 4's 200,000 training moves,
+    synthetic features of the heads' shapes.  Metric: training examples per second (epochs x examples / wall time of
+    the call, which includes one copy of the examples to the device); one full-batch gradient launch per head is also
+    timed with CUDA events on its own."""
+    import torch
+    import fastbart_b200 as F
+    from fastbart_b200 import _lib
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned proposal to train"}))
+        return 0
+    rng = np.random.default_rng(5)
+    N, IN, O = TRAIN_N, _lib.MLP_IN, _lib.MLP_OUT
+    x = rng.random((N, IN), dtype=np.float32)
+    mask = rng.integers(1, 1 << 32, N, dtype=np.uint64).astype(np.uint32) | np.uint32(1)
+    y = np.array([rng.choice(np.flatnonzero((int(m) >> np.arange(O)) & 1)) for m in mask[:4096]], np.int32)
+    y = np.resize(y, N)
+    mask = mask | (np.uint32(1) << y.astype(np.uint32))
+    cx = rng.random((N, _lib.CUT_IN), dtype=np.float32)
+    lo = rng.integers(0, 200, N).astype(np.int32)
+    hi = np.minimum(lo + rng.integers(0, 100, N), 254).astype(np.int32)
+    cc = (lo + (rng.random(N) * (hi - lo + 1)).astype(np.int32)).astype(np.int32)
+    epochs = max(1, args.steps)
+    F.train_proposal(x[:4096], y[:4096], mask[:4096], epochs=1, batch=512)   # warm-up (module load, first launch)
+    F.train_cut_proposal(cx[:4096], cc[:4096], lo[:4096], hi[:4096], epochs=1, batch=512)
+    torch.cuda.synchronize()
+    out = {}
+    for name, call in (("variable_head", lambda: F.train_proposal(x, y, mask, epochs=epochs, batch=512, seed=1)),
+                       ("cut_head", lambda: F.train_cut_proposal(cx, cc, lo, hi, epochs=epochs, batch=512, seed=1))):
+        t = time.perf_counter()
+        _, losses = call()
+        wall = time.perf_counter() - t
+        out[name] = {"examples_per_s": N * epochs / wall, "seconds": wall, "epochs": epochs,
+                     "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+    # one gradient launch over all examples (6,250 tiles of 32), device time from CUDA events around the call's copy
+    # and kernel (the call copies its inputs and results synchronously)
+    model = {k: np.zeros(v.shape, v.dtype) for k, v in F.api._empty_model().items()}
+    gflop = 2.0 * (IN * 64 + 64 * 64 + 64 * O) * 3 * N / 1e9
+    t = time.perf_counter()
+    F.mlp_loss_grad(model, x, y, mask)
+    out["variable_head"]["full_batch_gradient_s"] = time.perf_counter() - t
+    out["variable_head"]["gemm_gflop_per_pass"] = gflop
+    value = out["variable_head"]["examples_per_s"]
+    line = {"metric": "training examples/s of the learned variable head (config 4's 200,000 moves, minibatch 512)",
+            "value": value, "unit": "examples/s", "n_gpus": 1, "steps": epochs, "warmup": 1,
+            "ms_per_step": 1000 * out["variable_head"]["seconds"] / epochs, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "tf32x3 (f32 accuracy) on tensor cores, bf16 weights",
+            "data": "synthetic", "config": {"workload": "train_heads_200k", "examples": N, "batch": 512},
+            "e2e": {"value": value, "unit": "examples/s", "h2d_bytes_per_step": int(x.nbytes + y.nbytes + mask.nbytes),
+                    "d2h_bytes_per_step": 0, "api": "fb_train_proposal (host arrays in, model out)"},
+            "gpu_launches": int(2 * epochs * ((N + 511) // 512)), "heads": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1105,11 +1206,12 @@ def main():
     ap.add_argument("--autotune", action="store_true", help="time candidate launch shapes first (fb_autotune)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-posterior", action="store_true", help="predict: skip the posterior-shaped forest leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single", action="store_true", help="skip the one-chain-per-launch comparison")
     ap.add_argument("--workload", default="titer96",
                     choices=["titer96", "small", "single", "sparse", "probit", "predict", "learned", "text",
-                             "mixed"])
+                             "mixed", "train"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -1121,6 +1223,8 @@ def main():
         return bench_text(args)
     if args.workload == "mixed":
         return bench_mixed(args)
+    if args.workload == "train":
+        return bench_train(args)
     set_workload(args.workload)
     if args.impl == "reference":
         return bench_reference(args)

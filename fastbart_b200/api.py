@@ -444,6 +444,15 @@ class CompiledTrees:
         return dict(ndpost=self.ndpost, ntree=self.ntree, p=self.p, var=var, child=child, cut=cut, theta=theta,
                     root=root)
 
+    EVALUATORS = ("streaming", "tiled", "codes", "codes_carry")
+
+    def evaluator(self, n: int, ndraws: int) -> tuple[str, int]:
+        """(name of the device evaluator a bulk call of ndraws draws on n rows runs, trees that share their structure
+        with the previous draw's tree of the same index)."""
+        ev, sh = C.c_int(), C.c_longlong()
+        check(_lib.lib().fb_predict_evaluator(self._h, int(n), int(ndraws), C.byref(ev), C.byref(sh)))
+        return self.EVALUATORS[ev.value], sh.value
+
     def handle(self):
         return self._h
 

@@ -167,6 +167,10 @@ struct DForest {
   // (child | var << 16 | c << 24; leaves point to themselves with c = 255), and the cutpoints of every predictor
   // (cuts[cutoff[v] .. cutoff[v + 1]), strictly increasing)
   const uint32_t* n32; const double* cuts; const int* cutoff;
+  // reuse across consecutive draws (code-compare layout): bit t of same[d][.] says tree t of draw d has the structure
+  // of tree t of draw d - 1 (node count, splits and children relative to its root; leaf values may differ), so a row
+  // reaches the same leaf offset in both; tdep[d][t] is the tree's deepest leaf; nsame counts the set bits
+  const uint32_t* same; const uint8_t* tdep; long long nsame;
   int maxnd;               // most nodes of one draw
   int ntree, ndpost, p, nnodes;
 };
@@ -207,6 +211,8 @@ int launch_cut_codes(const double* x, int n, int p, const double* cuts, const in
 constexpr size_t PREDICT_SCRATCH_DOUBLES = size_t(1) << 20;
 // 0: *ptr = the scratch's address on `device` (the current device); -1: CUDA error; -2: device ordinal not tracked
 int predict_scratch_address(int device, double** ptr);
+// evaluator launch_predict uses for f: 0 streaming, 1 tiled, 2 code-compare, 3 code-compare carrying leaves across draws
+int predict_evaluator(const DForest& f, int n, int ndraws);
 int launch_predict(const DForest& f, const double* x, int n, int ld, int draw0, int ndraws, double mu, double* out,
                    int ldo, void* stream);
 

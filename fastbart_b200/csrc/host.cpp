@@ -886,19 +886,23 @@ struct fb_compiled {
   uint32_t* dn32 = nullptr;     // code-compare layout (null when the cutpoints do not allow it)
   double* dcutflat = nullptr;
   int* dcutoff = nullptr;
+  uint32_t* dsame = nullptr;    // trees with the structure of the previous draw's (code-compare layout)
+  uint8_t* dtdep = nullptr;
+  long long nsame = 0;
   int maxnd = 0;
   ~fb_compiled() {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(device);
     cudaFree(dvar); cudaFree(dchild); cudaFree(droot); cudaFree(dcut); cudaFree(dtheta); cudaFree(dnodes); cudaFree(dgdep);
-    cudaFree(dn32); cudaFree(dcutflat); cudaFree(dcutoff);
+    cudaFree(dn32); cudaFree(dcutflat); cudaFree(dcutoff); cudaFree(dsame); cudaFree(dtdep);
     cudaSetDevice(cur);
   }
   DForest forest() const {
     DForest f;
     f.var = dvar; f.child = dchild; f.cut = dcut; f.theta = dtheta; f.root = droot; f.nodes = dnodes; f.gdepth = dgdep;
     f.n32 = dn32; f.cuts = dcutflat; f.cutoff = dcutoff; f.maxnd = maxnd;
+    f.same = dsame; f.tdep = dtdep; f.nsame = nsame;
     f.ntree = ntree; f.ndpost = ndpost; f.p = p; f.nnodes = (int)var.size();
     return f;
   }
@@ -1016,7 +1020,7 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
     else pn[k] = PNode{ct->theta[k], (int)k, ct->p};
   }
   const int G = (ct->ntree + 3) / 4;
-  std::vector<uint8_t> gd((size_t)nd * G, 0);
+  std::vector<uint8_t> gd((size_t)nd * G, 0), td((size_t)(nd * m), 0);
   int deepest = 0;
   for (long long t = 0; t < nd * m; t++) {
     const size_t b = (size_t)ct->root[(size_t)t], e = t + 1 < nd * m ? (size_t)ct->root[(size_t)t + 1] : N;
@@ -1025,6 +1029,7 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
     deepest = std::max(deepest, mx);
     uint8_t& g = gd[(size_t)(t / m) * G + (size_t)(t % m) / 4];
     g = (uint8_t)std::min(255, std::max<int>(g, mx));
+    td[(size_t)t] = (uint8_t)std::min(255, mx);
   }
   const bool tiled = deepest <= 255;   // deeper trees use only the streaming evaluator
   // code-compare layout: x >= cutpoints[v][c]  <=>  code_v(x) > c, with code_v(x) the number of cutpoints of v that
@@ -1064,6 +1069,30 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
     if (cutflat.empty()) cutflat.push_back(0.0);
     ct->maxnd = maxnd;
   }
+  // trees whose structure equals the previous draw's tree of the same index (BART changes few trees per sweep, so
+  // consecutive posterior draws share most of theirs): same node count, and every node with the same split (var,
+  // cut index) and the same children relative to the tree's root
+  const int SW = (m + 31) / 32;
+  std::vector<uint32_t> same;
+  bool carry = codes && nd > 1;   // leaf offsets are kept in one byte: trees of at most 256 nodes
+  for (long long t = 0; carry && t < nd * m; t++)
+    carry = (t + 1 < nd * m ? (size_t)ct->root[(size_t)t + 1] : N) - (size_t)ct->root[(size_t)t] <= 256;
+  if (carry) {
+    same.assign((size_t)nd * SW, 0u);
+    for (long long d = 1; d < nd; d++)
+      for (int t = 0; t < m; t++) {
+        const long long t1 = (d - 1) * m + t, t2 = d * m + t;
+        const size_t b1 = (size_t)ct->root[(size_t)t1], e1 = (size_t)ct->root[(size_t)t1 + 1];
+        const size_t b2 = (size_t)ct->root[(size_t)t2], e2 = t2 + 1 < nd * m ? (size_t)ct->root[(size_t)t2 + 1] : N;
+        bool eq = e1 - b1 == e2 - b2;
+        for (size_t k = 0; eq && k < e1 - b1; k++) {
+          const int c1 = ct->child[b1 + k], c2 = ct->child[b2 + k];
+          eq = (c1 < 0) == (c2 < 0) && (c1 < 0 || (size_t)c1 - b1 == (size_t)c2 - b2) &&
+               ct->var[b1 + k] == ct->var[b2 + k] && ct->cidx[b1 + k] == ct->cidx[b2 + k];
+        }
+        if (eq) { same[(size_t)d * SW + t / 32] |= 1u << (t % 32); ct->nsame++; }
+      }
+  }
   if (tiled && (cudaMalloc(&ct->dnodes, N * sizeof(PNode)) != cudaSuccess ||
                 cudaMemcpy(ct->dnodes, pn.data(), N * sizeof(PNode), cudaMemcpyHostToDevice) != cudaSuccess ||
                 cudaMalloc(&ct->dgdep, gd.size()) != cudaSuccess ||
@@ -1080,6 +1109,14 @@ fb_status fb_compile_trees(const char* text, size_t len, const double* const* cu
     delete ct;
     return fail(FB_ERR_CUDA, "cannot upload the compiled trees");
   }
+  if (carry && (cudaMalloc(&ct->dsame, same.size() * 4) != cudaSuccess ||
+                cudaMemcpy(ct->dsame, same.data(), same.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMalloc(&ct->dtdep, td.size()) != cudaSuccess ||
+                cudaMemcpy(ct->dtdep, td.data(), td.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
+    delete ct;
+    return fail(FB_ERR_CUDA, "cannot upload the compiled trees");
+  }
+  if (!carry) ct->nsame = 0;
   if (cudaMalloc(&ct->dvar, N * 4) != cudaSuccess || cudaMalloc(&ct->dchild, N * 4) != cudaSuccess ||
       cudaMalloc(&ct->dcut, N * 8) != cudaSuccess || cudaMalloc(&ct->dtheta, N * 8) != cudaSuccess ||
       cudaMalloc(&ct->droot, ct->root.size() * 4) != cudaSuccess ||
@@ -1101,6 +1138,14 @@ fb_status fb_compiled_info(const fb_compiled* ct, int* ndpost, int* ntree, int* 
   if (ntree) *ntree = ct->ntree;
   if (p) *p = ct->p;
   if (nnodes) *nnodes = (int)ct->var.size();
+  return FB_OK;
+}
+
+fb_status fb_predict_evaluator(const fb_compiled* ct, int n, int ndraws, int* evaluator, long long* shared_trees) {
+  if (!ct) return fail(FB_ERR_ARG, "compiled trees are NULL");
+  if (n < 0 || ndraws < 0) return fail(FB_ERR_ARG, "negative size");
+  if (evaluator) *evaluator = predict_evaluator(ct->forest(), n, ndraws);
+  if (shared_trees) *shared_trees = ct->nsame;
   return FB_OK;
 }
 

@@ -8,7 +8,10 @@
 // w3 [OUT][H], b3 [OUT]; the forward pass reads the BF16-rounded weights, exactly as the sampler does.
 //   mlp_grad_kernel   one CTA per tile of MT_TILE examples: forward, softmax, backward for the tile in shared
 //                     memory, then one atomic add per parameter and tile into the FP32 gradient vector (and the
-//                     tile's summed loss).  Tiny GEMMs (at most 64 x 98 per layer): CUDA cores, no tensor cores.
+//                     tile's summed loss).  Every GEMM of the forward pass, the backward pass and the weight
+//                     gradients runs on the tensor cores (warp_gemm below: mma.sync m16n8k8 TF32 tiles with FP32
+//                     accumulation, operands split into two TF32 parts so that the products keep FP32 accuracy).
+//   cut_grad_kernel   the same for the cutpoint head (40 -> 64 -> 64 -> 16, then 255 cut logits).
 //   mlp_adam_kernel   Adam step on the master weights from the summed gradients / batch size, refreshing the BF16
 //                     copies of the weights.
 #include <cuda_runtime.h>
@@ -23,6 +26,54 @@ constexpr int MT_TILE = 32;
 constexpr int MT_THREADS = 256;
 
 __device__ __forceinline__ float bf16_to_f(uint16_t h) { return __uint_as_float((unsigned)h << 16); }
+
+// ---- GEMM tiles on the tensor cores.  A warp computes a 16 x 8 tile of C = A B with mma.sync m16n8k8 (TF32 inputs,
+// FP32 accumulation).  TF32 keeps 10 mantissa bits, so each operand is split as x = hi + lo with hi = tf32(x) and
+// lo = tf32(x - hi), and the tile accumulates lo*hi + hi*lo + hi*hi (the small terms first): the error of the
+// dropped lo*lo term and of the splits is about 2^-21 of the product, as with FP32 arithmetic (the split-TF32 scheme
+// of Ootomo and Yokota, 2022).  Fragment layout of m16n8k8 (PTX ISA): lane = 4 g + t; A holds (g, t), (g + 8, t),
+// (g, t + 4), (g + 8, t + 4); B holds (t, g), (t + 4, g); C holds (g, 2t), (g, 2t + 1), (g + 8, 2t), (g + 8, 2t + 1).
+__device__ __forceinline__ uint32_t tf32_of(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = tf32_of(x);
+  lo = tf32_of(__fsub_rn(x, __uint_as_float(hi)));
+}
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+               "{%0, %1, %2, %3};\n"
+               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+// C (M x N, multiples of 16 and 8) = A (M x K) B (K x N), K a multiple of 8: the CTA's warps take the 16 x 8 tiles in
+// turn; A(m, k) and B(k, n) return the operands (zero in the padding), E(m, n, value) consumes each result.
+template <class FA, class FB, class FE>
+__device__ __forceinline__ void warp_gemm(int M, int N, int K, FA A, FB B, FE E) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3, nt = N / 8, tiles = (M / 16) * nt;
+  for (int p = warp; p < tiles; p += nw) {
+    const int m0 = (p / nt) * 16, n0 = (p % nt) * 8;
+    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int k0 = 0; k0 < K; k0 += 8) {
+      uint32_t ah[4], al[4], bh[2], bl[2];
+      split_tf32(A(m0 + g, k0 + t), ah[0], al[0]);
+      split_tf32(A(m0 + g + 8, k0 + t), ah[1], al[1]);
+      split_tf32(A(m0 + g, k0 + t + 4), ah[2], al[2]);
+      split_tf32(A(m0 + g + 8, k0 + t + 4), ah[3], al[3]);
+      split_tf32(B(k0 + t, n0 + g), bh[0], bl[0]);
+      split_tf32(B(k0 + t + 4, n0 + g), bh[1], bl[1]);
+      mma_tf32(c, al, bh);
+      mma_tf32(c, ah, bl);
+      mma_tf32(c, ah, bh);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; e++) E(m0 + g + 8 * (e >> 1), n0 + 2 * t + (e & 1), c[e]);
+  }
+}
+constexpr int pad8(int k) { return (k + 7) / 8 * 8; }
 __device__ __forceinline__ uint16_t f_to_bf16(float f) {   // round to nearest even (finite inputs)
   const unsigned u = __float_as_uint(f);
   return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
@@ -56,27 +107,21 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_grad_kernel(MlpParams P, const
   }
   if (tid == 0) *lsum = 0.0f;
   __syncthreads();
-  // forward
-  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
-    const int b = k / MLP_H, h = k % MLP_H;
-    float a = P.b1[h];
-    for (int f = 0; f < MLP_IN; f++) a += w1[h * MLP_IN + f] * xs[b * MLP_IN + f];
-    h1[k] = a > 0.0f ? a : 0.0f;
-  }
+  // forward: h1 = relu(x W1^T + b1), h2 = relu(h1 W2^T + b2), logits = h2 W3^T + b3
+  warp_gemm(MT_TILE, MLP_H, pad8(MLP_IN),
+            [&](int b, int f) { return f < MLP_IN ? xs[b * MLP_IN + f] : 0.0f; },
+            [&](int f, int h) { return f < MLP_IN ? w1[h * MLP_IN + f] : 0.0f; },
+            [&](int b, int h, float v) { v = __fadd_rn(v, P.b1[h]); h1[b * MLP_H + h] = v > 0.0f ? v : 0.0f; });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
-    const int b = k / MLP_H, h = k % MLP_H;
-    float a = P.b2[h];
-    for (int f = 0; f < MLP_H; f++) a += w2[h * MLP_H + f] * h1[b * MLP_H + f];
-    h2[k] = a > 0.0f ? a : 0.0f;
-  }
+  warp_gemm(MT_TILE, MLP_H, MLP_H,
+            [&](int b, int f) { return h1[b * MLP_H + f]; },
+            [&](int f, int h) { return w2[h * MLP_H + f]; },
+            [&](int b, int h, float v) { v = __fadd_rn(v, P.b2[h]); h2[b * MLP_H + h] = v > 0.0f ? v : 0.0f; });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * MLP_OUT; k += MT_THREADS) {
-    const int b = k / MLP_OUT, o = k % MLP_OUT;
-    float a = P.b3[o];
-    for (int f = 0; f < MLP_H; f++) a += w3[o * MLP_H + f] * h2[b * MLP_H + f];
-    g3[k] = a;
-  }
+  warp_gemm(MT_TILE, MLP_OUT, MLP_H,
+            [&](int b, int f) { return h2[b * MLP_H + f]; },
+            [&](int f, int o) { return w3[o * MLP_H + f]; },
+            [&](int b, int o, float v) { g3[b * MLP_OUT + o] = __fadd_rn(v, P.b3[o]); });
   __syncthreads();
   // masked softmax and cross-entropy, one thread per example: g3 becomes dLoss/dz (summed, not averaged)
   if (tid < MT_TILE) {
@@ -98,46 +143,36 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_grad_kernel(MlpParams P, const
     }
   }
   __syncthreads();
-  // backward through layer 3 and the second ReLU
-  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
-    const int b = k / MLP_H, h = k % MLP_H;
-    float a = 0.0f;
-    for (int o = 0; o < MLP_OUT; o++) a += g3[b * MLP_OUT + o] * w3[o * MLP_H + h];
-    d2[k] = h2[k] > 0.0f ? a : 0.0f;
-  }
+  // backward through layer 3 and the second ReLU, then layer 2 and the first ReLU
+  warp_gemm(MT_TILE, MLP_H, MLP_OUT,
+            [&](int b, int o) { return g3[b * MLP_OUT + o]; },
+            [&](int o, int h) { return w3[o * MLP_H + h]; },
+            [&](int b, int h, float v) { d2[b * MLP_H + h] = h2[b * MLP_H + h] > 0.0f ? v : 0.0f; });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * MLP_H; k += MT_THREADS) {
-    const int b = k / MLP_H, h = k % MLP_H;
-    float a = 0.0f;
-    for (int o = 0; o < MLP_H; o++) a += d2[b * MLP_H + o] * w2[o * MLP_H + h];
-    d1[k] = h1[k] > 0.0f ? a : 0.0f;
-  }
+  warp_gemm(MT_TILE, MLP_H, MLP_H,
+            [&](int b, int o) { return d2[b * MLP_H + o]; },
+            [&](int o, int h) { return w2[o * MLP_H + h]; },
+            [&](int b, int h, float v) { d1[b * MLP_H + h] = h1[b * MLP_H + h] > 0.0f ? v : 0.0f; });
   __syncthreads();
-  // parameter gradients of the tile, one atomic add each
+  // parameter gradients of the tile (sums over its examples), one atomic add each
   float* gw1 = grad;
   float* gb1 = gw1 + MLP_H * MLP_IN;
   float* gw2 = gb1 + MLP_H;
   float* gb2 = gw2 + MLP_H * MLP_H;
   float* gw3 = gb2 + MLP_H;
   float* gb3 = gw3 + MLP_OUT * MLP_H;
-  for (int k = tid; k < MLP_H * MLP_IN; k += MT_THREADS) {
-    const int h = k / MLP_IN, f = k % MLP_IN;
-    float a = 0.0f;
-    for (int b = 0; b < nb; b++) a += d1[b * MLP_H + h] * xs[b * MLP_IN + f];
-    atomicAdd(gw1 + k, a);
-  }
-  for (int k = tid; k < MLP_H * MLP_H; k += MT_THREADS) {
-    const int h = k / MLP_H, f = k % MLP_H;
-    float a = 0.0f;
-    for (int b = 0; b < nb; b++) a += d2[b * MLP_H + h] * h1[b * MLP_H + f];
-    atomicAdd(gw2 + k, a);
-  }
-  for (int k = tid; k < MLP_OUT * MLP_H; k += MT_THREADS) {
-    const int o = k / MLP_H, f = k % MLP_H;
-    float a = 0.0f;
-    for (int b = 0; b < nb; b++) a += g3[b * MLP_OUT + o] * h2[b * MLP_H + f];
-    atomicAdd(gw3 + k, a);
-  }
+  warp_gemm(MLP_H, pad8(MLP_IN), MT_TILE,
+            [&](int h, int b) { return b < nb ? d1[b * MLP_H + h] : 0.0f; },
+            [&](int b, int f) { return f < MLP_IN ? xs[b * MLP_IN + f] : 0.0f; },
+            [&](int h, int f, float v) { if (f < MLP_IN) atomicAdd(gw1 + h * MLP_IN + f, v); });
+  warp_gemm(MLP_H, MLP_H, MT_TILE,
+            [&](int h, int b) { return b < nb ? d2[b * MLP_H + h] : 0.0f; },
+            [&](int b, int f) { return h1[b * MLP_H + f]; },
+            [&](int h, int f, float v) { atomicAdd(gw2 + h * MLP_H + f, v); });
+  warp_gemm(MLP_OUT, MLP_H, MT_TILE,
+            [&](int o, int b) { return b < nb ? g3[b * MLP_OUT + o] : 0.0f; },
+            [&](int b, int f) { return h2[b * MLP_H + f]; },
+            [&](int o, int f, float v) { atomicAdd(gw3 + o * MLP_H + f, v); });
   if (tid < MLP_H) {
     float a = 0.0f, c = 0.0f;
     for (int b = 0; b < nb; b++) { a += d1[b * MLP_H + tid]; c += d2[b * MLP_H + tid]; }
@@ -242,36 +277,28 @@ __global__ void __launch_bounds__(MT_THREADS) cut_grad_kernel(CutParams P, const
   }
   if (tid == 0) *lsum = 0.0f;
   __syncthreads();
-  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
-    const int b = k / CUT_H, h = k % CUT_H;
-    float a = P.b1[h];
-    for (int f = 0; f < CUT_IN; f++) a += w1[h * CUT_IN + f] * xs[b * CUT_IN + f];
-    h1[k] = a > 0.0f ? a : 0.0f;
-  }
+  // forward: h1, h2 (ReLU), the embedding e = h2 W3^T + b3, and the logits be[c] + emb[c] . e inside [lo, hi]
+  warp_gemm(MT_TILE, CUT_H, pad8(CUT_IN),
+            [&](int b, int f) { return f < CUT_IN ? xs[b * CUT_IN + f] : 0.0f; },
+            [&](int f, int h) { return f < CUT_IN ? w1[h * CUT_IN + f] : 0.0f; },
+            [&](int b, int h, float v) { v = __fadd_rn(v, P.b1[h]); h1[b * CUT_H + h] = v > 0.0f ? v : 0.0f; });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
-    const int b = k / CUT_H, h = k % CUT_H;
-    float a = P.b2[h];
-    for (int f = 0; f < CUT_H; f++) a += w2[h * CUT_H + f] * h1[b * CUT_H + f];
-    h2[k] = a > 0.0f ? a : 0.0f;
-  }
+  warp_gemm(MT_TILE, CUT_H, CUT_H,
+            [&](int b, int f) { return h1[b * CUT_H + f]; },
+            [&](int f, int h) { return w2[h * CUT_H + f]; },
+            [&](int b, int h, float v) { v = __fadd_rn(v, P.b2[h]); h2[b * CUT_H + h] = v > 0.0f ? v : 0.0f; });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * CUT_E; k += MT_THREADS) {
-    const int b = k / CUT_E, q = k % CUT_E;
-    float a = P.b3[q];
-    for (int f = 0; f < CUT_H; f++) a += w3[q * CUT_H + f] * h2[b * CUT_H + f];
-    ev[k] = a;
-  }
+  warp_gemm(MT_TILE, CUT_E, CUT_H,
+            [&](int b, int f) { return h2[b * CUT_H + f]; },
+            [&](int f, int q) { return w3[q * CUT_H + f]; },
+            [&](int b, int q, float v) { ev[b * CUT_E + q] = __fadd_rn(v, P.b3[q]); });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * CT_ZS; k += MT_THREADS) {
-    const int b = k / CT_ZS, c = k % CT_ZS;
-    float a = 0.0f;
-    if (c >= lo[b] && c <= hi[b]) {
-      a = P.be[c];
-      for (int q = 0; q < CUT_E; q++) a += em[c * CUT_E + q] * ev[b * CUT_E + q];
-    }
-    dz[k] = a;
-  }
+  warp_gemm(MT_TILE, CT_ZS, CUT_E,
+            [&](int b, int q) { return ev[b * CUT_E + q]; },
+            [&](int q, int c) { return c < CUT_BINS ? em[c * CUT_E + q] : 0.0f; },
+            [&](int b, int c, float v) {
+              dz[b * CT_ZS + c] = (c >= lo[b] && c <= hi[b]) ? __fadd_rn(v, P.be[c]) : 0.0f;
+            });
   __syncthreads();
   // softmax over [lo, hi] and cross-entropy, one warp per example: dz becomes dLoss/dz (summed, not averaged)
   for (int b = warp; b < MT_TILE; b += MT_THREADS / 32) {
@@ -294,26 +321,21 @@ __global__ void __launch_bounds__(MT_THREADS) cut_grad_kernel(CutParams P, const
     if (lane == 0) atomicAdd(lsum, -(zy - zm - __logf(S)));
   }
   __syncthreads();
-  for (int k = tid; k < MT_TILE * CUT_E; k += MT_THREADS) {
-    const int b = k / CUT_E, q = k % CUT_E;
-    float a = 0.0f;
-    for (int c = lo[b]; c <= hi[b]; c++) a += dz[b * CT_ZS + c] * em[c * CUT_E + q];
-    de[k] = a;
-  }
+  // backward: de = dz emb (dz is zero outside [lo, hi]), then the two ReLU layers
+  warp_gemm(MT_TILE, CUT_E, CT_ZS,
+            [&](int b, int c) { return dz[b * CT_ZS + c]; },
+            [&](int c, int q) { return c < CUT_BINS ? em[c * CUT_E + q] : 0.0f; },
+            [&](int b, int q, float v) { de[b * CUT_E + q] = v; });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
-    const int b = k / CUT_H, f = k % CUT_H;
-    float a = 0.0f;
-    for (int q = 0; q < CUT_E; q++) a += de[b * CUT_E + q] * w3[q * CUT_H + f];
-    d2[k] = h2[k] > 0.0f ? a : 0.0f;
-  }
+  warp_gemm(MT_TILE, CUT_H, CUT_E,
+            [&](int b, int q) { return de[b * CUT_E + q]; },
+            [&](int q, int f) { return w3[q * CUT_H + f]; },
+            [&](int b, int f, float v) { d2[b * CUT_H + f] = h2[b * CUT_H + f] > 0.0f ? v : 0.0f; });
   __syncthreads();
-  for (int k = tid; k < MT_TILE * CUT_H; k += MT_THREADS) {
-    const int b = k / CUT_H, f = k % CUT_H;
-    float a = 0.0f;
-    for (int h = 0; h < CUT_H; h++) a += d2[b * CUT_H + h] * w2[h * CUT_H + f];
-    d1[k] = h1[k] > 0.0f ? a : 0.0f;
-  }
+  warp_gemm(MT_TILE, CUT_H, CUT_H,
+            [&](int b, int h) { return d2[b * CUT_H + h]; },
+            [&](int h, int f) { return w2[h * CUT_H + f]; },
+            [&](int b, int f, float v) { d1[b * CUT_H + f] = h1[b * CUT_H + f] > 0.0f ? v : 0.0f; });
   __syncthreads();
   float* gw1 = grad;
   float* gb1 = gw1 + CUT_H * CUT_IN;
@@ -323,30 +345,23 @@ __global__ void __launch_bounds__(MT_THREADS) cut_grad_kernel(CutParams P, const
   float* gb3 = gw3 + CUT_E * CUT_H;
   float* gem = gb3 + CUT_E;
   float* gbe = gem + CUT_BINS * CUT_E;
-  for (int k = tid; k < CUT_H * CUT_IN; k += MT_THREADS) {
-    const int h = k / CUT_IN, f = k % CUT_IN;
-    float a = 0.0f;
-    for (int b = 0; b < nb; b++) a += d1[b * CUT_H + h] * xs[b * CUT_IN + f];
-    atomicAdd(gw1 + k, a);
-  }
-  for (int k = tid; k < CUT_H * CUT_H; k += MT_THREADS) {
-    const int h = k / CUT_H, f = k % CUT_H;
-    float a = 0.0f;
-    for (int b = 0; b < nb; b++) a += d2[b * CUT_H + h] * h1[b * CUT_H + f];
-    atomicAdd(gw2 + k, a);
-  }
-  for (int k = tid; k < CUT_E * CUT_H; k += MT_THREADS) {
-    const int q = k / CUT_H, f = k % CUT_H;
-    float a = 0.0f;
-    for (int b = 0; b < nb; b++) a += de[b * CUT_E + q] * h2[b * CUT_H + f];
-    atomicAdd(gw3 + k, a);
-  }
-  for (int k = tid; k < CUT_BINS * CUT_E; k += MT_THREADS) {
-    const int c = k / CUT_E, q = k % CUT_E;
-    float a = 0.0f;
-    for (int b = 0; b < nb; b++) a += dz[b * CT_ZS + c] * ev[b * CUT_E + q];
-    atomicAdd(gem + k, a);
-  }
+  // parameter gradients of the tile (sums over its examples), one atomic add each
+  warp_gemm(CUT_H, pad8(CUT_IN), MT_TILE,
+            [&](int h, int b) { return b < nb ? d1[b * CUT_H + h] : 0.0f; },
+            [&](int b, int f) { return f < CUT_IN ? xs[b * CUT_IN + f] : 0.0f; },
+            [&](int h, int f, float v) { if (f < CUT_IN) atomicAdd(gw1 + h * CUT_IN + f, v); });
+  warp_gemm(CUT_H, CUT_H, MT_TILE,
+            [&](int h, int b) { return b < nb ? d2[b * CUT_H + h] : 0.0f; },
+            [&](int b, int f) { return h1[b * CUT_H + f]; },
+            [&](int h, int f, float v) { atomicAdd(gw2 + h * CUT_H + f, v); });
+  warp_gemm(CUT_E, CUT_H, MT_TILE,
+            [&](int q, int b) { return b < nb ? de[b * CUT_E + q] : 0.0f; },
+            [&](int b, int f) { return h2[b * CUT_H + f]; },
+            [&](int q, int f, float v) { atomicAdd(gw3 + q * CUT_H + f, v); });
+  warp_gemm(CT_ZS, CUT_E, MT_TILE,
+            [&](int c, int b) { return b < nb ? dz[b * CT_ZS + c] : 0.0f; },
+            [&](int b, int q) { return ev[b * CUT_E + q]; },
+            [&](int c, int q, float v) { if (c < CUT_BINS) atomicAdd(gem + c * CUT_E + q, v); });
   if (tid < CUT_H) {
     float a = 0.0f, c = 0.0f;
     for (int b = 0; b < nb; b++) { a += d1[b * CUT_H + tid]; c += d2[b * CUT_H + tid]; }

@@ -1022,7 +1022,6 @@ __device__ void commit_tree(const Smem& S, const DChain& C, const DBufs& B, DTre
       default: break;
     }
   }
-  fence_proxy_async_global();   // the next sweep's bulk copy of these statistics sees the stores
   __syncwarp();
 }
 
@@ -1658,7 +1657,13 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
       __syncthreads();
     }
     // ---------------------------------------------------------------- end of sweep
-    if (warp == 0) commit_tree<LP>(S, C, B, trees, s0g, m - 1, lane, lead);
+    if (warp == 0) {
+      commit_tree<LP>(S, C, B, trees, s0g, m - 1, lane, lead);
+      // the next sweep's bulk copies see every statistic this sweep's commits stored: each storing lane orders its
+      // own generic-proxy stores before the async proxy once, here, and the barrier below orders them before lane 0's
+      // copies (no statistic is fetched again within the sweep that stores it)
+      fence_proxy_async_global();
+    }
     __syncthreads();
     const bool keep = it >= C.nskip;
     const int dr = it - C.nskip;

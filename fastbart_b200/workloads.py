@@ -16,6 +16,7 @@ shipped, so these generators stand in for them with the same shapes, sizes and v
                     ten of the fwbart chains (p 32) share one cutpoint grid, so their kept draws pool into one
                     1,000-draw forest for bulk predict on fresh rows of the same distribution
   random_forest     posterior draws of trees grown from BART's tree prior (packed node format), for bulk predict
+  posterior_forest  the same, shaped like consecutive draws of one chain (most tree structures kept from draw to draw)
 """
 from __future__ import annotations
 
@@ -187,33 +188,62 @@ def friedman_large(nchains=16, n=65536, p=32, seed=0, **kw) -> list:
     return out
 
 
+def _grow_tree(rng, p, nc, base, power, sd, max_depth) -> dict:
+    """One tree from BART's tree prior as {slot: packed word}: a node at depth d splits with probability
+    base / (1 + d)^power, on a uniform predictor and cut index; leaf values N(0, sd^2) as float."""
+    words = {}
+    free = list(range(1, 64))
+
+    def grow(s, depth):
+        if (depth < max_depth and len(free) >= 2 and p > 0
+                and rng.random() < base / (1.0 + depth) ** power):
+            l, r = free.pop(0), free.pop(0)
+            v = int(rng.integers(p))
+            c = int(rng.integers(max(int(nc[v]), 1)))
+            words[s] = v | (c << 8) | (l << 16) | (r << 24)
+            grow(l, depth + 1)
+            grow(r, depth + 1)
+        else:
+            th = int(np.float32(rng.normal(0.0, sd)).view(np.uint32))
+            words[s] = th << 32
+    grow(0, 0)
+    return words
+
+
 def random_forest(ndpost: int, ntree: int, p: int, ncut, seed=0, base=0.95, power=2.0, sd=0.3,
                   max_depth=6) -> np.ndarray:
     """Packed trees [ndpost][ntree][64] (src/bart_kernel.cpp:559-571 format: v | c<<8 | l<<16 | r<<24 |
-    float_bits(theta)<<32, v = 255 for unused slots) grown from BART's tree prior: a node at depth d splits with
-    probability base / (1 + d)^power, on a uniform predictor and cut index; leaf values N(0, sd^2) as float.
+    float_bits(theta)<<32, v = 255 for unused slots), every tree grown independently from BART's tree prior.
     `ncut` is the cutpoint count of every predictor (an int, or one per predictor)."""
     rng = np.random.default_rng(seed)
     nc = np.broadcast_to(np.asarray(ncut, dtype=np.int64), (p,))
     out = np.full((ndpost, ntree, 64), 255, dtype=np.uint64)
     for d in range(ndpost):
         for t in range(ntree):
-            words = {}
-            free = list(range(1, 64))
+            for sl, wd in _grow_tree(rng, p, nc, base, power, sd, max_depth).items():
+                out[d, t, sl] = np.uint64(wd)
+    return out
 
-            def grow(s, depth):
-                if (depth < max_depth and len(free) >= 2 and p > 0
-                        and rng.random() < base / (1.0 + depth) ** power):
-                    l, r = free.pop(0), free.pop(0)
-                    v = int(rng.integers(p))
-                    c = int(rng.integers(max(int(nc[v]), 1)))
-                    words[s] = v | (c << 8) | (l << 16) | (r << 24)
-                    grow(l, depth + 1)
-                    grow(r, depth + 1)
-                else:
-                    th = int(np.float32(rng.normal(0.0, sd)).view(np.uint32))
-                    words[s] = th << 32
-            grow(0, 0)
-            for sl, wd in words.items():
+
+def posterior_forest(ndpost: int, ntree: int, p: int, ncut, change=0.25, seed=0, base=0.95, power=2.0, sd=0.3,
+                     max_depth=6) -> np.ndarray:
+    """Packed trees [ndpost][ntree][64] shaped like consecutive posterior draws of one chain: draw 0 from BART's
+    tree prior; each later draw keeps the previous draw's tree structures except a fraction `change` of the trees,
+    which are grown again (BART accepts a move for a minority of its trees per sweep), and redraws every leaf value
+    (as every sweep does)."""
+    rng = np.random.default_rng(seed)
+    nc = np.broadcast_to(np.asarray(ncut, dtype=np.int64), (p,))
+    out = np.full((ndpost, ntree, 64), 255, dtype=np.uint64)
+    for d in range(ndpost):
+        regrow = np.ones(ntree, bool) if d == 0 else rng.random(ntree) < change
+        if d > 0:
+            kept = out[d - 1, ~regrow]
+            leaf = ((kept & np.uint64(255)) != np.uint64(255)) & (((kept >> np.uint64(16)) & np.uint64(255)) == 0)
+            th = rng.normal(0.0, sd, int(leaf.sum())).astype(np.float32).view(np.uint32).astype(np.uint64)
+            kept = kept.copy()
+            kept[leaf] = th << np.uint64(32)
+            out[d, ~regrow] = kept
+        for t in np.flatnonzero(regrow):
+            for sl, wd in _grow_tree(rng, p, nc, base, power, sd, max_depth).items():
                 out[d, t, sl] = np.uint64(wd)
     return out

@@ -234,6 +234,11 @@ typedef struct fb_compiled fb_compiled;
 fb_status fb_compile_trees(const char* text, size_t len, const double* const* cutpoints, const int* ncut, int ncol,
                            int device, fb_compiled** out);
 fb_status fb_compiled_info(const fb_compiled* ct, int* ndpost, int* ntree, int* p, int* nnodes);
+/* Which device evaluator a bulk call of ndraws draws on n rows runs (0 streaming FP64 compares, 1 tiled FP64
+ * compares, 2 cutpoint codes, 3 cutpoint codes carrying each row's leaves across consecutive draws), and how many
+ * trees have the structure of the previous draw's tree of the same index (the leaves the carrying evaluator reuses;
+ * 0 when it is not applicable).  Every evaluator gives the same results. */
+fb_status fb_predict_evaluator(const fb_compiled* ct, int n, int ndraws, int* evaluator, long long* shared_trees);
 /* Copies the host arrays of compile_trees_cpp's result list (var, child, cut, theta [nnodes]; root [ndpost*ntree]). */
 fb_status fb_compiled_arrays(const fb_compiled* ct, int* var, int* child, double* cut, double* theta, int* root);
 void fb_compiled_free(fb_compiled* ct);

@@ -88,6 +88,44 @@ def test_bulk_predict_bit_exact_all_evaluators(orc, p, n, ndraws, dup):
         assert np.array_equal(F.predict_draw(ct, x, d + 1), o)
 
 
+@pytest.mark.parametrize("n,ndraws,ntree,change", [(1000, 40, 37, 0.25), (257, 9, 200, 0.0), (3001, 25, 50, 1.0)])
+def test_carry_evaluator_bit_exact(orc, n, ndraws, ntree, change):
+    """Draws shaped like consecutive posterior draws (most tree structures kept, every leaf value redrawn) run the
+    evaluator that carries each row's leaves across draws; its results equal the oracle's for every draw, and the
+    single-draw path's.  change 1.0 (independent draws) keeps the plain code-compare evaluator."""
+    import torch
+    p, ncut = 7, 20
+    rng = np.random.default_rng(n + ndraws)
+    cps = [np.sort(rng.random(ncut)) for _ in range(p)]
+    trees = W.posterior_forest(ndraws, ntree, p, ncut, change=change, seed=n, base=0.95, power=1.0, max_depth=6)
+    text = orc.trees_text(trees, p)
+    ct = F.CompiledTrees(text, cps, mu=-0.5)
+    ev, shared = ct.evaluator(n, ndraws)
+    assert ev == ("codes_carry" if change < 0.5 else "codes"), (ev, shared)
+    if change == 0.0:
+        assert shared == (ndraws - 1) * ntree
+    ref = orc.compile_trees(text, cps)
+    x = rng.random((n, p))
+    for v in range(p):
+        hit = rng.random(n) < 0.2
+        x[hit, v] = cps[v][rng.integers(0, ncut, hit.sum())]
+    xd = torch.tensor(np.ascontiguousarray(x.T), device="cuda")
+    out = torch.full((ndraws, n), float("nan"), dtype=torch.float64, device="cuda")
+    F.predict_draws_device(ct, xd.data_ptr(), p, n, n, 1, ndraws, out.data_ptr(), n)
+    # a range that starts inside the forest (its first draw walks every tree)
+    out2 = torch.full((ndraws - 3, n), float("nan"), dtype=torch.float64, device="cuda")
+    F.predict_draws_device(ct, xd.data_ptr(), p, n, n, 4, ndraws - 3, out2.data_ptr(), n)
+    torch.cuda.synchronize()
+    got, got2 = out.cpu().numpy(), out2.cpu().numpy()
+    cols = [x[:, v] for v in range(p)]
+    for d in range(ndraws):
+        o = orc.predict_draw(ref, cols, d + 1, -0.5)
+        assert np.array_equal(got[d], o), d
+        if d >= 3:
+            assert np.array_equal(got2[d - 3], o), d
+    assert np.array_equal(F.predict_draw(ct, x, ndraws), got[-1])
+
+
 def test_cut_codes_match_find_interval():
     """Device cut codes equal numpy searchsorted(side='right') (R's findInterval), ties and NaN included."""
     rng = np.random.default_rng(5)
