@@ -94,6 +94,54 @@ def set_workload(name: str):
         workload = small
 
 
+LATENT_ROWS = 1 << 24   # a streaming size well beyond L2: 16,777,216 rows x 20 B
+
+
+def latent_redraw(F, ch, out, stream, args):
+    """fpbart's latent redraw as a streaming kernel on its own (fb_probit_latent_device): at the chain's size (its
+    posterior-mean fit, 24,576 rows) and over 16,777,216 rows (the fit tiled; inputs and output beyond L2, L2 flushed
+    before each timed call), CUDA-event timed after warm-up calls.  Algorithmic bytes per row: fit 8 + outcome 4 +
+    z 8."""
+    import torch
+    res = {}
+    f0 = np.asarray(out["yhat_mean"], np.float64)   # the fit of the trees (the sampler's f, without the offset)
+    y0 = np.asarray(ch["ybin"], np.int32)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    peak, peak_kind = measured_peak()
+    for name, n in (("chain_rows", f0.size), ("rows_16M", LATENT_ROWS)):
+        reps = -(-n // f0.size)
+        fd = torch.tensor(np.tile(f0, reps)[:n], device="cuda")
+        yd = torch.tensor(np.tile(y0, reps)[:n], device="cuda")
+        zd = torch.empty(n, dtype=torch.float64, device="cuda")
+        cap = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+        def run(sweep):
+            F.probit_latent_device(fd.data_ptr(), yd.data_ptr(), n, float(ch["offset"]), int(ch["seed"]), sweep,
+                                   zd.data_ptr(), cap.data_ptr(), stream.cuda_stream)
+        for k in range(args.warmup):
+            run(k)
+        torch.cuda.synchronize()
+        ms = []
+        for k in range(max(args.steps, 3)):
+            flush.zero_()
+            a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            run(100 + k)
+            c.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(c))
+        sec = float(np.median(ms)) / 1000.0
+        gbs = 20.0 * n / sec / 1e9
+        z = zd.cpu().numpy()
+        ok = bool(np.all(z[yd.cpu().numpy() == 1] > -float(ch["offset"])))
+        res[name] = {"rows": int(n), "ms": 1000 * sec, "rows_per_s": n / sec, "achieved_gbs": gbs, "peak": peak,
+                     "frac": gbs / peak, "peak_source": peak_kind, "capped": int(cap.item()), "truncation_ok": ok}
+        del fd, yd, zd
+    res["note"] = ("one thread per row (grid-stride, 8 CTAs of 256 per SM); each draw runs Philox and FP64 log/exp "
+                   "in a rejection loop; algorithmic bytes 20 per row")
+    return res
+
+
 def predict_fresh_rows(F, ch, out, stream, device):
     """The probit configuration's second half: compile_trees of the fit's 100 kept draws, then predict_draw of every
     draw on a fresh 24,576-row table from the same distribution (FP64), timed with CUDA events on the device
@@ -430,9 +478,10 @@ def bench_ours(args):
                 "sigma_mean_ess": float(np.mean(ess_s)), "f_median_ess": float(np.mean(ess_f)), "kept": NDPOST}
     if WORKLOAD_NAME.startswith("fpbart"):   # probit: sigma is fixed at 1
         ess_line["sigma_per_s"] = ess_line["sigma_mean_ess"] = None
-    predict = None
+    predict = latent = None
     if WORKLOAD_NAME.startswith("fpbart"):
         predict = predict_fresh_rows(F, chains[0], outs[0], stream, local)
+        latent = latent_redraw(F, chains[0], outs[0], stream, args)
     b.close()
 
     # roofline of the sampler kernel (one launch per step)
@@ -539,6 +588,8 @@ def bench_ours(args):
                 "one_chain_per_launch": per_launch, "wall_s": wall}
         if predict is not None:
             line["predict_draw"] = predict
+        if latent is not None:
+            line["latent_redraw"] = latent
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

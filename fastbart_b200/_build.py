@@ -12,7 +12,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libfastbart_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["sampler.cu", "predict.cu", "mlp.cu", "text.cu", "host.cpp"]
+SOURCES = ["sampler.cu", "predict.cu", "mlp.cu", "text.cu", "latent.cu", "host.cpp"]
 HEADERS = ["fb_internal.h", "fb_math.cuh"]
 
 # -fmad=false: no implicit a*b+c contraction, so the sampler's FP64/FP32 arithmetic is exactly the IEEE sequence

@@ -295,6 +295,14 @@ def mlp_loss_grad(model: dict, x, y, mask, device: int = 0) -> tuple[float, dict
     return loss.value, g
 
 
+def probit_latent_device(fit_ptr: int, ybin_ptr: int, n: int, offset: float, seed: int, sweep: int, z_ptr: int,
+                         capped_ptr: int = 0, stream: int = 0):
+    """fpbart's latent redraw on device arrays (fb_probit_latent_device): z[i] for fits fit[i] (FP64) and outcomes
+    ybin[i] (int32) as the sampler draws it for that row at the end of 0-based sweep `sweep` (-1: the initial draw)."""
+    check(_lib.lib().fb_probit_latent_device(fit_ptr, ybin_ptr, int(n), float(offset), int(seed) & (2**64 - 1),
+                                             int(sweep), z_ptr, capped_ptr or None, stream or None))
+
+
 def cut_codes(x, cutpoints: Sequence[np.ndarray], device: int = 0) -> np.ndarray:
     """Cutpoint codes on the device (fb_cut_codes): q [p][n] uint8 with x < cutpoints[v][c] <=> q <= c."""
     X = np.asarray(x, dtype=np.float64)

@@ -48,7 +48,7 @@ __device__ __forceinline__ double u52d(uint32_t hi, uint32_t lo) {
 }
 
 __device__ __forceinline__ double fb_log_inl(double x);
-__device__ __noinline__ double fb_log(double x) { return fb_log_inl(x); }
+static __device__ __noinline__ double fb_log(double x) { return fb_log_inl(x); }
 // the same logarithm, inlined where its latency is on the critical path (the MH likelihoods)
 __device__ __forceinline__ double fb_log_inl(double x) {
   if (x != x) return x;
@@ -79,7 +79,7 @@ __device__ __forceinline__ double fb_log_inl(double x) {
   return fma(kd, 0x1.62e42fee00000p-1, fma(kd, 0x1.a39ef35793c76p-33, lf));
 }
 
-__device__ __noinline__ double fb_exp(double x) {
+static __device__ __noinline__ double fb_exp(double x) {
   if (x != x) return x;
   if (x > 709.78) return __longlong_as_double(0x7FF0000000000000LL);
   if (x < -745.2) return 0.0;
@@ -107,7 +107,7 @@ __device__ __noinline__ double fb_exp(double x) {
   return p * __longlong_as_double((long long)((unsigned long long)(k + 1023) << 52));
 }
 
-__device__ __noinline__ double fb_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag) {
+static __device__ __noinline__ double fb_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag) {
   for (uint32_t t = 0; t < 64; t++) {
     const U4 x = philox(c0base + t, c1, c2, tag, seed);
     const double a = 2.0 * u52d(x.x, x.y) - 1.0, b = 2.0 * u52d(x.z, x.w) - 1.0;
@@ -117,7 +117,7 @@ __device__ __noinline__ double fb_normal(uint64_t seed, uint32_t c0base, uint32_
   return 0.0;
 }
 
-__device__ __noinline__ double fb_gamma(uint64_t seed, uint32_t it, double a) {
+static __device__ __noinline__ double fb_gamma(uint64_t seed, uint32_t it, double a) {
   const double d = a - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
   for (uint32_t tt = 0; tt < 32; tt++) {
     const double x = fb_normal(seed, tt << 8, 0u, it, TAG_SIG_N);
@@ -132,7 +132,7 @@ __device__ __noinline__ double fb_gamma(uint64_t seed, uint32_t it, double a) {
 }
 
 // N(mean, 1) truncated to > tau; *capped is incremented when a loop gives up (then tau is returned).
-__device__ __noinline__ double fb_rtnorm(uint64_t seed, uint32_t row, uint32_t it, double mean, double tau, int* capped) {
+static __device__ __noinline__ double fb_rtnorm(uint64_t seed, uint32_t row, uint32_t it, double mean, double tau, int* capped) {
   tau = tau - mean;
   if (tau <= 0.0) {
     for (uint32_t tt = 0; tt < 64; tt++) {

@@ -1600,6 +1600,20 @@ fb_status fb_cut_loss_grad(const fb_cut_model* model, const float* x, const int*
   return FB_OK;
 }
 
+fb_status fb_probit_latent_device(const double* fit_dev, const int* ybin_dev, long long n, double offset,
+                                  uint64_t seed, int sweep, double* z_dev, int* capped_dev, void* cuda_stream) {
+  if (n < 0) return fail(FB_ERR_ARG, "n must be >= 0");
+  if (n > 0xFFFFFFFFll) return fail(FB_ERR_LIMIT, "n %lld exceeds the 2^32 rows a chain's counters address", n);
+  if (sweep < -1) return fail(FB_ERR_ARG, "sweep %d: 0-based, or -1 for the initial draw", sweep);
+  if (n == 0) return FB_OK;
+  if (!fit_dev || !ybin_dev || !z_dev) return fail(FB_ERR_ARG, "fit, ybin and z are required");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  if (launch_probit_latent(fit_dev, ybin_dev, n, offset, seed, (uint32_t)sweep, z_dev, capped_dev, cuda_stream) != 0)
+    return fail(FB_ERR_CUDA, "latent redraw launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return FB_OK;
+}
+
 fb_status fb_cut_codes(const double* const* cols, int ncol, int n, const double* const* cutpoints, const int* ncut,
                        int device, uint8_t* q) {
   if (ncol < 0 || n < 0) return fail(FB_ERR_ARG, "ncol and n must be >= 0");

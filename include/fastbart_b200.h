@@ -269,6 +269,13 @@ fb_status fb_predict_draws_device(const fb_compiled* ct, const double* x_dev, in
 fb_status fb_predict_draw_static(const fb_compiled* ct, const double* const* cols, int ncol, int n, int draw,
                                  double mu, double* out);
 
+/* The probit latent redraw of fpbart (src/bart_kernel.cpp:280-292, 543-547) on its own, over device arrays:
+ * z_dev[i] = N(fit_dev[i], 1) truncated to z > -offset when ybin_dev[i] is 1 and to z < -offset when it is 0, the
+ * value the sampler draws for row i of the chain with this seed at the end of 0-based sweep `sweep` (-1: the
+ * initial draw, whose fit is 0).  fit excludes the offset, as the sampler's fit does.  Draws that hit the 64-try cap
+ * are counted into *capped_dev when it is not NULL.  Enqueued on cuda_stream; rows up to 2^32. */
+fb_status fb_probit_latent_device(const double* fit_dev, const int* ybin_dev, long long n, double offset,
+                                  uint64_t seed, int sweep, double* z_dev, int* capped_dev, void* cuda_stream);
 /* Cutpoint codes on the device, the findInterval step of R/fwbart.R:19 and R/fpbart.R:13: q[v][i] = number of
  * cutpoints of predictor v that are <= cols[v][i] (so x < cutpoints[v][c] <=> q <= c; NaN gives 0).  cutpoints[v]
  * has ncut[v] (0..255) strictly increasing values; q is [ncol][n] bytes (host). */

@@ -157,6 +157,17 @@ double orc_rtnorm(uint64_t seed, uint32_t row, uint32_t it, double mean, double 
   return tau + mean;
 }
 
+/* The latent redraw of every row of a probit chain at one sweep (bart_kernel.cpp:543-547): z[i] = -rtnorm(-f, offset)
+   for ybin 0, rtnorm(f, -offset) for ybin 1, with the DEV counters (seed, row, sweep). Returns the capped draws. */
+int orc_probit_latent(uint64_t seed, uint32_t it, double offset, const double* fit, const int* ybin, long long n,
+                      double* z) {
+  int caps = 0;
+  for (long long i = 0; i < n; i++)
+    z[i] = ybin[i] == 0 ? -orc_rtnorm(seed, (uint32_t)i, it, -fit[i], offset, &caps)
+                        : orc_rtnorm(seed, (uint32_t)i, it, fit[i], -offset, &caps);
+  return caps;
+}
+
 /* ================================================================ tree helpers (bart_kernel.cpp:85-109, 220-278) */
 typedef struct {
   uint8_t l[ORC_NODES], r[ORC_NODES], par[ORC_NODES], v[ORC_NODES], c[ORC_NODES], d[ORC_NODES], ngv[ORC_NODES];

@@ -152,6 +152,8 @@ double orc_exp(double x);
 double orc_normal(uint64_t seed, uint32_t c0base, uint32_t c1, uint32_t c2, uint32_t tag);
 double orc_gamma(uint64_t seed, uint32_t it, double a);
 double orc_rtnorm(uint64_t seed, uint32_t row, uint32_t it, double mean, double tau, int* capped);
+int orc_probit_latent(uint64_t seed, uint32_t it, double offset, const double* fit, const int* ybin, long long n,
+                      double* z);
 
 /* ---------------------------------------------------------------- evaluator (src/predict.cpp) */
 typedef struct {

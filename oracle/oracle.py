@@ -130,6 +130,9 @@ def lib():
         L.orc_gamma.restype = C.c_double
         L.orc_rtnorm.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.POINTER(C.c_int)]
         L.orc_rtnorm.restype = C.c_double
+        L.orc_probit_latent.argtypes = [C.c_uint64, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p, C.c_longlong,
+                                        C.c_void_p]
+        L.orc_probit_latent.restype = C.c_int
         L.orc_compile_trees.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(_CT)]
         L.orc_compile_trees.restype = C.c_int
         L.orc_ct_free.argtypes = [C.POINTER(_CT)]
@@ -323,6 +326,16 @@ def normal(seed, c0, c1, c2, tag):
 
 def gamma(seed, it, a):
     return lib().orc_gamma(seed, it, a)
+
+
+def probit_latent(seed, it, offset, fit, ybin):
+    """z of every row at sweep `it` (-1: the initial draw) as the sampler draws it, and the capped draw count."""
+    f = np.ascontiguousarray(fit, dtype=np.float64)
+    y = np.ascontiguousarray(ybin, dtype=np.int32)
+    z = np.empty_like(f)
+    caps = lib().orc_probit_latent(int(seed) & (2**64 - 1), int(it) & 0xFFFFFFFF, float(offset), f.ctypes.data,
+                                   y.ctypes.data, f.size, z.ctypes.data)
+    return z, caps
 
 
 def rtnorm(seed, row, it, mean, tau):

@@ -56,6 +56,15 @@ def test_limits_on_shape():
     assert e.value.status == _lib.FB_ERR_LIMIT
 
 
+def test_latent_redraw_argument_errors():
+    with pytest.raises(F.FastbartError, match="sweep") as e:
+        F.probit_latent_device(1, 1, 10, 0.0, 1, -2, 1)
+    assert e.value.status == _lib.FB_ERR_ARG
+    with pytest.raises(F.FastbartError, match="required"):
+        F.probit_latent_device(0, 0, 10, 0.0, 1, 0, 0)
+    F.probit_latent_device(0, 0, 0, 0.0, 1, 0, 0)   # nothing to draw
+
+
 @pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-device path")
 def test_no_device_fails_loudly():
     with pytest.raises(F.FastbartError) as e:
@@ -63,6 +72,9 @@ def test_no_device_fails_loudly():
     assert e.value.status == _lib.FB_ERR_CUDA
     with pytest.raises(F.FastbartError):
         F.CompiledTrees("1 1 1\n1\n1 0 0 0.5\n", [np.array([0.5])])
+    with pytest.raises(F.FastbartError) as e:   # non-null stand-ins: the device check comes before any access
+        F.probit_latent_device(1, 1, 10, 0.0, 1, 0, 1)
+    assert e.value.status == _lib.FB_ERR_CUDA
 
 
 def test_text_and_varcount_match_oracle(orc):
