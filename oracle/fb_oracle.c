@@ -1286,7 +1286,7 @@ int orc_compile_trees(const char* text, const double* const* xi, const int* ncut
       th[k] = strtod(s, &e); s = e;
     }
     /* position of a node id among this tree's lines (ids are unique per tree); missing ids map to line 0, as
-       std::unordered_map::operator[] would insert 0 (predict.cpp:100) */
+       std::unordered_map::operator[] would insert 0 (src/predict.cpp:26, 38) */
 #define POS(id) ({ long _r = -1; for (long _k = 0; _k < nn; _k++) if (nid[_k] == (size_t)(id)) { _r = _k; break; } _r; })
     long* q = malloc(sizeof(long) * (size_t)(nn + 1)); int* slot = malloc(sizeof(int) * (size_t)(nn + 1));
     long qn = 0;
