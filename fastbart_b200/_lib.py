@@ -17,7 +17,7 @@ FB_OK, FB_ERR_ARG, FB_ERR_LIMIT, FB_ERR_CUDA, FB_ERR_PARSE, FB_ERR_SHAPE, FB_ERR
 
 EXPORTS = ["fb_last_error", "fb_version", "fb_fit_batch", "fb_batch_create", "fb_batch_run", "fb_batch_sync",
            "fb_batch_download", "fb_batch_launch_info", "fb_batch_destroy", "fb_fbart", "fb_trees_text",
-           "fb_varcount", "fb_compile_trees", "fb_compiled_info", "fb_predict_evaluator", "fb_probit_latent_device", "fb_compiled_arrays", "fb_compiled_free",
+           "fb_varcount", "fb_compile_trees", "fb_compiled_info", "fb_predict_evaluator", "fb_probit_latent_device", "fb_sigma_estimate", "fb_compiled_arrays", "fb_compiled_free",
            "fb_predict_draw", "fb_predict_draws_device", "fb_predict_draw_static", "fb_debug_tree_pass",
            "fb_batch_set_proposal", "fb_batch_collect", "fb_batch_training_data", "fb_train_proposal",
            "fb_mlp_loss_grad", "fb_autotune", "fb_cut_codes", "fb_trees_text_gpu", "fb_batch_trees_text",
@@ -124,6 +124,7 @@ def lib() -> C.CDLL:
         L.fb_compiled_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.fb_predict_evaluator.argtypes = [vp, i, i, C.POINTER(i), C.POINTER(C.c_longlong)]
         L.fb_probit_latent_device.argtypes = [vp, vp, C.c_longlong, d, C.c_uint64, i, vp, vp, vp]
+        L.fb_sigma_estimate.argtypes = [vp, i, i, vp, i, C.POINTER(d), C.POINTER(i)]
         L.fb_compiled_arrays.argtypes = [vp, vp, vp, vp, vp, vp]
         L.fb_compiled_free.argtypes = [vp]
         L.fb_compiled_free.restype = None

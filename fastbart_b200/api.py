@@ -303,6 +303,20 @@ def probit_latent_device(fit_ptr: int, ybin_ptr: int, n: int, offset: float, see
                                              int(sweep), z_ptr, capped_ptr or None, stream or None))
 
 
+def sigma_estimate(x, yc, device: int = 0) -> tuple[float, int]:
+    """(sigest, rank): the residual standard error of the least-squares fit yc ~ 1 + x computed from device Gram
+    sums (fb_sigma_estimate; R/fwbart.R:22), or sd(yc) when x has at least as many columns as rows."""
+    X = np.asarray(x, dtype=np.float64)
+    if X.ndim == 1:
+        X = X[:, None]
+    cols = [np.ascontiguousarray(X[:, v]) for v in range(X.shape[1])]
+    ptrs = (C.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+    y = np.ascontiguousarray(yc, dtype=np.float64)
+    out, rank = C.c_double(), C.c_int()
+    check(_lib.lib().fb_sigma_estimate(ptrs, len(cols), y.size, ptr(y), int(device), C.byref(out), C.byref(rank)))
+    return out.value, rank.value
+
+
 def cut_codes(x, cutpoints: Sequence[np.ndarray], device: int = 0) -> np.ndarray:
     """Cutpoint codes on the device (fb_cut_codes): q [p][n] uint8 with x < cutpoints[v][c] <=> q <= c."""
     X = np.asarray(x, dtype=np.float64)
@@ -374,8 +388,8 @@ def fwbart(x_train, y_train, x_test=None, sparse=False, xinfo=None, usequants=Fa
     yc = y - fm
     nu = float(sigdf)
     if lambda_ is None:
-        if sigest is None:
-            sigest = prep.sigest_lm(d.X, yc) if p < n else float(np.std(yc, ddof=1))
+        if sigest is None:   # lm's residual standard error (sd(yc) when p >= n), from Gram sums on the device
+            sigest = sigma_estimate(d.X, yc, device)[0]
         lambda_ = sigest * sigest * stats.chi2.ppf(1.0 - sigquant, nu) / nu
     else:
         sigest = float(np.sqrt(lambda_))

@@ -214,6 +214,8 @@ int predict_scratch_address(int device, double** ptr);
 // the probit latent redraw on its own (latent.cu): z[i] for fits fit[i] and outcomes ybin[i] at `sweep`
 int launch_probit_latent(const double* fit, const int* ybin, long long n, double offset, uint64_t seed, uint32_t sweep,
                          double* z, int* capped, void* stream);
+// Gram sums of [1, x_1 .. x_p, y] for the least-squares sigest (latent.cu): part[block][pair], x column-major [p][n]
+int launch_gram(const double* x, int n, int p, const double* y, int nblocks, int chunk, double* part, void* stream);
 // evaluator launch_predict uses for f: 0 streaming, 1 tiled, 2 code-compare, 3 code-compare carrying leaves across draws
 int predict_evaluator(const DForest& f, int n, int ndraws);
 int launch_predict(const DForest& f, const double* x, int n, int ld, int draw0, int ndraws, double mu, double* out,

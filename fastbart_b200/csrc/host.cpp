@@ -1614,6 +1614,87 @@ fb_status fb_probit_latent_device(const double* fit_dev, const int* ybin_dev, lo
   return FB_OK;
 }
 
+fb_status fb_sigma_estimate(const double* const* cols, int ncol, int n, const double* y, int device, double* sigest,
+                            int* rank) {
+  if (ncol < 0 || n < 2) return fail(FB_ERR_ARG, "need ncol >= 0 and n >= 2 (n = %d)", n);
+  if (ncol > 32) return fail(FB_ERR_LIMIT, "%d columns (at most 32)", ncol);
+  if (!y || !sigest || (ncol > 0 && !cols)) return fail(FB_ERR_ARG, "cols, y and sigest are required");
+  for (int v = 0; v < ncol; v++)
+    if (!cols[v]) return fail(FB_ERR_ARG, "column %d is missing", v);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FB_ERR_CUDA, "no CUDA device is available");
+  if (cudaSetDevice(device) != cudaSuccess) return fail(FB_ERR_CUDA, "cannot use device %d", device);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  const int q = ncol + 2, npairs = q * (q + 1) / 2;
+  long long nb = std::min<long long>(((long long)n + 63) / 64, 4ll * nsm);
+  const long long chunk = (((long long)n + nb - 1) / nb + 63) / 64 * 64;
+  nb = ((long long)n + chunk - 1) / chunk;
+  double *dx = nullptr, *dy = nullptr, *dp = nullptr;
+  fb_status st = FB_OK;
+  if (cudaMalloc(&dx, sizeof(double) * (size_t)std::max(ncol, 1) * n) != cudaSuccess ||
+      cudaMalloc(&dy, sizeof(double) * (size_t)n) != cudaSuccess ||
+      cudaMalloc(&dp, sizeof(double) * (size_t)nb * npairs) != cudaSuccess)
+    st = fail(FB_ERR_CUDA, "cannot allocate %lld rows x %d columns", (long long)n, ncol);
+  for (int v = 0; st == FB_OK && v < ncol; v++)
+    if (cudaMemcpy(dx + (size_t)v * n, cols[v], sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+      st = fail(FB_ERR_CUDA, "column copy failed");
+  if (st == FB_OK && cudaMemcpy(dy, y, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    st = fail(FB_ERR_CUDA, "y copy failed");
+  if (st == FB_OK && launch_gram(dx, n, ncol, dy, (int)nb, (int)chunk, dp, nullptr) != 0)
+    st = fail(FB_ERR_CUDA, "gram launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  std::vector<double> part((size_t)nb * npairs);
+  if (st == FB_OK && cudaMemcpy(part.data(), dp, sizeof(double) * part.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = fail(FB_ERR_CUDA, "gram copy failed: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaFree(dx); cudaFree(dy); cudaFree(dp);
+  if (st != FB_OK) return st;
+  // the blocks' sums in block order, into the symmetric matrix M of [1, x, y]
+  std::vector<double> M((size_t)q * q, 0.0);
+  for (int t = 0, j = 0, k = 0; t < npairs; t++) {
+    double a = 0.0;
+    for (long long b = 0; b < nb; b++) a += part[(size_t)b * npairs + t];
+    M[(size_t)j * q + k] = M[(size_t)k * q + j] = a;
+    if (++k == q) { ++j; k = j; }
+  }
+  const int yi = q - 1;
+  if (ncol >= n) {   // sd(yc) (R/fwbart.R:22 when p >= n)
+    const double sy = M[yi], syy = M[(size_t)yi * q + yi];
+    *sigest = std::sqrt(std::max(0.0, (syy - sy * sy / n) / (n - 1)));
+    if (rank) *rank = 0;
+    return FB_OK;
+  }
+  // lm's residual standard error: eliminate the columns of [1, x] with symmetric pivoting (largest remaining
+  // diagonal first, columns whose remaining diagonal falls below 1e-12 of the largest are aliased, as lm drops
+  // them); what remains in the y, y entry is the residual sum of squares, with n - rank degrees of freedom
+  const int p1 = ncol + 1;
+  double dmax = 0.0;
+  for (int i = 0; i < p1; i++) dmax = std::max(dmax, M[(size_t)i * q + i]);
+  std::vector<int> perm(q);
+  for (int i = 0; i < q; i++) perm[i] = i;
+  int r = 0;
+  for (; r < p1; r++) {
+    int piv = r;
+    for (int i = r + 1; i < p1; i++)
+      if (M[(size_t)perm[i] * q + perm[i]] > M[(size_t)perm[piv] * q + perm[piv]]) piv = i;
+    std::swap(perm[r], perm[piv]);
+    const int s_ = perm[r];
+    const double d = M[(size_t)s_ * q + s_];
+    if (!(d > 1e-12 * dmax)) break;
+    for (int i = r + 1; i < q; i++) {
+      const int a = perm[i];
+      const double f = M[(size_t)a * q + s_] / d;
+      for (int jj = r + 1; jj < q; jj++) {
+        const int b = perm[jj];
+        M[(size_t)a * q + b] -= f * M[(size_t)s_ * q + b];
+      }
+    }
+  }
+  const double rss = std::max(0.0, M[(size_t)yi * q + yi]);
+  *sigest = std::sqrt(rss / (n - r));
+  if (rank) *rank = r;
+  return FB_OK;
+}
+
 fb_status fb_cut_codes(const double* const* cols, int ncol, int n, const double* const* cutpoints, const int* ncut,
                        int device, uint8_t* q) {
   if (ncol < 0 || n < 0) return fail(FB_ERR_ARG, "ncol and n must be >= 0");

@@ -276,6 +276,12 @@ fb_status fb_predict_draw_static(const fb_compiled* ct, const double* const* col
  * are counted into *capped_dev when it is not NULL.  Enqueued on cuda_stream; rows up to 2^32. */
 fb_status fb_probit_latent_device(const double* fit_dev, const int* ybin_dev, long long n, double offset,
                                   uint64_t seed, int sweep, double* z_dev, int* capped_dev, void* cuda_stream);
+/* sigest of the preprocessing (R/fwbart.R:22): the residual standard error of the least-squares fit of y on an
+ * intercept and the columns (summary(lm(yc ~ X))$sigma), from FP64 Gram sums computed on the device; aliased columns
+ * are dropped as lm drops them (*rank = the columns kept, intercept included).  When ncol >= n it is sd(y), as in
+ * the reference (*rank = 0).  cols[v] are host columns of n doubles, at most 32. */
+fb_status fb_sigma_estimate(const double* const* cols, int ncol, int n, const double* y, int device, double* sigest,
+                            int* rank);
 /* Cutpoint codes on the device, the findInterval step of R/fwbart.R:19 and R/fpbart.R:13: q[v][i] = number of
  * cutpoints of predictor v that are <= cols[v][i] (so x < cutpoints[v][c] <=> q <= c; NaN gives 0).  cutpoints[v]
  * has ncut[v] (0..255) strictly increasing values; q is [ncol][n] bytes (host). */

@@ -56,6 +56,15 @@ def test_limits_on_shape():
     assert e.value.status == _lib.FB_ERR_LIMIT
 
 
+def test_sigma_estimate_argument_errors():
+    with pytest.raises(F.FastbartError, match="n >= 2") as e:
+        F.sigma_estimate(np.zeros((1, 2)), np.zeros(1))
+    assert e.value.status == _lib.FB_ERR_ARG
+    with pytest.raises(F.FastbartError, match="at most 32") as e:
+        F.sigma_estimate(np.zeros((40, 33)), np.zeros(40))
+    assert e.value.status == _lib.FB_ERR_LIMIT
+
+
 def test_latent_redraw_argument_errors():
     with pytest.raises(F.FastbartError, match="sweep") as e:
         F.probit_latent_device(1, 1, 10, 0.0, 1, -2, 1)

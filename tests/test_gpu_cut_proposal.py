@@ -105,6 +105,23 @@ def test_cut_gradients_match_oracle(orc):
         assert np.abs(g[k] - og[k]).max() <= tol, k
 
 
+def test_cut_gradients_match_oracle_many_tiles(orc):
+    # 6,000 examples: CTAs sum several 32-example tiles before their atomics
+    rng = np.random.default_rng(22)
+    n = 6000
+    x = rng.random((n, 40), dtype=np.float32)
+    lo = rng.integers(0, 200, n).astype(np.int32)
+    hi = np.minimum(lo + rng.integers(0, 60, n), 254).astype(np.int32)
+    c = (lo + (rng.random(n) * (hi - lo + 1)).astype(np.int32)).astype(np.int32)
+    cut = random_cut(13, scale=0.2)
+    loss, g = F.cut_loss_grad(cut, x, c, lo, hi)
+    oloss, og = orc.cut_loss_grad(cut, x, c, lo, hi)
+    assert abs(loss - oloss) <= 1e-4 * max(1.0, abs(oloss))
+    for k in og:
+        tol = 2e-3 * max(np.abs(og[k]).max(), 1e-6)
+        assert np.abs(g[k] - og[k]).max() <= tol, k
+
+
 def test_cut_training_and_posterior_unchanged(orc):
     # accepted births of plain chains teach both heads; chains with both learned heads agree with plain chains
     ch0 = W.fwbart_friedman(n=1500, p=16, seed=41, ntree=50, nskip=200, ndpost=100)

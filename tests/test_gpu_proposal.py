@@ -86,6 +86,22 @@ def test_training_gradients_match_oracle(orc):
         assert np.abs(g[k] - og[k]).max() <= tol, k
 
 
+def test_training_gradients_match_oracle_many_tiles(orc):
+    # 6,000 examples: 188 tiles of 32 on at most one CTA per SM, so CTAs sum several tiles before their atomics
+    rng = np.random.default_rng(21)
+    n = 6000
+    x = rng.random((n, 98), dtype=np.float32)
+    m = rng.integers(1, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    y = np.array([rng.choice(np.flatnonzero((int(v) >> np.arange(32)) & 1)) for v in m], np.int32)
+    model = random_model(12, scale=0.2)
+    loss, g = F.mlp_loss_grad(model, x, y, m)
+    oloss, og = orc.mlp_loss_grad(model, x, y, m)
+    assert abs(loss - oloss) <= 1e-4 * max(1.0, abs(oloss))
+    for k in og:
+        tol = 2e-3 * max(np.abs(og[k]).max(), 1e-6)
+        assert np.abs(g[k] - og[k]).max() <= tol, k
+
+
 def test_training_learns_the_signal_predictors(orc):
     # Friedman signal on x1..x5 among 16 predictors: accepted births concentrate on the signal
     chains = [W.fwbart_friedman(n=2000, p=16, seed=20 + k, ntree=50, nskip=150, ndpost=50) for k in range(4)]
