@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(PC_ROWS) predict_codes_kernel(DForest f, const
 // draw walks only the trees whose structure changed (the flags are per draw and tree, so the branch is uniform across
 // the CTA), each for its own depth, and reads the other leaves' offsets.  Leaf values are added in tree order, the
 // same FP64 additions as src/predict.cpp:62-70, so the results equal the other evaluators' bit for bit.
-__global__ void __launch_bounds__(PC_ROWS) predict_carry_kernel(DForest f, const double* __restrict__ x, int n, int ld,
+__global__ void __launch_bounds__(PC_ROWS, 3) predict_carry_kernel(DForest f, const double* __restrict__ x, int n, int ld,
                                                                 int draw0, int ndraws, int dpc, double mu,
                                                                 double* __restrict__ out, int ldo, int ncodes) {
   extern __shared__ __align__(16) unsigned char pc_smem[];
@@ -230,27 +230,64 @@ __global__ void __launch_bounds__(PC_ROWS) predict_carry_kernel(DForest f, const
   const long long ntot = (long long)f.ndpost * m;
   const int SW = (m + 31) / 32;
   const int d0 = blockIdx.y * dpc, d1 = min(ndraws, d0 + dpc);
-  for (int d = d0; d < d1; d++) {
+  // a range's first draw walks every tree; trees past ntree (padding of the last group) never walk
+  auto keep_bits = [&](int d, int g) {
+    uint32_t keep = d == d0 ? 0u : (__ldg(f.same + (long long)(draw0 + d) * SW + (g >> 3)) >> ((g & 7) * 4)) & 15u;
+    for (int u = 0; u < 4; u++)
+      if (4 * g + u >= m) keep |= 1u << u;
+    return keep;
+  };
+  // When a draw has at most PF x PC_ROWS nodes (4 G <= 200 < PC_ROWS always), each thread loads its share of the next
+  // draw's tables into registers while the current draw is evaluated, and stores them after the next barrier, so
+  // the tables' global-memory latency is not exposed once per draw.
+  constexpr int PF = 4;
+  const bool pipe = f.maxnd <= PF * PC_ROWS;
+  uint32_t pn[PF];
+  double pt[PF];
+  uint32_t prt = 0, ptd = 0, psg = 0;
+  int pcnt = 0;
+  auto load_next = [&](int d) {
     const long long t0 = (long long)(draw0 + d) * m;
     const int base = __ldg(f.root + t0);
-    const int cnt = (t0 + m < ntot ? __ldg(f.root + t0 + m) : f.nnodes) - base;
+    pcnt = (t0 + m < ntot ? __ldg(f.root + t0 + m) : f.nnodes) - base;
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+      const int k = tid + u * PC_ROWS;
+      if (k < pcnt) { pn[u] = __ldg(f.n32 + base + k); pt[u] = __ldg(f.theta + base + k); }
+    }
+    if (tid < 4 * G) {
+      prt = tid < m ? (uint32_t)(__ldg(f.root + t0 + tid) - base) : 0u;
+      ptd = tid < m ? (uint32_t)__ldg(f.tdep + t0 + tid) : 0u;
+    }
+    if (tid < G) psg = keep_bits(d, tid);
+  };
+  if (pipe && d0 < d1) load_next(d0);
+  for (int d = d0; d < d1; d++) {
     __syncthreads();   // the previous draw's tables are no longer read
-    for (int k = tid; k < cnt; k += PC_ROWS) {
-      nd_s[k] = __ldg(f.n32 + base + k);
-      th_s[k] = __ldg(f.theta + base + k);
-    }
-    for (int t = tid; t < 4 * G; t += PC_ROWS) {
-      rt_s[t] = t < m ? (uint16_t)(__ldg(f.root + t0 + t) - base) : (uint16_t)0;
-      td_s[t] = t < m ? __ldg(f.tdep + t0 + t) : (uint8_t)0;
-    }
-    for (int g = tid; g < G; g += PC_ROWS) {
-      // a range's first draw walks every tree; trees past ntree (padding of the last group) never walk
-      uint32_t keep = d == d0 ? 0u : (__ldg(f.same + (long long)(draw0 + d) * SW + (g >> 3)) >> ((g & 7) * 4)) & 15u;
-      for (int u = 0; u < 4; u++)
-        if (4 * g + u >= m) keep |= 1u << u;
-      sg_s[g] = (uint8_t)keep;
+    if (pipe) {
+#pragma unroll
+      for (int u = 0; u < PF; u++) {
+        const int k = tid + u * PC_ROWS;
+        if (k < pcnt) { nd_s[k] = pn[u]; th_s[k] = pt[u]; }
+      }
+      if (tid < 4 * G) { rt_s[tid] = (uint16_t)prt; td_s[tid] = (uint8_t)ptd; }
+      if (tid < G) sg_s[tid] = (uint8_t)psg;
+    } else {
+      const long long t0 = (long long)(draw0 + d) * m;
+      const int base = __ldg(f.root + t0);
+      const int cnt = (t0 + m < ntot ? __ldg(f.root + t0 + m) : f.nnodes) - base;
+      for (int k = tid; k < cnt; k += PC_ROWS) {
+        nd_s[k] = __ldg(f.n32 + base + k);
+        th_s[k] = __ldg(f.theta + base + k);
+      }
+      for (int t = tid; t < 4 * G; t += PC_ROWS) {
+        rt_s[t] = t < m ? (uint16_t)(__ldg(f.root + t0 + t) - base) : (uint16_t)0;
+        td_s[t] = t < m ? __ldg(f.tdep + t0 + t) : (uint8_t)0;
+      }
+      for (int g = tid; g < G; g += PC_ROWS) sg_s[g] = (uint8_t)keep_bits(d, g);
     }
     __syncthreads();
+    if (pipe && d + 1 < d1) load_next(d + 1);
     if (!live) continue;
     double acc = 0.0;
     uint32_t wn = lf[0];
