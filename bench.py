@@ -286,6 +286,9 @@ def agreement(picks, gpu_main, gpu_second, ref_results):
             "ref_seed_spread_median": float(np.median(col("ref_seed_spread"))),
             "r_f_pooled_min": min(col("r_f_pooled")), "r_f_pooled_median": float(np.median(col("r_f_pooled"))),
             "sigma_ratio_min": min(col("sigma_ratio")), "sigma_ratio_max": max(col("sigma_ratio")),
+            # over all shapes (geometric mean of the per-shape ratios): the per-shape ratios scatter by the reference's
+            # own seed-to-seed spread, the pooled one carries the systematic difference
+            "sigma_ratio_pooled": float(np.exp(np.mean(np.log(col("sigma_ratio"))))),
             "ref_sigma_seed_ratio_max": max(col("ref_sigma_seed_ratio")),
             "per_shape": per,
             "what": "one chain per shape; r_f = corr(posterior-mean f) of this sampler's chain and one reference "
