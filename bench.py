@@ -638,17 +638,50 @@ def _pred_forest():
     from fastbart_b200 import workloads as W
     trees = W.random_forest(PRED_DRAWS, 200, PRED_P, 100, seed=11)
     cps = [np.arange(1, 101, dtype=np.float64) / 101.0 for _ in range(PRED_P)]
-    return F.trees_text(trees, PRED_P), cps, 0.5
+    return F.trees_text(trees, PRED_P), cps, 0.5, trees
+
+
+def walk_steps(trees: np.ndarray) -> float:
+    """Node steps the code-compare evaluator executes per row and draw: per group of four consecutive trees, four
+    walks of the group's deepest leaf (averaged over the draws of the packed forest [D][T][64])."""
+    t = np.asarray(trees, dtype=np.uint64)
+    used = (t & np.uint64(255)) != np.uint64(255)
+    lch = ((t >> np.uint64(16)) & np.uint64(255)).astype(np.int64)
+    rch = ((t >> np.uint64(24)) & np.uint64(255)).astype(np.int64)
+    D, T, S = t.shape
+    depth = np.full((D, T, S), -1, np.int64)
+    depth[:, :, 0] = 0
+    di, ti = np.meshgrid(np.arange(D), np.arange(T), indexing="ij")
+    for _ in range(S):   # children one level below their parents, until nothing changes
+        inner = used & (lch > 0) & (depth >= 0)
+        if not inner.any():
+            break
+        old = depth.copy()
+        for ch in (lch, rch):
+            d_, t_, s_ = np.nonzero(inner)
+            depth[d_, t_, ch[d_, t_, s_]] = depth[d_, t_, s_] + 1
+        if np.array_equal(old, depth):
+            break
+    tdep = depth.max(axis=2)                       # [D][T]
+    G = (T + 3) // 4
+    pad = np.zeros((D, 4 * G), np.int64)
+    pad[:, :T] = tdep
+    return float((4 * pad.reshape(D, G, 4).max(axis=2)).sum(axis=1).mean())
 
 
 def bench_predict(args):
+    global PRED_DRAWS, PRED_ROWS
+    if args.pred_rows:
+        PRED_ROWS = int(args.pred_rows)
+    if args.pred_draws:
+        PRED_DRAWS = int(args.pred_draws)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference" and rank != 0:
         return 0
     import fastbart_b200 as F
-    text, cps, mu = _pred_forest()
+    text, cps, mu, ptrees = _pred_forest()
     impl_ref = args.impl == "reference"
     cpu = None
     if rank == 0 and (impl_ref or (world == 1 and not args.no_cpu_baseline)):
@@ -725,6 +758,12 @@ def bench_predict(args):
             "algorithmic_bytes": alg,
             "node_steps_note": "x read once, every output written once, each draw's packed nodes and leaf values read"}
     roof["evaluator"] = ct.evaluator(PRED_ROWS, PRED_DRAWS)[0]
+    # the rate in tree visits and in the node steps the code-compare evaluator executes (per group of four trees, four
+    # walks of the group's deepest leaf): the issue-bound figure to compare kernels by
+    steps = walk_steps(ptrees)
+    roof["tree_visits_per_s"] = value * 200
+    roof["walk_steps_per_row_draw"] = steps
+    roof["node_steps_per_s"] = value * steps
     # the same call on draws shaped like one chain's consecutive posterior draws (most tree structures kept from
     # draw to draw, every leaf value redrawn): the evaluator then carries each row's leaves across draws
     post = None
@@ -788,7 +827,8 @@ def bench_predict(args):
         line = {"metric": PRED_METRIC, "value": value, "unit": PRED_UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "predict_bulk_1000x1M", "draws": PRED_DRAWS, "ntree": 200,
+                "config": {"workload": "predict_bulk_1000x1M" if (PRED_DRAWS, PRED_ROWS) == (1000, 1_000_000)
+                           else f"predict_bulk_{PRED_DRAWS}x{PRED_ROWS}", "draws": PRED_DRAWS, "ntree": 200,
                            "rows": PRED_ROWS, "p": PRED_P, "nodes": ct.nnodes,
                            "l2": "flushed (512 MiB write) before every timed step; inputs and outputs exceed L2"},
                 "e2e": e2e, "gpu_launches": args.steps * (2 if post else 1), "roofline": roof, "cpu_baseline": cpu,
@@ -1261,6 +1301,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-posterior", action="store_true", help="predict: skip the posterior-shaped forest leg")
+    ap.add_argument("--pred-rows", type=int, default=0, help="predict: rows (default 1,000,000; smaller for profiling)")
+    ap.add_argument("--pred-draws", type=int, default=0, help="predict: draws (default 1,000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single", action="store_true", help="skip the one-chain-per-launch comparison")
     ap.add_argument("--workload", default="titer96",

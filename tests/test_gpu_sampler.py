@@ -92,6 +92,19 @@ def test_batch_uneven_chains_bit_exact(orc):
         _compare(g, orc.fit(ch, orc.MODE_DEV))
 
 
+def test_fit_batch_over_devices_equals_one_batch():
+    """fit_batch(devices=...) partitions the chains (longest processing time first) and runs each share as its own
+    batch from its own host thread; with the one GPU of this box listed twice, two batches run concurrently on it.
+    Chains are independent, so every chain's outputs equal those of the single batch bit for bit, in chain order."""
+    chains = [W.fwbart_friedman(n=n, p=4, seed=50 + n, ntree=15, nskip=10, ndpost=5) for n in (300, 1200, 700, 2000)]
+    chains.append(W.fpbart_hazard(n=900, seed=57, ntree=8, nskip=10, ndpost=5))
+    one = fit_batch(chains, 10, 5)
+    two = fit_batch(chains, 10, 5, devices=[0, 0])
+    assert len(two) == len(chains)
+    for a, b in zip(one, two):
+        _compare(b, a, keys=("sigma", "yhat_mean", "yhat", "trees", "moves"))
+
+
 @pytest.mark.parametrize("threads,spl", [(64, 7), (512, 0)])
 def test_launch_shape_does_not_change_results(orc, threads, spl):
     ch = W.fwbart_friedman(n=700, p=6, seed=21, ntree=25, nskip=20, ndpost=10)
