@@ -1482,11 +1482,19 @@ __device__ void run_chain(const DBufs& B, int ci, int it0, int it1, const Smem& 
         U.xhist = cutb ? 1 : 0;
         U.sqa = (cutb || csq) ? P.nx : cutd ? P.l : -1;
         U.sqb = cutd ? P.r : U.sqa;
+        // the pass with the cut proposal's extras (squared residuals, code histogram) only in the steps that use
+        // them: a step of a chain without a cut head runs the plain pass
         if constexpr (G > 0) {
-          if (regs) pass_rows_regs<G, MP>(U, j == 0, lcr, qcr, nlc, nqc);
-          else pass_rows_stream<MP>(U);
+          if (regs) {
+            if (MP && sqon) pass_rows_regs<G, MP>(U, j == 0, lcr, qcr, nlc, nqc);
+            else pass_rows_regs<G, false>(U, j == 0, lcr, qcr, nlc, nqc);
+          } else {
+            if (MP && sqon) pass_rows_stream<MP>(U);
+            else pass_rows_stream<false>(U);
+          }
         } else {
-          pass_rows_stream<MP>(U);
+          if (MP && sqon) pass_rows_stream<MP>(U);
+          else pass_rows_stream<false>(U);
         }
       } else {
         // control warp: commit tree j-1, fetch tree j+1 into the freed buffer, draw the normals of every slot that
