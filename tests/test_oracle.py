@@ -67,6 +67,37 @@ def test_normal_gamma_rtnorm_moments(orc):
     assert abs(t.mean() - ref) < 0.03
 
 
+def test_oracle_probit_latent_truncation_and_moments(orc):
+    # the latent redraw the GPU kernel is checked against: z on the side of -offset that ybin gives, row by row the
+    # rtnorm of the sampler's counters, and N(f, 1) truncated to that side in distribution
+    rng = np.random.default_rng(8)
+    n, off = 20000, 0.4
+    f = rng.normal(0.0, 0.5, n)
+    yb = (rng.random(n) < 0.5).astype(np.int32)
+    z, caps = orc.probit_latent(77, 12, off, f, yb)
+    assert caps == 0
+    assert np.all(z[yb == 1] > -off) and np.all(z[yb == 0] < -off)
+    for i in (0, 1, 2, 999):
+        one = orc.rtnorm(77, i, 12, f[i], -off)[0] if yb[i] else -orc.rtnorm(77, i, 12, -f[i], off)[0]
+        assert one == z[i]
+    c = np.zeros(n)   # fit 0: E[z | z > -off] for ybin 1
+    z0, _ = orc.probit_latent(5, 0, off, c, np.ones(n, np.int32))
+    a = -off
+    ref = math.exp(-a * a / 2) / math.sqrt(2 * math.pi) / (0.5 * math.erfc(a / math.sqrt(2)))
+    assert abs(z0.mean() - ref) < 0.02
+
+
+def test_posterior_forest_keeps_structures_and_redraws_leaves():
+    from fastbart_b200 import workloads as W
+    t = W.posterior_forest(40, 50, 6, 20, change=0.25, seed=3)
+    low = np.uint64(0xFFFFFFFF)
+    same = np.array([np.all((t[d] & low) == (t[d - 1] & low), axis=1) for d in range(1, 40)])
+    assert 0.65 < same.mean() < 0.85                      # about 1 - change of the trees keep their structure
+    leaf = ((t & np.uint64(255)) != np.uint64(255)) & (((t >> np.uint64(16)) & np.uint64(255)) == np.uint64(0))
+    kept = same[:, :, None] & leaf[1:]
+    assert np.mean((t[1:] >> np.uint64(32))[kept] != (t[:-1] >> np.uint64(32))[kept]) > 0.99   # new leaf values
+
+
 def _random_pass_state(rng, n, nleaf, pmode):
     slots = np.sort(rng.choice(np.arange(64), size=nleaf, replace=False)).astype(np.uint8)
     lc = rng.choice(slots, n).astype(np.uint8)
